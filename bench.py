@@ -1,0 +1,387 @@
+"""Benchmark: simulated time per wall-second of the 2-D LLG integration.
+
+Workload (one B200, the configuration the metric is quoted on): 1536x512
+cells, centred square hole of side 0.25*ny, open-boundary FFT demag
+(strength 4, thickness 1, zero-padded 3072x1024 transform grid), exchange
+A=1, uniaxial k=0.1 along +x, Zeeman (0,0,0.05), alpha=0.02, free edges,
+uniform (1,0,0) + seeded +-0.01 jitter, BDF + Newton + SPGMR(5) with 3x3
+block-Jacobi, rtol 1e-4 / atol 1e-6, FP64.  Synthetic data (seeded builders).
+
+A "step" integrates `--dt` units of simulated time (default 1.0) through
+llg_integrate at the reference's 0.1 output cadence.  value = K*dt / device
+time of K steps (CUDA events on the library's stream, max over ranks);
+the state (>= 20 vectors of 18.9 MB) exceeds L2, so no flush is needed.
+
+--impl reference runs the CPU restatement of the reference path (the oracle;
+the reference itself needs SUNDIALS, which is absent) on all host cores.
+Multi-GPU: independent replicas (one instance per rank, no collective in
+the hot path); only the timing max uses torch.distributed.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "gpu-micromagnetics-irregular_b200")
+sys.path.insert(0, PKG)
+import llg  # noqa: E402
+
+METRIC = "sim-time/wall-s @1536x512+demag, learned+mixed vs plain FP64, |Δm|≤1e-4"
+UNIT = "sim-time/wall-s"
+KERNEL_NAMES = ["rhs", "jtv", "arnoldi_op", "psetup", "psolve", "normalize", "demag_rows_fwd",
+                "demag_cols_conv", "demag_rows_inv", "reduce", "elementwise", "learned", "other"]
+
+
+def workload(ng=1536, ny=512, seed=12345):
+    p = llg.default_params(ng, ny, demag_mode=llg.DEMAG_OPEN, demag_strength=4.0, demag_thick=1.0,
+                           bc=llg.BC_FREE, norm_kind=llg.NORM_REG)
+    g = llg.default_geom(ng, ny, geometry_kind=llg.GEOM_HOLE_SQUARE, hole_radius_frac_y=0.125,
+                         ic_jitter_eps=0.01, init_random_seed=seed)
+    o = llg.default_solver_opts(rtol=1e-4, atol=1e-6, maxl=5, gs_type=llg.GS_CLASSICAL)
+    return p, g, o
+
+
+def algorithmic_bytes(kid, ng, ny, dims):
+    """Compulsory HBM bytes of one launch of kernel family kid (FP64)."""
+    n = ng * ny
+    px, py, hx, nrows = dims
+    S = 3 * hx * nrows * 16
+    if kid == 0:   # rhs: y, hd, mask in; ydot out
+        return 24 * n + 24 * n + n + 24 * n
+    if kid == 1:   # jtv: y, v, mask in; Jv out
+        return 24 * n + 24 * n + n + 24 * n
+    if kid == 2:   # arnoldi: V_l, ewt, y, frozen m, frozen h, mask in; V_l+1 out
+        return 5 * 24 * n + n + 24 * n
+    if kid == 3:   # psetup: y, hd, mask in; m, h out
+        return 24 * n + 24 * n + n + 48 * n
+    if kid == 4:   # psolve: m, h, r, mask in; z out
+        return 72 * n + n + 24 * n
+    if kid == 6:   # rows forward: y in; row spectra out
+        return 24 * n + S
+    if kid == 7:   # columns: spectra in/out + tensor (xx,yy,zz real, xy complex)
+        return 2 * S + hx * py * 40
+    if kid == 8:   # rows inverse: spectra in; h out
+        return S + 24 * n
+    if kid == 9:   # dot_multi of 6 vectors: 7 vectors read
+        return 7 * 24 * n
+    if kid == 10:  # linear combination of 6 vectors: 6 read + 1 write
+        return 7 * 24 * n
+    return 0
+
+
+class Clocks:
+    def __init__(self, dev):
+        self.proc = None
+        self.dev = dev
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (getattr(self, "out", "") or "").splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                try:
+                    rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+                except ValueError:
+                    pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_ctx(p, g):
+    geo = llg.build_geometry(g, want=("active", "y0"))
+    ctx = llg.Context(p)
+    ctx.set_mask(np.tile(geo["active"].astype(np.float64), 3))
+    return ctx, geo
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    lib = llg.load()
+    p, g, o = workload(seed=12345 + rank)
+    ng, ny = p.ng, p.ny
+    n = ng * ny
+    ctx, geo = make_ctx(p, g)
+    y0 = torch.from_numpy(geo["y0"]).cuda()
+    ctx.integrator_init(0.0, y0, o)
+    yout = torch.zeros_like(y0)
+    t = 0.0
+    sub = max(1, int(round(args.dt / 0.1)))
+
+    def step():
+        nonlocal t
+        for k in range(sub):
+            ctx.integrate(t + args.dt * (k + 1) / sub, yout)
+        t += args.dt
+
+    for _ in range(args.warmup):
+        step()
+    counts0 = (C.c_int64 * 16)()
+    counts1 = (C.c_int64 * 16)()
+    lib.llg_kernel_counts(counts0, 16)
+    st0 = ctx.stats()
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms_local = e0.elapsed_time(e1)
+    dist_barrier(world)
+    ms = dist_max(ms_local, world)
+    lib.llg_kernel_counts(counts1, 16)
+    st1 = ctx.stats()
+    launches = {KERNEL_NAMES[k]: int(counts1[k] - counts0[k]) for k in range(13)}
+    total_launches = sum(launches.values())
+    sim = args.steps * args.dt
+    value = world * sim / (ms / 1000.0)
+
+    # per-family device time on live buffers → shares and the dominant kernel
+    dims = (C.c_int * 4)()
+    fam_ms = {}
+    for kid in (0, 1, 2, 3, 4, 6, 7, 8, 9, 10):
+        if launches[KERNEL_NAMES[kid]] == 0 and kid not in (6, 7, 8):
+            continue
+        avg = C.c_double()
+        if lib.llg_time_kernel(ctx.h, kid, 20, C.byref(avg)) == 0:
+            fam_ms[kid] = avg.value
+    share = {k: fam_ms[k] * launches[KERNEL_NAMES[k]] for k in fam_ms}
+    dom = max(share, key=share.get) if share else 7
+    px, py = 2 * ng, 2 * ny
+    dd = (px, py, px // 2 + 1, ny)
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    abytes = algorithmic_bytes(dom, ng, ny, dd)
+    achieved = abytes / (fam_ms[dom] * 1e-3) / 1e9 if dom in fam_ms else None
+    traffic = None
+    try:
+        with open(os.path.join(REPO, "profiles", "traffic_per_launch.json")) as f:
+            traffic = json.load(f).get(KERNEL_NAMES[dom])
+    except Exception:
+        pass
+
+    # end to end: host buffers in, host frames out, through the public API
+    e2e = None
+    if not args.no_e2e:
+        ctx2 = llg.Context(p)
+        geo2 = llg.build_geometry(g, want=("active", "y0"))
+        mask_h = torch.from_numpy(np.tile(geo2["active"].astype(np.float64), 3)).pin_memory()
+        y0_h = torch.from_numpy(geo2["y0"]).pin_memory()
+        frame_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+        y0_d = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+        yo_d = torch.empty_like(y0_d)
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        ctx2.set_mask(mask_h.numpy())
+        y0_d.copy_(y0_h, non_blocking=True)
+        ctx2.integrator_init(0.0, y0_d, o)
+        tt = 0.0
+        for _ in range(args.steps):
+            for k in range(sub):
+                ctx2.integrate(tt + args.dt * (k + 1) / sub, yo_d)
+            tt += args.dt
+            frame_h.copy_(yo_d, non_blocking=True)
+        f1.record()
+        torch.cuda.synchronize()
+        ems = dist_max(f0.elapsed_time(f1), world)
+        e2e = {"value": world * args.steps * args.dt / (ems / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": int((y0_h.numel() * 8 + mask_h.numel() * 8) / args.steps),
+               "d2h_bytes_per_step": int(frame_h.numel() * 8),
+               "note": "fresh instance from t=0: pinned y0 + mask uploaded once and amortised over the steps; "
+                       "one y(t) frame copied back per step; includes integrator start-up"}
+        ctx2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args)
+
+    dst = {k: st1[k] - st0[k] for k in ("nst", "nfe", "nni", "nli", "nsetups", "netf", "ncfn")}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry/IC builders)",
+        "config": {"workload": "1536x512 cells, square hole side 0.25*ny, open FFT demag strength 4 "
+                               "(3072x1024 padded), A=1 k=0.1(+x) h=(0,0,0.05) alpha=0.02, free edges, "
+                               "rtol 1e-4 atol 1e-6, SPGMR(5)+block-Jacobi, classical GS, FP64",
+                   "form": "plain FP64 (block-Jacobi, FP64 demag)", "sim_time_per_step": args.dt,
+                   "output_interval": 0.1, "parallelism": f"replicas x{world}",
+                   "l2": "state > 126 MB L2 (>= 20 vectors x 18.9 MB); no flush",
+                   "solver_counters_timed": dst},
+        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": fam_ms.get(dom),
+                     "peak_source": f"{peak_src} hbm_gbs (burst copy)",
+                     "kernel_avg_ms": {KERNEL_NAMES[k]: v for k, v in fam_ms.items()},
+                     "kernel_share": {KERNEL_NAMES[k]: v / max(sum(share.values()), 1e-30)
+                                      for k, v in share.items()}},
+        "e2e": e2e, "gpu_launches": total_launches, "launches_by_family": launches,
+        "clocks": clk.summary(), "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_oracle_run(dt_step, steps, warmup, threads):
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import binding
+    binding.build()
+    used = binding.set_threads(threads)
+    p, g, o = workload()
+    geo = binding.build_geometry(g)
+    orc = binding.Oracle(p)
+    orc.set_active(geo["active"])
+    orc.integrator_init(geo["y0"], o)
+    t = 0.0
+    for _ in range(warmup):
+        t += dt_step
+        rc, _, _ = orc.integrate(t)
+        if rc != 0:
+            raise RuntimeError(f"oracle integrate rc={rc}")
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        t += dt_step
+        rc, _, _ = orc.integrate(t)
+        if rc != 0:
+            raise RuntimeError(f"oracle integrate rc={rc}")
+    el = time.perf_counter() - t0
+    return steps * dt_step / el, used, el, orc.stats()
+
+
+def cpu_baseline(args):
+    threads = os.cpu_count() or 1
+    val, used, el, st = cpu_oracle_run(args.cpu_dt, args.cpu_steps, 1, threads)
+    return {"value": val, "unit": UNIT, "cores": used, "kind": "port",
+            "sample": f"same 1536x512+open-demag workload, {args.cpu_steps} output steps of {args.cpu_dt} "
+                      f"sim-time after 1 warm-up step from t=0 ({el:.1f} s CPU wall, {st['nst']} BDF steps total); "
+                      "C FP64 restatement of the reference path with OpenMP",
+            "cpu_model": cpu_model()}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    dt = args.cpu_dt
+    val, used, el, st = cpu_oracle_run(dt, args.steps, args.warmup, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry/IC builders)",
+        "config": {"workload": "1536x512 cells, square hole, open FFT demag strength 4, rtol 1e-4, SPGMR(5)+BJ",
+                   "sim_time_per_step": dt},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": used, "kind": "port",
+                         "sample": f"{args.steps} steps of {dt} sim-time after {args.warmup} warm-up steps from t=0; "
+                                   "CPU FP64 restatement of the reference path (SUNDIALS absent, so the reference "
+                                   "solver itself cannot be built)"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--dt", type=float, default=1.0)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-dt", type=float, default=0.02)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,782 @@
+// k_demag.cu — FFT demagnetising field for sm_100a, FP64.
+//
+// Reference chain (src/irregular/2d_fft/2d_i2/demag_fft.cu:325-363, windowed
+// 2d_i3/demag_fft.cu:371-419):  gather (× w) → cufftExecD2Z (batch 3) →
+// Ĥ_a = Σ_b N̂_ab M̂_b → cufftExecZ2D (batch 3) → FFT-shift, × strength/(nx·ny),
+// scatter to SoA.  Tensor: 81-point face average of the closed-form Newell
+// integrals (demag_fft.cu:27-91) computed once at init.
+//
+// Here the chain is three hand-written kernels and no library FFT:
+//   K1 rows_fwd : SoA y (× w) → real FFT along x of each data row (two real
+//                 rows packed into one complex transform) → spectrum S written
+//                 column-major [comp][kx][y] so K2 reads whole columns.
+//   K2 cols     : per x-frequency column, all three components: FFT along y
+//                 (zero-padded rows in open mode) → 3x3 tensor multiply →
+//                 inverse FFT along y → S (only the data rows are kept).
+//   K3 rows_inv : inverse real FFT along x → h, × strength/(Px·Py) folded into
+//                 the tensor, written SoA for the first ng columns only.
+// Every transform runs in shared memory as in-place mixed-radix DIT (digit-
+// reversed load) or DIF (digit-reversed store) passes, radices 8/4/2/3/5 and a
+// generic odd radix; HBM sees each element of y, S and h once per kernel.
+// The tensor is stored wrapped at displacement d mod P (d in [-P/2, P-1-P/2]),
+// which equals the reference's centring + output shift; the open-boundary
+// tensor has its unused d = -P/2 lines zeroed, so its spectra are real.  Only
+// xx, yy, zz (real) and xy = yx (complex) are kept: for the single-layer film
+// (field point in the mid-plane) the xz, yz, zx, zy integrals cancel; init
+// verifies this numerically and refuses the plan otherwise.
+#include <math.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "llg_internal.h"
+
+namespace {
+
+constexpr int MAXR = 24;  // passes
+
+struct FftPlan {
+  int n, nr;
+  int radix[MAXR];
+  const double2* tw;   // tw[k] = exp(-2 pi i k / n)
+  const int* revinv;   // natural index -> DIT position
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// multiply by -i*SIGN... : rot(v) = v * (SIGN < 0 ? -i : +i)
+template <int SIGN>
+__device__ __forceinline__ double2 rot90(double2 v) {
+  return (SIGN < 0) ? make_double2(v.y, -v.x) : make_double2(-v.y, v.x);
+}
+
+template <int SIGN>
+__device__ __forceinline__ double2 twid(const FftPlan& pl, int idx) {
+  double2 w = __ldg(&pl.tw[idx]);
+  if (SIGN > 0) w.y = -w.y;
+  return w;
+}
+
+// in-register DFTs, out[q] = sum_r v[r] exp(SIGN 2 pi i r q / R)
+template <int SIGN>
+__device__ __forceinline__ void dft2(double2* v) {
+  const double2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+template <int SIGN>
+__device__ __forceinline__ void dft4(double2* v) {
+  const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+  const double2 b0 = cadd(v[1], v[3]), b1 = rot90<SIGN>(csub(v[1], v[3]));
+  v[0] = cadd(a0, b0);
+  v[2] = csub(a0, b0);
+  v[1] = cadd(a1, b1);
+  v[3] = csub(a1, b1);
+}
+template <int SIGN>
+__device__ __forceinline__ void dft3(double2* v) {
+  const double c = -0.5, s = SIGN * 0.86602540378443864676;  // sin(2pi/3)
+  const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+  const double2 a = make_double2(v[0].x + c * t1.x, v[0].y + c * t1.y);
+  const double2 b = make_double2(-s * t2.y, s * t2.x);  // i*s*t2
+  v[0] = cadd(v[0], t1);
+  v[1] = cadd(a, b);
+  v[2] = csub(a, b);
+}
+template <int SIGN>
+__device__ __forceinline__ void dft5(double2* v) {
+  const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+  const double s1 = SIGN * 0.95105651629515357212, s2 = SIGN * 0.58778525229247312917;
+  const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+  const double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+  const double2 a1 = make_double2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+  const double2 a2 = make_double2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+  const double2 b1 = make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+  const double2 b2 = make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+  v[0] = make_double2(v[0].x + t1.x + t2.x, v[0].y + t1.y + t2.y);
+  // multiply b by i
+  v[1] = make_double2(a1.x - b1.y, a1.y + b1.x);
+  v[4] = make_double2(a1.x + b1.y, a1.y - b1.x);
+  v[2] = make_double2(a2.x - b2.y, a2.y + b2.x);
+  v[3] = make_double2(a2.x + b2.y, a2.y - b2.x);
+}
+template <int SIGN>
+__device__ __forceinline__ void dft8(double2* v) {
+  const double h = 0.70710678118654752440;
+  // radix-2 split: even / odd
+  double2 e[4] = {v[0], v[2], v[4], v[6]};
+  double2 o[4] = {v[1], v[3], v[5], v[7]};
+  dft4<SIGN>(e);
+  dft4<SIGN>(o);
+  // twiddles w8^k for k=0..3 (SIGN)
+  const double2 o1 = make_double2(h * (o[1].x - SIGN * o[1].y), h * (o[1].y + SIGN * o[1].x));
+  const double2 o2 = rot90<SIGN>(o[2]);
+  const double2 o3 = make_double2(-h * (o[3].x + SIGN * o[3].y), h * (SIGN * o[3].x - o[3].y));
+  v[0] = cadd(e[0], o[0]);
+  v[4] = csub(e[0], o[0]);
+  v[1] = cadd(e[1], o1);
+  v[5] = csub(e[1], o1);
+  v[2] = cadd(e[2], o2);
+  v[6] = csub(e[2], o2);
+  v[3] = cadd(e[3], o3);
+  v[7] = csub(e[3], o3);
+}
+
+template <int R, int SIGN>
+__device__ __forceinline__ void dft_fixed(double2* v) {
+  if constexpr (R == 2) dft2<SIGN>(v);
+  else if constexpr (R == 3) dft3<SIGN>(v);
+  else if constexpr (R == 4) dft4<SIGN>(v);
+  else if constexpr (R == 5) dft5<SIGN>(v);
+  else if constexpr (R == 8) dft8<SIGN>(v);
+}
+
+// one pass over all butterflies of nbatch transforms held in buf
+template <int R, int SIGN, bool DIF>
+__device__ __forceinline__ void pass_fixed(double2* buf, int nbatch, const FftPlan& pl, int S) {
+  const int nb = pl.n / R;
+  const int total = nb * nbatch;
+  const int tstride = pl.n / (S * R);
+  for (int bf = threadIdx.x; bf < total; bf += blockDim.x) {
+    const int b = bf / nb, k = bf - b * nb;
+    const int g = k / S, j = k - g * S;
+    double2* base = buf + b * pl.n + g * S * R + j;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = base[r * S];
+    if (!DIF) {
+#pragma unroll
+      for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<SIGN>(pl, j * r * tstride));
+    }
+    dft_fixed<R, SIGN>(v);
+    if (DIF) {
+#pragma unroll
+      for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<SIGN>(pl, j * r * tstride));
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) base[r * S] = v[r];
+  }
+}
+
+// generic odd radix (small primes beyond 5), O(R^2), registers spill to local
+template <int SIGN, bool DIF>
+__device__ void pass_generic(double2* buf, int nbatch, const FftPlan& pl, int S, int R) {
+  const int nb = pl.n / R;
+  const int total = nb * nbatch;
+  const int tstride = pl.n / (S * R);
+  const int rstride = pl.n / R;
+  for (int bf = threadIdx.x; bf < total; bf += blockDim.x) {
+    const int b = bf / nb, k = bf - b * nb;
+    const int g = k / S, j = k - g * S;
+    double2* base = buf + b * pl.n + g * S * R + j;
+    double2 v[64], o[64];
+    for (int r = 0; r < R; r++) {
+      v[r] = base[r * S];
+      if (!DIF && r > 0) v[r] = cmul(v[r], twid<SIGN>(pl, j * r * tstride));
+    }
+    for (int q = 0; q < R; q++) {
+      double2 acc = v[0];
+      for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid<SIGN>(pl, ((r * q) % R) * rstride)));
+      o[q] = acc;
+    }
+    for (int q = 0; q < R; q++) {
+      double2 w = o[q];
+      if (DIF && q > 0) w = cmul(w, twid<SIGN>(pl, j * q * tstride));
+      base[q * S] = w;
+    }
+  }
+}
+
+template <int SIGN, bool DIF>
+__device__ __forceinline__ void run_pass(double2* buf, int nbatch, const FftPlan& pl, int S, int R) {
+  switch (R) {
+    case 2: pass_fixed<2, SIGN, DIF>(buf, nbatch, pl, S); break;
+    case 3: pass_fixed<3, SIGN, DIF>(buf, nbatch, pl, S); break;
+    case 4: pass_fixed<4, SIGN, DIF>(buf, nbatch, pl, S); break;
+    case 5: pass_fixed<5, SIGN, DIF>(buf, nbatch, pl, S); break;
+    case 8: pass_fixed<8, SIGN, DIF>(buf, nbatch, pl, S); break;
+    default: pass_generic<SIGN, DIF>(buf, nbatch, pl, S, R); break;
+  }
+}
+
+// natural-order output from digit-reversed input
+template <int SIGN>
+__device__ void fft_dit(double2* buf, int nbatch, const FftPlan& pl) {
+  int S = 1;
+  for (int p = 0; p < pl.nr; p++) {
+    const int R = pl.radix[p];
+    run_pass<SIGN, false>(buf, nbatch, pl, S, R);
+    __syncthreads();
+    S *= R;
+  }
+}
+// digit-reversed output from natural-order input
+template <int SIGN>
+__device__ void fft_dif(double2* buf, int nbatch, const FftPlan& pl) {
+  int S = pl.n;
+  for (int p = pl.nr - 1; p >= 0; p--) {
+    const int R = pl.radix[p];
+    S /= R;
+    run_pass<SIGN, true>(buf, nbatch, pl, S, R);
+    __syncthreads();
+  }
+}
+
+// ── K1: forward real transform of data rows along x ─────────────────────
+// CTA = (component c, group of 2*NB rows); NB complex transforms of length n.
+// in: comp c row r at in + c*comp_stride + r*row_len, valid i < row_len.
+template <int NB>
+__global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long comp_stride, int row_len,
+                           int nrows, const double* __restrict__ w, double2* __restrict__ S, int ld,
+                           int Hx) {
+  extern __shared__ double2 sm[];
+  const int c = blockIdx.y;
+  const int y0 = blockIdx.x * (2 * NB);
+  const int n = pl.n;
+  const double* src = in + (long long)c * comp_stride;
+  for (int e = threadIdx.x; e < NB * n; e += blockDim.x) {
+    const int b = e / n, i = e - b * n;
+    const int ya = y0 + 2 * b, yb = ya + 1;
+    double va = 0.0, vb = 0.0;
+    if (i < row_len) {
+      if (ya < nrows) {
+        const long long q = (long long)ya * row_len + i;
+        va = src[q] * (w ? w[q] : 1.0);
+      }
+      if (yb < nrows) {
+        const long long q = (long long)yb * row_len + i;
+        vb = src[q] * (w ? w[q] : 1.0);
+      }
+    }
+    sm[b * n + pl.revinv[i]] = make_double2(va, vb);
+  }
+  __syncthreads();
+  fft_dit<-1>(sm, NB, pl);
+  // split the packed spectrum into the two real rows' half spectra
+  for (int e = threadIdx.x; e < Hx * 2 * NB; e += blockDim.x) {
+    const int kx = e / (2 * NB), r = e - kx * (2 * NB);
+    const int b = r >> 1, which = r & 1;
+    const int y = y0 + r;
+    if (y >= nrows) continue;
+    const double2 zk = sm[b * n + kx];
+    const double2 zm = sm[b * n + ((n - kx) % n)];
+    double2 out;
+    if (!which) out = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+    else out = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+    S[((long long)c * Hx + kx) * ld + y] = out;
+  }
+}
+
+// ── K2: column transform + tensor multiply + inverse column transform ─────
+__global__ void k_cols_conv(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx,
+                            const double* __restrict__ txx, const double* __restrict__ tyy,
+                            const double* __restrict__ tzz, const double2* __restrict__ txy) {
+  extern __shared__ double2 sm[];
+  const int kx = blockIdx.x;
+  const int n = pl.n;
+  for (int e = threadIdx.x; e < 3 * n; e += blockDim.x) {
+    const int c = e / n, yy = e - c * n;
+    double2 v = make_double2(0.0, 0.0);
+    if (yy < nrows) v = S[((long long)c * Hx + kx) * ld + yy];
+    sm[c * n + pl.revinv[yy]] = v;
+  }
+  __syncthreads();
+  fft_dit<-1>(sm, 3, pl);
+  const long long tb = (long long)kx * n;
+  for (int ky = threadIdx.x; ky < n; ky += blockDim.x) {
+    const double2 mx = sm[ky], my = sm[n + ky], mz = sm[2 * n + ky];
+    const double a = __ldg(&txx[tb + ky]), b = __ldg(&tyy[tb + ky]), d = __ldg(&tzz[tb + ky]);
+    const double2 xy = __ldg(&txy[tb + ky]);
+    const double2 hxy = cmul(xy, my), hyx = cmul(xy, mx);
+    sm[ky] = make_double2(a * mx.x + hxy.x, a * mx.y + hxy.y);
+    sm[n + ky] = make_double2(hyx.x + b * my.x, hyx.y + b * my.y);
+    sm[2 * n + ky] = make_double2(d * mz.x, d * mz.y);
+  }
+  __syncthreads();
+  fft_dif<+1>(sm, 3, pl);
+  for (int e = threadIdx.x; e < 3 * nrows; e += blockDim.x) {
+    const int c = e / nrows, yy = e - c * nrows;
+    S[((long long)c * Hx + kx) * ld + yy] = sm[c * n + pl.revinv[yy]];
+  }
+}
+
+// forward column transform only (tensor spectra at init)
+__global__ void k_cols_fwd(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx) {
+  extern __shared__ double2 sm[];
+  const int kx = blockIdx.x;
+  const int n = pl.n;
+  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) {
+    double2 v = make_double2(0.0, 0.0);
+    if (yy < nrows) v = S[(long long)kx * ld + yy];
+    sm[pl.revinv[yy]] = v;
+  }
+  __syncthreads();
+  fft_dit<-1>(sm, 1, pl);
+  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) S[(long long)kx * ld + yy] = sm[yy];
+}
+
+// ── K3: inverse real transform along x, scatter to SoA h ─────────────────
+template <int NB>
+__global__ void k_rows_inv(FftPlan pl, const double2* __restrict__ S, int ld, int nrows, int Hx,
+                           double* __restrict__ h, long long comp_stride, int ng) {
+  extern __shared__ double2 sm[];
+  const int c = blockIdx.y;
+  const int y0 = blockIdx.x * (2 * NB);
+  const int n = pl.n;
+  const bool even = (n % 2) == 0;
+  for (int e = threadIdx.x; e < n * 2 * NB; e += blockDim.x) {
+    const int k = e / (2 * NB), r = e - k * (2 * NB);
+    if (r & 1) continue;  // one thread builds both rows of a packed pair
+    const int b = r >> 1;
+    const int ya = y0 + 2 * b, yb = ya + 1;
+    const int kk = (k < Hx) ? k : n - k;
+    double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+    if (ya < nrows) A = S[((long long)c * Hx + kk) * ld + ya];
+    if (yb < nrows) B = S[((long long)c * Hx + kk) * ld + yb];
+    if (kk == 0 || (even && kk == n / 2)) { A.y = 0.0; B.y = 0.0; }
+    if (k >= Hx) { A.y = -A.y; B.y = -B.y; }
+    sm[b * n + pl.revinv[k]] = make_double2(A.x - B.y, A.y + B.x);
+  }
+  __syncthreads();
+  fft_dit<+1>(sm, NB, pl);
+  double* dst = h + (long long)c * comp_stride;
+  for (int e = threadIdx.x; e < NB * 2 * ng; e += blockDim.x) {
+    const int r = e / ng, i = e - r * ng;
+    const int y = y0 + r;
+    if (y >= nrows) continue;
+    const double2 z = sm[(r >> 1) * n + i];
+    dst[(long long)y * ng + i] = (r & 1) ? z.y : z.x;
+  }
+}
+
+// ── Newell tensor (81-point average of the closed-form integrals) ────────
+// Same term grouping as the reference's ctt/calt (demag_fft.cu:27-91).
+__device__ void newell_point(double thick, double sx, double sy, double out[9]) {
+  const double a = 0.49999, bb = 0.5 * thick, sz = 0.0;
+  const double X[2] = {sx - a, sx + a};
+  const double Y[2] = {sy - a, sy + a};
+  const double Z[2] = {sz - bb, sz + bb};
+  double r[2][2][2];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int k = 0; k < 2; k++) r[i][j][k] = sqrt(X[i] * X[i] + Y[j] * Y[j] + Z[k] * Z[k]);
+  double xx = 0.0, yy = 0.0, zz = 0.0;
+  bool first = true;
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const double tm = atan(Z[k] * Y[j] / (X[i] * r[i][j][k]));
+        const double sg = ((i + j + k) & 1) ? -1.0 : 1.0;
+        xx = first ? tm : xx + sg * tm;
+        first = false;
+      }
+  first = true;
+#pragma unroll
+  for (int j = 0; j < 2; j++)
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const double tm = atan(Z[k] * X[i] / (Y[j] * r[i][j][k]));
+        const double sg = ((i + j + k) & 1) ? -1.0 : 1.0;
+        yy = first ? tm : yy + sg * tm;
+        first = false;
+      }
+  first = true;
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const double tm = atan(X[i] * Y[j] / (Z[k] * r[i][j][k]));
+        const double sg = ((i + j + k) & 1) ? -1.0 : 1.0;
+        zz = first ? tm : zz + sg * tm;
+        first = false;
+      }
+#define LZ(i, j) log((r[i][j][0] - Z[0]) / (r[i][j][1] - Z[1]))
+#define LY(i, k) log((r[i][0][k] - Y[0]) / (r[i][1][k] - Y[1]))
+#define LX(j, k) log((r[0][j][k] - X[0]) / (r[1][j][k] - X[1]))
+  out[0] = xx;
+  out[1] = LZ(0, 0) - LZ(1, 0) - LZ(0, 1) + LZ(1, 1);
+  out[2] = LY(0, 0) - LY(1, 0) - LY(0, 1) + LY(1, 1);
+  out[3] = LZ(0, 0) - LZ(0, 1) - LZ(1, 0) + LZ(1, 1);
+  out[4] = yy;
+  out[5] = LX(0, 0) - LX(1, 0) - LX(0, 1) + LX(1, 1);
+  out[6] = LY(0, 0) - LY(0, 1) - LY(1, 0) + LY(1, 1);
+  out[7] = LX(0, 0) - LX(0, 1) - LX(1, 0) + LX(1, 1);
+  out[8] = zz;
+#undef LZ
+#undef LY
+#undef LX
+}
+
+__device__ __forceinline__ int rep_disp(int i, int n) {
+  const int hi = n - 1 - n / 2;
+  return (i <= hi) ? i : i - n;
+}
+
+// T[c][j*px + i] for c < 9; open: the d = -P/2 lines are zeroed (never used
+// by the zero-padded linear convolution).
+__global__ void k_newell(double* __restrict__ T, int px, int py, double thick, int open) {
+  const long long np = (long long)px * py;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < np;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % px), j = (int)(e / px);
+    double acc[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) acc[c] = 0.0;
+    const bool dead = open && (i == px / 2 || j == py / 2);
+    if (!dead) {
+      const int dx = rep_disp(i, px), dy = rep_disp(j, py);
+      double dm[9];
+      for (int jy = -4; jy <= 4; jy++) {
+        const double sy = (double)dy + 0.1 * (double)jy;
+        for (int ix = -4; ix <= 4; ix++) {
+          const double sx = (double)dx + 0.1 * (double)ix;
+          newell_point(thick, sx, sy, dm);
+#pragma unroll
+          for (int c = 0; c < 9; c++) acc[c] += dm[c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 9; c++) acc[c] = acc[c] / 81.;
+    }
+#pragma unroll
+    for (int c = 0; c < 9; c++) T[c * np + e] = acc[c];
+  }
+}
+
+// spectra: out arrays [kx*Py + ky]; S_c holds component c's spectrum (col-major, ld = Py)
+__global__ void k_tensor_finish(const double2* __restrict__ Sxx, const double2* __restrict__ Syy,
+                                const double2* __restrict__ Szz, const double2* __restrict__ Sxy,
+                                const double2* __restrict__ Syx, const double2* __restrict__ Sxz,
+                                const double2* __restrict__ Syz, const double2* __restrict__ Szx,
+                                const double2* __restrict__ Szy, long long total, double scale,
+                                double* __restrict__ txx, double* __restrict__ tyy, double* __restrict__ tzz,
+                                double2* __restrict__ txy, double* __restrict__ stats) {
+  // stats (per block partial max): [0] max|diag|, [1] max imag diag, [2] max |xz family|, [3] max |xy-yx|
+  __shared__ double red[4][256];
+  double m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double2 a = Sxx[e], b = Syy[e], d = Szz[e], p = Sxy[e], q = Syx[e];
+    m0 = fmax(m0, fmax(fabs(a.x), fmax(fabs(b.x), fabs(d.x))));
+    m1 = fmax(m1, fmax(fabs(a.y), fmax(fabs(b.y), fabs(d.y))));
+    const double2 u = Sxz[e], v = Syz[e], s = Szx[e], t = Szy[e];
+    m2 = fmax(m2, fmax(fmax(fabs(u.x), fabs(u.y)), fmax(fabs(v.x), fabs(v.y))));
+    m2 = fmax(m2, fmax(fmax(fabs(s.x), fabs(s.y)), fmax(fabs(t.x), fabs(t.y))));
+    m3 = fmax(m3, fmax(fabs(p.x - q.x), fabs(p.y - q.y)));
+    txx[e] = a.x * scale;
+    tyy[e] = b.x * scale;
+    tzz[e] = d.x * scale;
+    txy[e] = make_double2(0.5 * (p.x + q.x) * scale, 0.5 * (p.y + q.y) * scale);
+  }
+  red[0][threadIdx.x] = m0; red[1][threadIdx.x] = m1; red[2][threadIdx.x] = m2; red[3][threadIdx.x] = m3;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 4; k++) red[k][threadIdx.x] = fmax(red[k][threadIdx.x], red[k][threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) stats[blockIdx.x * 4 + k] = red[k][0];
+}
+
+}  // namespace
+
+// ── host side ───────────────────────────────────────────────────────────
+struct HostFft {
+  int n = 0;
+  std::vector<int> radix;
+  double2* d_tw = nullptr;
+  int* d_revinv = nullptr;
+  FftPlan dev() const {
+    FftPlan p{};
+    p.n = n;
+    p.nr = (int)radix.size();
+    for (int i = 0; i < p.nr; i++) p.radix[i] = radix[i];
+    p.tw = d_tw;
+    p.revinv = d_revinv;
+    return p;
+  }
+};
+
+struct DemagPlan {
+  int px = 0, py = 0, hx = 0, ng = 0, ny = 0;
+  int open = 0;
+  double strength = 0.0;
+  double n0[3] = {0, 0, 0};      // unscaled N(0)
+  HostFft fx, fy;
+  double2* d_S = nullptr;        // 3*hx*ny
+  double* d_txx = nullptr;
+  double* d_tyy = nullptr;
+  double* d_tzz = nullptr;
+  double2* d_txy = nullptr;
+  double* d_T = nullptr;         // 9 real tensor components (kept for host queries)
+  size_t smem_rows = 0, smem_cols = 0;
+};
+
+static int factorize(int n, std::vector<int>& rad) {
+  rad.clear();
+  int m = n;
+  while (m % 8 == 0) { rad.push_back(8); m /= 8; }
+  while (m % 4 == 0) { rad.push_back(4); m /= 4; }
+  while (m % 2 == 0) { rad.push_back(2); m /= 2; }
+  while (m % 3 == 0) { rad.push_back(3); m /= 3; }
+  while (m % 5 == 0) { rad.push_back(5); m /= 5; }
+  for (int p = 7; m > 1; p += 2) {
+    while (m % p == 0) {
+      if (p > 64) return -1;
+      rad.push_back(p);
+      m /= p;
+    }
+    if (p * p > m && m > 1) {
+      if (m > 64) return -1;
+      rad.push_back(m);
+      m = 1;
+    }
+  }
+  if ((int)rad.size() > MAXR) return -1;
+  if (rad.empty()) rad.push_back(1);
+  return 0;
+}
+
+static int fft_init(HostFft& f, int n) {
+  f.n = n;
+  if (factorize(n, f.radix) != 0) {
+    llg_set_error("FFT length " + std::to_string(n) + " has a prime factor > 64");
+    return LLG_ERR_NOTSUP;
+  }
+  if (f.radix.size() == 1 && f.radix[0] == 1) f.radix.clear();
+  std::vector<double2> tw(n);
+  for (int k = 0; k < n; k++) {
+    // exp(-2 pi i k/n) using octant-reduced arguments for accuracy
+    const long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+    tw[k] = make_double2((double)cosl(ang), (double)-sinl(ang));
+  }
+  // digit reversal: position p (digits r_1.. LSD first, radices in pass order)
+  std::vector<int> revinv(n);
+  const int k = (int)f.radix.size();
+  for (int p = 0; p < n; p++) {
+    int rem = p;
+    std::vector<int> dig(k);
+    for (int s = 0; s < k; s++) { dig[s] = rem % f.radix[s]; rem /= f.radix[s]; }
+    int x = 0;
+    for (int s = 0; s < k; s++) x = x * f.radix[s] + dig[s];
+    // x = r_k + R_k (r_{k-1} + ...): build from MSD = r_1
+    revinv[x] = p;
+  }
+  LLG_CUDA_TRY(cudaMalloc(&f.d_tw, sizeof(double2) * n));
+  LLG_CUDA_TRY(cudaMalloc(&f.d_revinv, sizeof(int) * n));
+  LLG_CUDA_TRY(cudaMemcpy(f.d_tw, tw.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+  LLG_CUDA_TRY(cudaMemcpy(f.d_revinv, revinv.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static void fft_free(HostFft& f) {
+  cudaFree(f.d_tw);
+  cudaFree(f.d_revinv);
+  f.d_tw = nullptr;
+  f.d_revinv = nullptr;
+}
+
+static constexpr int kRowsNB = 2;     // complex transforms per row-CTA (4 real rows)
+static constexpr int kRowThreads = 256;
+static constexpr int kColThreads = 256;
+
+void demag_destroy(DemagPlan* d) {
+  if (!d) return;
+  fft_free(d->fx);
+  fft_free(d->fy);
+  cudaFree(d->d_S);
+  cudaFree(d->d_txx);
+  cudaFree(d->d_tyy);
+  cudaFree(d->d_tzz);
+  cudaFree(d->d_txy);
+  cudaFree(d->d_T);
+  delete d;
+}
+
+static int set_smem(const void* fn, size_t bytes) {
+  if (bytes > 48 * 1024) {
+    LLG_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  }
+  return 0;
+}
+
+int demag_create(llg_ctx* c) {
+  const llg_params& p = c->p;
+  DemagPlan* d = new DemagPlan();
+  d->ng = p.ng;
+  d->ny = p.ny;
+  d->open = (p.demag_mode == LLG_DEMAG_OPEN);
+  d->px = d->open ? 2 * p.ng : p.ng;
+  d->py = d->open ? 2 * p.ny : p.ny;
+  d->hx = d->px / 2 + 1;
+  d->strength = p.demag_strength;
+  int rc = fft_init(d->fx, d->px);
+  if (!rc) rc = fft_init(d->fy, d->py);
+  if (rc) { demag_destroy(d); return rc; }
+  d->smem_rows = sizeof(double2) * (size_t)kRowsNB * d->px;
+  d->smem_cols = sizeof(double2) * 3 * (size_t)d->py;
+  if (d->smem_rows > 227 * 1024 || d->smem_cols > 227 * 1024) {
+    llg_set_error("demag grid too large for the shared-memory transform");
+    demag_destroy(d);
+    return LLG_ERR_NOTSUP;
+  }
+  if ((rc = set_smem((const void*)k_rows_fwd<kRowsNB>, d->smem_rows)) ||
+      (rc = set_smem((const void*)k_rows_inv<kRowsNB>, d->smem_rows)) ||
+      (rc = set_smem((const void*)k_cols_conv, d->smem_cols)) ||
+      (rc = set_smem((const void*)k_cols_fwd, sizeof(double2) * (size_t)d->py))) {
+    demag_destroy(d);
+    return rc;
+  }
+  const long long np = (long long)d->px * d->py;
+  const long long nspec = (long long)d->hx * d->py;
+  LLG_CUDA_TRY(cudaMalloc(&d->d_S, sizeof(double2) * 3 * (size_t)d->hx * d->ny));
+  LLG_CUDA_TRY(cudaMalloc(&d->d_txx, sizeof(double) * nspec));
+  LLG_CUDA_TRY(cudaMalloc(&d->d_tyy, sizeof(double) * nspec));
+  LLG_CUDA_TRY(cudaMalloc(&d->d_tzz, sizeof(double) * nspec));
+  LLG_CUDA_TRY(cudaMalloc(&d->d_txy, sizeof(double2) * nspec));
+  LLG_CUDA_TRY(cudaMalloc(&d->d_T, sizeof(double) * 9 * np));
+
+  cudaStream_t s = c->stream;
+  k_newell<<<c->num_sms * 8, 128, 0, s>>>(d->d_T, d->px, d->py, p.demag_thick, d->open);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  // N(0) (wrapped index 0)
+  double n0[9];
+  for (int k = 0; k < 9; k++)
+    LLG_CUDA_TRY(cudaMemcpyAsync(&n0[k], d->d_T + k * np, sizeof(double), cudaMemcpyDeviceToHost, s));
+  LLG_CUDA_TRY(cudaStreamSynchronize(s));
+  d->n0[0] = n0[0];
+  d->n0[1] = n0[4];
+  d->n0[2] = n0[8];
+
+  // spectra of all 9 components (real 2-D FFT: rows then columns)
+  double2* spec = nullptr;
+  LLG_CUDA_TRY(cudaMalloc(&spec, sizeof(double2) * 9 * (size_t)nspec));
+  const FftPlan fxp = d->fx.dev(), fyp = d->fy.dev();
+  for (int k = 0; k < 9; k++) {
+    dim3 g1((d->py + 2 * kRowsNB - 1) / (2 * kRowsNB), 1);
+    k_rows_fwd<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, d->d_T + k * np, 0, d->px, d->py, nullptr,
+                                                              spec + k * nspec, d->py, d->hx);
+    LLG_CUDA_TRY(cudaPeekAtLastError());
+    k_cols_fwd<<<d->hx, kColThreads, sizeof(double2) * d->py, s>>>(fyp, spec + k * nspec, d->py, d->py, d->hx);
+    LLG_CUDA_TRY(cudaPeekAtLastError());
+  }
+  const int nblk = 256;
+  double* d_stats = nullptr;
+  LLG_CUDA_TRY(cudaMalloc(&d_stats, sizeof(double) * 4 * nblk));
+  const double scale = d->strength / (double)np;
+  k_tensor_finish<<<nblk, 256, 0, s>>>(spec + 0 * nspec, spec + 4 * nspec, spec + 8 * nspec, spec + 1 * nspec,
+                                       spec + 3 * nspec, spec + 2 * nspec, spec + 5 * nspec, spec + 6 * nspec,
+                                       spec + 7 * nspec, nspec, scale, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy,
+                                       d_stats);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  std::vector<double> st(4 * nblk);
+  LLG_CUDA_TRY(cudaMemcpyAsync(st.data(), d_stats, sizeof(double) * 4 * nblk, cudaMemcpyDeviceToHost, s));
+  LLG_CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(d_stats);
+  cudaFree(spec);
+  double mx[4] = {0, 0, 0, 0};
+  for (int b = 0; b < nblk; b++)
+    for (int k = 0; k < 4; k++) mx[k] = std::max(mx[k], st[4 * b + k]);
+  const double tol = 1e-10 * std::max(mx[0], 1e-300);
+  if (mx[1] > tol || mx[2] > tol || mx[3] > tol) {
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "demag tensor outside the film form: max|diag|=%.3e imag(diag)=%.3e |xz..|=%.3e |xy-yx|=%.3e", mx[0],
+             mx[1], mx[2], mx[3]);
+    llg_set_error(buf);
+    c->demag = d;
+    return LLG_ERR_NOTSUP;
+  }
+  c->demag = d;
+  return 0;
+}
+
+int demag_apply(llg_ctx* c, const double* y, double* h) {
+  return demag_apply_w(c, y, c->p.windowed ? c->d_w : nullptr, h);
+}
+
+int demag_apply_w(llg_ctx* c, const double* y, const double* w, double* h) {
+  DemagPlan* d = c->demag;
+  if (!d) {
+    LLG_CUDA_TRY(cudaMemsetAsync(h, 0, sizeof(double) * 3 * (size_t)c->ncell, c->stream));
+    return 0;
+  }
+  cudaStream_t s = c->stream;
+  const FftPlan fxp = d->fx.dev(), fyp = d->fy.dev();
+  dim3 g1((d->ny + 2 * kRowsNB - 1) / (2 * kRowsNB), 3);
+  LLG_COUNT(KID_DEMAG_ROWS_FWD);
+  k_rows_fwd<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, y, (long long)c->ncell, d->ng, d->ny, w, d->d_S,
+                                                            d->ny, d->hx);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  LLG_COUNT(KID_DEMAG_COLS);
+  k_cols_conv<<<d->hx, kColThreads, d->smem_cols, s>>>(fyp, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy,
+                                                       d->d_tzz, d->d_txy);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  LLG_COUNT(KID_DEMAG_ROWS_INV);
+  k_rows_inv<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, d->d_S, d->ny, d->ny, d->hx, h,
+                                                            (long long)c->ncell, d->ng);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+// one stage of the chain alone (profiling): 0 rows_fwd, 1 cols_conv, 2 rows_inv
+int demag_stage(llg_ctx* c, int stage, const double* y, double* h) {
+  DemagPlan* d = c->demag;
+  if (!d) return LLG_ERR_STATE;
+  cudaStream_t s = c->stream;
+  const FftPlan fxp = d->fx.dev(), fyp = d->fy.dev();
+  dim3 g1((d->ny + 2 * kRowsNB - 1) / (2 * kRowsNB), 3);
+  if (stage == 0) {
+    LLG_COUNT(KID_DEMAG_ROWS_FWD);
+    k_rows_fwd<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, y, (long long)c->ncell, d->ng, d->ny,
+                                                              c->p.windowed ? c->d_w : nullptr, d->d_S, d->ny, d->hx);
+  } else if (stage == 1) {
+    LLG_COUNT(KID_DEMAG_COLS);
+    k_cols_conv<<<d->hx, kColThreads, d->smem_cols, s>>>(fyp, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy,
+                                                         d->d_tzz, d->d_txy);
+  } else {
+    LLG_COUNT(KID_DEMAG_ROWS_INV);
+    k_rows_inv<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, d->d_S, d->ny, d->ny, d->hx, h,
+                                                              (long long)c->ncell, d->ng);
+  }
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int demag_dims(llg_ctx* c, int out[4]) {
+  DemagPlan* d = c->demag;
+  if (!d) return LLG_ERR_STATE;
+  out[0] = d->px; out[1] = d->py; out[2] = d->hx; out[3] = d->ny;
+  return 0;
+}
+
+int demag_self(llg_ctx* c, double out3[3]) {
+  if (!c->demag) { out3[0] = out3[1] = out3[2] = 0.0; return 0; }
+  for (int a = 0; a < 3; a++) out3[a] = c->demag->n0[a] * c->demag->strength;
+  return 0;
+}
+
+int demag_tensor_host(llg_ctx* c, int comp, int dx, int dy, double* out) {
+  DemagPlan* d = c->demag;
+  if (!d || comp < 0 || comp > 8) { *out = 0.0; return d ? LLG_ERR_ARG : 0; }
+  const int wx = ((dx % d->px) + d->px) % d->px, wy = ((dy % d->py) + d->py) % d->py;
+  const long long np = (long long)d->px * d->py;
+  LLG_CUDA_TRY(cudaMemcpy(out, d->d_T + comp * np + (long long)wy * d->px + wx, sizeof(double),
+                          cudaMemcpyDeviceToHost));
+  return 0;
+}

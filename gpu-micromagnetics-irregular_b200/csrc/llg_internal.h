@@ -1,0 +1,150 @@
+// llg_internal.h — shared declarations of libllg.so (B200 / sm_100a).
+//
+// HBM layout of one problem instance (ncell = ng*ny, FP64 unless noted):
+//   y, ydot, Jv, z, Krylov vectors   3*ncell   SoA [mx|my|mz]
+//   act                               ncell     uint8, 1 active / 0 hole (EXEC_YMSK)
+//   active_ids / inactive_ids         int32 lists (EXEC_COMPACT)
+//   w                                 ncell     window (polycrystal only)
+//   msk3 / nsk3                       3*ncell   per-cell axes (polycrystal only)
+//   hd                                3*ncell   demag field of the last RHS
+//   pm, ph                            3*ncell   m and h frozen at the last psetup;
+//                                               psolve rebuilds each 3x3 block from
+//                                               them (48 B/cell instead of 72 B of P^-1)
+//   spec                              3*Hx*ny   complex row spectra, column-major
+//                                               (x-frequency outer, y inner)
+//   tensor spectra                    Hx*Py     xx, yy, zz real + xy complex, scaled
+//                                               by strength/(Px*Py)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/llg.h"
+
+#define LLG_CUDA_TRY(expr)                                                   \
+  do {                                                                       \
+    cudaError_t _e = (expr);                                                 \
+    if (_e != cudaSuccess) {                                                 \
+      llg_set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));     \
+      return LLG_ERR_CUDA;                                                   \
+    }                                                                        \
+  } while (0)
+
+void llg_set_error(const std::string& msg);
+
+// Launch accounting (host counters, one per kernel family), read by
+// llg_kernel_counts; every launch site bumps exactly one counter.
+enum LlgKernel {
+  KID_RHS = 0, KID_JTV, KID_ARNOLDI, KID_PSETUP, KID_PSOLVE, KID_NORM,
+  KID_DEMAG_ROWS_FWD, KID_DEMAG_COLS, KID_DEMAG_ROWS_INV, KID_REDUCE, KID_ELEMWISE,
+  KID_LEARNED, KID_OTHER, KID_COUNT
+};
+extern long long g_kcount[KID_COUNT];
+#define LLG_COUNT(k) (g_kcount[(k)]++)
+
+// Physics + geometry view passed by value to every per-cell kernel.
+struct DevProblem {
+  int ng, ny;
+  int ncell;
+  int bc;          // LLG_BC_*
+  int aniso;       // LLG_ANISO_*
+  int windowed;    // 0/1
+  int jv_full;     // 1: Jv field includes hd + happ
+  double che, chk, cha, chb, alpha, chg;
+  double msk[3], nsk[3], happ[3];
+  double n0[3];    // strength-scaled N(0) diagonal
+  const uint8_t* act;    // nullptr: all active
+  const double* w;       // windowed
+  const double* msk3;    // windowed
+  const double* nsk3;    // windowed
+};
+
+struct DemagPlan;   // k_demag.cu
+struct Integrator;  // integrator.cu
+struct Learned;     // k_learned.cu
+
+struct llg_ctx {
+  llg_params p{};
+  DevProblem dp{};
+  int ncell = 0;
+  long long neq = 0;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int num_sms = 148;
+
+  // geometry
+  uint8_t* d_act = nullptr;
+  int32_t* d_active_ids = nullptr;
+  int32_t* d_inactive_ids = nullptr;
+  int n_active = 0, n_inactive = 0;
+  double* d_w = nullptr;
+  double* d_msk3 = nullptr;
+  double* d_nsk3 = nullptr;
+
+  // fields
+  double* d_hd = nullptr;    // demag field of the last RHS (3N)
+  double* d_pm = nullptr;    // m at the last psetup (3N)
+  double* d_ph = nullptr;    // h at the last psetup (3N)
+  double gamma_setup = 0.0;
+  int have_setup = 0;
+
+  // reductions
+  double* d_red = nullptr;      // partial sums scratch
+  double* d_scal = nullptr;     // scalar results (device)
+  unsigned int* d_counter = nullptr;
+  double* h_scal = nullptr;     // pinned host mirror
+  int red_blocks_max = 0;
+
+  DemagPlan* demag = nullptr;
+  Integrator* integ = nullptr;
+  Learned* learned = nullptr;
+  long long nfe_demag = 0;
+};
+
+// ── physics kernels (k_physics.cu) ─────────────────────────────────────
+int launch_normalize(llg_ctx* c, double* y);
+int launch_rhs(llg_ctx* c, const double* y, const double* hd, double* ydot);
+int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y);
+int launch_psetup(llg_ctx* c, const double* y, double gamma);
+int launch_psolve(llg_ctx* c, const double* r, double* z);
+// fused Arnoldi operator:  out = s1 ⊙ P^-1 ( vt − γ J vt ),  vt = in / s2
+int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out,
+                      const double* y, double gamma);
+int rhs_full(llg_ctx* c, double t, double* y, double* ydot);
+
+// ── demag (k_demag.cu) ─────────────────────────────────────────────────
+int demag_create(llg_ctx* c);
+void demag_destroy(DemagPlan* d);
+int demag_apply(llg_ctx* c, const double* y, double* h);
+int demag_apply_w(llg_ctx* c, const double* y, const double* w, double* h);
+int demag_self(llg_ctx* c, double out3[3]);
+int demag_stage(llg_ctx* c, int stage, const double* y, double* h);
+int demag_dims(llg_ctx* c, int out[4]);
+int demag_tensor_host(llg_ctx* c, int comp, int dx, int dy, double* out);
+
+// ── vector ops (k_vector.cu) ───────────────────────────────────────────
+int reductions_init(llg_ctx* c);
+void reductions_free(llg_ctx* c);
+// device-side: results land in c->d_scal[slot..]; host copy via fetch_scalars
+int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot);
+int vwrms_dev(llg_ctx* c, const double* x, const double* w, int slot);
+int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double* y,
+                   const double* w, int slot);
+int fetch_scalars(llg_ctx* c, int slot, int n, double* out);
+double vmaxnorm_host(llg_ctx* c, const double* x);
+int vlin(llg_ctx* c, double a, const double* x, double b, const double* y, double* z);
+int vscale(llg_ctx* c, double a, const double* x, double* z);
+int vconst(llg_ctx* c, double a, double* z);
+int vprod(llg_ctx* c, const double* x, const double* y, double* z);
+int vdiv(llg_ctx* c, const double* x, const double* y, double* z);
+int vlincomb(llg_ctx* c, int nvec, const double* coef, const double* const* X, double* z);
+int vscale_add_multi(llg_ctx* c, int nvec, const double* a, const double* x,
+                     double* const* Y, double* const* Z);
+int vnordsieck_shift(llg_ctx* c, int q, double* const* zn, int sign);
+int vscale_columns(llg_ctx* c, int q, double eta, double* const* zn);
+int vset_ewt(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot);
+int vhin_bound(llg_ctx* c, double rtol, double atol, const double* y0, const double* f0,
+               double* tmp);

@@ -1,0 +1,357 @@
+"""Host-side binding of libllg.so, the C ABI declared in include/llg.h.
+
+This module is a thin ctypes layer for Python callers (the test-suite and
+bench.py); it mirrors the POD structs of include/llg.h field for field and
+exposes the operator callbacks with the reference's argument meaning:
+
+    rhs(t, y, ydot)                     f(t, y, ydot, user_data)       2d_i2/2d_fft.cu:366
+    jtv(v, Jv, t, y, fy)                JtvProduct(v, Jv, t, y, fy, …)  2d_i2/jtv.cu:131
+    psetup(t, y, fy, jok, gamma)        PrecondSetup(…)                 2d_i2/precond.cu:323
+    psolve(t, y, fy, r, z, gamma, δ, lr) PrecondSolve(…)                2d_i2/precond.cu:360
+
+Device buffers are passed as integer device addresses (torch tensors'
+data_ptr()).  A call that returns a negative status raises LLGError; the
+CUDA library must be present — there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libllg.so")
+
+# ── constants (include/llg.h) ───────────────────────────────────────────
+LLG_SUCCESS = 0
+EXEC_YMSK, EXEC_COMPACT = 0, 1
+BC_PERIODIC, BC_FREE = 0, 1
+NORM_NONE, NORM_EXACT, NORM_REG = 0, 1, 2
+ANISO_LINEAR, ANISO_CUBIC = 0, 1
+DEMAG_OFF, DEMAG_PERIODIC, DEMAG_OPEN = 0, 1, 2
+DEMAG_FP64, DEMAG_MIXED = 0, 1
+JV_REFERENCE, JV_FULL_FIELD = 0, 1
+GS_AUTO, GS_CLASSICAL, GS_MODIFIED = 0, 1, 2
+PREC_BLOCK_JACOBI, PREC_LEARNED = 0, 1
+GEOM_BULK, GEOM_HOLE_SQUARE, GEOM_RING, GEOM_POLYCRYSTAL, GEOM_CUSTOM, GEOM_ELLIPSE, GEOM_ANNULUS = range(7)
+IC_UNIFORM, IC_HEAD_ON_STRIPES, IC_TWO_DOMAIN, IC_GRAIN_BUMPS, IC_CUSTOM, IC_TWO_DOMAIN_X, IC_VORTEX = range(7)
+
+CV_CODES = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC", -3: "CV_ERR_FAILURE",
+            -4: "CV_CONV_FAILURE", -6: "CV_LSETUP_FAIL", -7: "CV_LSOLVE_FAIL", -8: "CV_RHSFUNC_FAIL",
+            -22: "CV_ILL_INPUT", -27: "CV_TOO_CLOSE", -40: "CV_BAD_STATE"}
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("ng", C.c_int32), ("ny", C.c_int32), ("exec_model", C.c_int32), ("bc", C.c_int32),
+        ("norm_kind", C.c_int32), ("aniso_kind", C.c_int32), ("demag_mode", C.c_int32),
+        ("demag_precision", C.c_int32), ("windowed", C.c_int32), ("jv_mode", C.c_int32),
+        ("precond_kind", C.c_int32), ("reserved0", C.c_int32),
+        ("norm_eps", C.c_double), ("che", C.c_double), ("chk", C.c_double), ("cha", C.c_double),
+        ("chb", C.c_double), ("alpha", C.c_double), ("chg", C.c_double),
+        ("msk", C.c_double * 3), ("nsk", C.c_double * 3), ("happ", C.c_double * 3),
+        ("demag_strength", C.c_double), ("demag_thick", C.c_double),
+    ]
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [
+        ("rtol", C.c_double), ("atol", C.c_double), ("maxl", C.c_int32), ("maxord", C.c_int32),
+        ("gs_type", C.c_int32), ("mxstep", C.c_int32), ("device_resident", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("nst", C.c_int64), ("nfe", C.c_int64), ("nsetups", C.c_int64), ("nni", C.c_int64),
+        ("ncfn", C.c_int64), ("netf", C.c_int64), ("nli", C.c_int64), ("nlcf", C.c_int64),
+        ("njvevals", C.c_int64), ("npsolves", C.c_int64), ("npe", C.c_int64),
+        ("nfe_demag", C.c_int64), ("qlast", C.c_int32), ("qcur", C.c_int32),
+        ("hlast", C.c_double), ("hcur", C.c_double), ("tcur", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GeomSpec(C.Structure):
+    _fields_ = [
+        ("ng", C.c_int32), ("ny", C.c_int32), ("geometry_kind", C.c_int32), ("ic_kind", C.c_int32),
+        ("hole_center_x_frac", C.c_double), ("hole_center_y_frac", C.c_double),
+        ("hole_radius_frac_y", C.c_double),
+        ("outer_w_frac", C.c_double), ("outer_h_frac", C.c_double),
+        ("inner_w_frac_of_outer", C.c_double), ("inner_h_frac_of_outer", C.c_double),
+        ("active_rx_frac", C.c_double), ("active_ry_frac", C.c_double),
+        ("annulus_r_in_frac", C.c_double), ("annulus_r_out_frac", C.c_double),
+        ("num_grains", C.c_int32), ("hole_seed", C.c_uint32),
+        ("dead_grain_frac", C.c_double), ("mask_eps_cells", C.c_double), ("grain_z_bias", C.c_double),
+        ("init_m", C.c_double * 3), ("init_random_seed", C.c_uint32), ("reserved0", C.c_int32),
+        ("init_random_eps", C.c_double), ("stripe_left_frac", C.c_double),
+        ("stripe_right_frac", C.c_double), ("two_domain_split_frac", C.c_double),
+        ("two_domain_tail_my", C.c_double), ("ic_core_mz", C.c_double), ("ic_jitter_eps", C.c_double),
+    ]
+
+
+def default_params(ng, ny, **kw) -> Params:
+    """Physics of the 128x64 local case: A=1, k=0.1 along +x (linear/uniaxial),
+    h_app=(0,0,0.05), alpha=0.02, free edges, no demag, no normalisation."""
+    p = Params()
+    p.ng, p.ny = ng, ny
+    p.exec_model, p.bc, p.norm_kind = EXEC_YMSK, BC_FREE, NORM_NONE
+    p.aniso_kind, p.demag_mode, p.demag_precision = ANISO_LINEAR, DEMAG_OFF, DEMAG_FP64
+    p.windowed, p.jv_mode, p.precond_kind = 0, JV_REFERENCE, PREC_BLOCK_JACOBI
+    p.norm_eps = 1e-3
+    p.che, p.chk, p.cha, p.chb, p.alpha, p.chg = 1.0, 0.1, 0.0, 0.0, 0.02, 1.0
+    p.msk[:] = (1.0, 0.0, 0.0)
+    p.nsk[:] = (1.0, 0.0, 0.0)
+    p.happ[:] = (0.0, 0.0, 0.05)
+    p.demag_strength, p.demag_thick = 0.0, 1.0
+    for k, v in kw.items():
+        if k in ("msk", "nsk", "happ"):
+            getattr(p, k)[:] = v
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def default_solver_opts(**kw) -> SolverOpts:
+    o = SolverOpts()
+    o.rtol, o.atol, o.maxl, o.maxord = 1e-4, 1e-6, 5, 5
+    o.gs_type, o.mxstep, o.device_resident = GS_AUTO, 500, 0
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def default_geom(ng, ny, **kw) -> GeomSpec:
+    g = GeomSpec()
+    g.ng, g.ny = ng, ny
+    g.geometry_kind, g.ic_kind = GEOM_BULK, IC_UNIFORM
+    g.hole_center_x_frac, g.hole_center_y_frac, g.hole_radius_frac_y = 0.5, 0.5, 0.22
+    g.outer_w_frac, g.outer_h_frac = 0.5, 0.5
+    g.inner_w_frac_of_outer, g.inner_h_frac_of_outer = 0.5, 0.5
+    g.active_rx_frac, g.active_ry_frac = 0.25, 0.25
+    g.annulus_r_in_frac, g.annulus_r_out_frac = 0.15, 0.35
+    g.num_grains, g.hole_seed = 72, 20251104
+    g.dead_grain_frac, g.mask_eps_cells, g.grain_z_bias = 0.16, 2.2, 1.6
+    g.init_m[:] = (1.0, 0.0, 0.0)
+    g.init_random_seed = 12345
+    g.init_random_eps = 0.01
+    g.stripe_left_frac, g.stripe_right_frac = 0.25, 0.75
+    g.two_domain_split_frac, g.two_domain_tail_my = 0.875, -0.0175
+    g.ic_core_mz, g.ic_jitter_eps = 0.95, 0.0
+    for k, v in kw.items():
+        if k == "init_m":
+            g.init_m[:] = v
+        else:
+            setattr(g, k, v)
+    return g
+
+
+class LLGError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libllg.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise LLGError(f"libllg.so not built at {p}; run __graft_entry__.build()")
+    lib = C.CDLL(p)
+    P, VP, D, I = C.POINTER, C.c_void_p, C.c_double, C.c_int
+    sig = {
+        "llg_default_params": (I, [P(Params)]),
+        "llg_default_solver_opts": (I, [P(SolverOpts)]),
+        "llg_create": (I, [P(Params), P(VP)]),
+        "llg_destroy": (None, [VP]),
+        "llg_set_stream": (I, [VP, VP]),
+        "llg_last_error": (C.c_char_p, []),
+        "llg_set_mask": (I, [VP, P(D)]),
+        "llg_set_active_ids": (I, [VP, P(C.c_int32), C.c_int32, P(C.c_int32), C.c_int32]),
+        "llg_set_window": (I, [VP, P(D), P(D), P(D)]),
+        "llg_rhs": (I, [VP, D, VP, VP]),
+        "llg_jtv": (I, [VP, VP, VP, D, VP, VP]),
+        "llg_psetup": (I, [VP, D, VP, VP, I, P(I), D]),
+        "llg_psolve": (I, [VP, D, VP, VP, VP, VP, D, D, I]),
+        "llg_normalize": (I, [VP, VP]),
+        "llg_demag_apply": (I, [VP, VP, VP]),
+        "llg_demag_self_coupling": (I, [VP, P(D)]),
+        "llg_demag_tensor_host": (I, [VP, I, I, I, P(D)]),
+        "llg_hdemag_device": (VP, [VP]),
+        "llg_dot_multi": (I, [VP, I, VP, P(VP), P(D)]),
+        "llg_linear_combination": (I, [VP, I, P(D), P(VP), VP]),
+        "llg_wrms_norm": (I, [VP, VP, VP, P(D)]),
+        "llg_integrator_init": (I, [VP, D, VP, P(SolverOpts)]),
+        "llg_integrate": (I, [VP, D, VP, P(D)]),
+        "llg_get_stats": (I, [VP, P(Stats)]),
+        "llg_default_geom_spec": (I, [P(GeomSpec)]),
+        "llg_build_geometry": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
+        "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc, what):
+    if rc < 0:
+        msg = _lib.llg_last_error() if _lib is not None else b""
+        raise LLGError(f"{what} failed with status {rc}: {(msg or b'').decode(errors='replace')}")
+    return rc
+
+
+def _ptr(x):
+    """Device/host address of a torch tensor, numpy array or int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(type(x))
+
+
+class Context:
+    """Owns one llg_ctx (one problem instance on the current CUDA device)."""
+
+    def __init__(self, params: Params, stream=None):
+        self.lib = load()
+        self.params = params
+        h = C.c_void_p()
+        _check(self.lib.llg_create(C.byref(params), C.byref(h)), "llg_create")
+        self.h = h
+        self.ncell = params.ng * params.ny
+        if stream is not None:
+            _check(self.lib.llg_set_stream(self.h, _ptr(stream) if not hasattr(stream, "cuda_stream") else stream.cuda_stream), "llg_set_stream")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.llg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # geometry
+    def set_mask(self, ymsk3):
+        import numpy as np
+        a = np.ascontiguousarray(ymsk3, dtype=np.float64)
+        _check(self.lib.llg_set_mask(self.h, a.ctypes.data_as(C.POINTER(C.c_double))), "llg_set_mask")
+
+    def set_active_ids(self, active, inactive):
+        import numpy as np
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        b = np.ascontiguousarray(inactive, dtype=np.int32)
+        _check(self.lib.llg_set_active_ids(self.h, a.ctypes.data_as(C.POINTER(C.c_int32)), len(a),
+                                           b.ctypes.data_as(C.POINTER(C.c_int32)), len(b)), "llg_set_active_ids")
+
+    def set_window(self, w, msk3, nsk3):
+        import numpy as np
+        f = lambda x: None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+        w, msk3, nsk3 = f(w), f(msk3), f(nsk3)
+        cp = lambda x: None if x is None else x.ctypes.data_as(C.POINTER(C.c_double))
+        _check(self.lib.llg_set_window(self.h, cp(w), cp(msk3), cp(nsk3)), "llg_set_window")
+
+    # operators
+    def rhs(self, t, y, ydot):
+        return _check(self.lib.llg_rhs(self.h, t, _ptr(y), _ptr(ydot)), "llg_rhs")
+
+    def jtv(self, v, Jv, t, y, fy=None):
+        return _check(self.lib.llg_jtv(self.h, _ptr(v), _ptr(Jv), t, _ptr(y), _ptr(fy)), "llg_jtv")
+
+    def psetup(self, t, y, fy, jok, gamma):
+        jcur = C.c_int(0)
+        _check(self.lib.llg_psetup(self.h, t, _ptr(y), _ptr(fy), jok, C.byref(jcur), gamma), "llg_psetup")
+        return jcur.value
+
+    def psolve(self, t, y, fy, r, z, gamma, delta=0.0, lr=1):
+        return _check(self.lib.llg_psolve(self.h, t, _ptr(y), _ptr(fy), _ptr(r), _ptr(z), gamma, delta, lr), "llg_psolve")
+
+    def normalize(self, y):
+        return _check(self.lib.llg_normalize(self.h, _ptr(y)), "llg_normalize")
+
+    def demag_apply(self, y, h):
+        return _check(self.lib.llg_demag_apply(self.h, _ptr(y), _ptr(h)), "llg_demag_apply")
+
+    def demag_self_coupling(self):
+        out = (C.c_double * 3)()
+        _check(self.lib.llg_demag_self_coupling(self.h, out), "llg_demag_self_coupling")
+        return tuple(out)
+
+    def demag_tensor(self, comp, dx, dy):
+        out = C.c_double()
+        _check(self.lib.llg_demag_tensor_host(self.h, comp, dx, dy, C.byref(out)), "llg_demag_tensor_host")
+        return out.value
+
+    def hdemag_ptr(self):
+        return self.lib.llg_hdemag_device(self.h)
+
+    def dot_multi(self, x, Ys):
+        n = len(Ys)
+        arr = (C.c_void_p * n)(*[_ptr(y) for y in Ys])
+        out = (C.c_double * n)()
+        _check(self.lib.llg_dot_multi(self.h, n, _ptr(x), arr, out), "llg_dot_multi")
+        return list(out)
+
+    def linear_combination(self, coeffs, Xs, z):
+        n = len(Xs)
+        arr = (C.c_void_p * n)(*[_ptr(x) for x in Xs])
+        c = (C.c_double * n)(*coeffs)
+        return _check(self.lib.llg_linear_combination(self.h, n, c, arr, _ptr(z)), "llg_linear_combination")
+
+    def wrms_norm(self, x, w):
+        out = C.c_double()
+        _check(self.lib.llg_wrms_norm(self.h, _ptr(x), _ptr(w), C.byref(out)), "llg_wrms_norm")
+        return out.value
+
+    # integrator
+    def integrator_init(self, t0, y0, opts: SolverOpts):
+        return _check(self.lib.llg_integrator_init(self.h, t0, _ptr(y0), C.byref(opts)), "llg_integrator_init")
+
+    def integrate(self, tout, yout):
+        tret = C.c_double()
+        rc = self.lib.llg_integrate(self.h, tout, _ptr(yout), C.byref(tret))
+        if rc < 0:
+            raise LLGError(f"llg_integrate -> {CV_CODES.get(rc, rc)}: "
+                           f"{(self.lib.llg_last_error() or b'').decode(errors='replace')}")
+        return tret.value
+
+    def stats(self):
+        st = Stats()
+        _check(self.lib.llg_get_stats(self.h, C.byref(st)), "llg_get_stats")
+        return st.as_dict()
+
+
+def build_geometry(spec: GeomSpec, want=("active", "w", "msk3", "nsk3", "grain_id", "y0")):
+    """Host geometry/IC builder of libllg.so; returns numpy arrays."""
+    import numpy as np
+    lib = load()
+    n = spec.ng * spec.ny
+    out = {
+        "active": np.zeros(n, np.uint8) if "active" in want else None,
+        "w": np.zeros(n, np.float64) if "w" in want else None,
+        "msk3": np.zeros(3 * n, np.float64) if "msk3" in want else None,
+        "nsk3": np.zeros(3 * n, np.float64) if "nsk3" in want else None,
+        "grain_id": np.zeros(n, np.int32) if "grain_id" in want else None,
+        "y0": np.zeros(3 * n, np.float64) if "y0" in want else None,
+    }
+    ptr = lambda a: None if a is None else a.ctypes.data
+    rc = lib.llg_build_geometry(C.byref(spec), ptr(out["active"]), ptr(out["w"]), ptr(out["msk3"]),
+                                ptr(out["nsk3"]), ptr(out["grain_id"]), ptr(out["y0"]))
+    _check(rc, "llg_build_geometry")
+    out["n_active"] = rc
+    return out

@@ -1,0 +1,279 @@
+/*
+ * llg.h — C ABI of the B200-native 2-D Landau–Lifshitz–Gilbert hot path.
+ *
+ * Everything here is plain C: pointers, sizes and POD structs, no CUDA or
+ * torch types.  Vectors are FP64 SoA [mx | my | mz], each block `ncell`
+ * long, cell = j*ng + i (row-major, x fastest), exactly the N_Vector layout
+ * of the reference (src/irregular/2d_fft/2d_i2/2d_fft.cu:233-235).
+ *
+ * Entry points and the reference interface each one replaces:
+ *
+ *   llg_rhs        ← f(t, y, ydot, user_data)            2d_i2/2d_fft.cu:366-411
+ *                                                        (compact 2d_i6/2d_i6.cu:352-396,
+ *                                                         polycrystal 2d_i3/2d_fft.cu:656-726,
+ *                                                         linear+DMI 2d_i1/2d_fft.cu:380-435)
+ *   llg_jtv        ← JtvProduct(v, Jv, t, y, fy, ud, tmp) 2d_i2/jtv.h:26-27, jtv.cu:131-149
+ *   llg_psetup     ← PrecondSetup(t,y,fy,jok,jcur,γ,ud)   2d_i2/precond.h:31-34, precond.cu:323-357
+ *   llg_psolve     ← PrecondSolve(t,y,fy,r,z,γ,δ,lr,ud)   2d_i2/precond.h:35-38, precond.cu:360-384
+ *   llg_demag_apply← Demag_Apply(d, y, h)                 2d_i2/demag_fft.h:33
+ *   llg_dot_multi  ← FusedNVec_DotProdMulti (nvdotprodmulti slot)
+ *                                                        2d_i2/deferred_nvector.cu:146-180
+ *   llg_integrator_* / llg_integrate
+ *                  ← CVodeCreate(CV_BDF)/CVodeInit/CVodeSVtolerances/
+ *                    SUNLinSol_SPGMR/CVode(…, CV_NORMAL)  2d_i2/2d_fft.cu:648-724
+ *
+ * Status convention (CVODE callback convention, 2d_i2/2d_fft.cu:404-410):
+ *   0 success, <0 unrecoverable, >0 recoverable.
+ */
+#ifndef LLG_H
+#define LLG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ── status codes ─────────────────────────────────────────────────────── */
+#define LLG_SUCCESS          0
+#define LLG_RECOVERABLE      1     /* callback: recoverable failure          */
+#define LLG_ERR_LAUNCH      (-1)   /* callback: CUDA launch failed (ref. -1) */
+#define LLG_ERR_ARG       (-100)   /* bad argument / inconsistent config     */
+#define LLG_ERR_CUDA      (-101)   /* CUDA runtime error                     */
+#define LLG_ERR_NOMEM     (-102)   /* allocation failed                      */
+#define LLG_ERR_STATE     (-103)   /* call out of order (e.g. no integrator) */
+#define LLG_ERR_TIMEOUT   (-104)   /* bounded device wait ran out            */
+#define LLG_ERR_NOTSUP    (-105)   /* size/feature not supported             */
+
+/* integrator return codes (same values as CVODE's CV_* flags) */
+#define LLG_CV_SUCCESS          0
+#define LLG_CV_TOO_MUCH_WORK  (-1)
+#define LLG_CV_TOO_MUCH_ACC   (-2)
+#define LLG_CV_ERR_FAILURE    (-3)
+#define LLG_CV_CONV_FAILURE   (-4)
+#define LLG_CV_LSETUP_FAIL    (-6)
+#define LLG_CV_LSOLVE_FAIL    (-7)
+#define LLG_CV_RHSFUNC_FAIL   (-8)
+#define LLG_CV_ILL_INPUT     (-22)
+#define LLG_CV_TOO_CLOSE     (-27)
+#define LLG_CV_BAD_STATE     (-40)  /* non-finite state detected (no CVODE twin) */
+
+/* ── knob enums (values follow configs/sim_config.h) ──────────────────── */
+#define LLG_EXEC_YMSK        0     /* sim_config.h EXEC_YMSK    */
+#define LLG_EXEC_COMPACT     1     /* sim_config.h EXEC_COMPACT */
+
+#define LLG_BC_PERIODIC      0     /* wrap in x and y (every reference kernel) */
+#define LLG_BC_FREE          1     /* out-of-grid neighbour reads 0            */
+
+#define LLG_NORM_NONE        0     /* i4/i5/i6: no normalisation inside f       */
+#define LLG_NORM_EXACT       1     /* i1: m/|m| when |m| > 1e-30                */
+#define LLG_NORM_REG         2     /* i2/i3: m/(|m| + eps)                      */
+
+#define LLG_ANISO_LINEAR     0     /* sim_config.h ANISO_LINEAR: h += msk (chk (m·msk) + cha) */
+#define LLG_ANISO_CUBIC      1     /* sim_config.h ANISO_CUBIC:  h_a += msk_a chk m_a (m_a^2 - 1) */
+
+#define LLG_DEMAG_OFF        0
+#define LLG_DEMAG_PERIODIC   1     /* reference: circular convolution on ng x ny */
+#define LLG_DEMAG_OPEN       2     /* zero-padded 2ng x 2ny (open boundaries)    */
+
+#define LLG_DEMAG_FP64       0     /* plain FP64 transform chain                 */
+#define LLG_DEMAG_MIXED      1     /* reduced-precision transform chain          */
+
+#define LLG_JV_REFERENCE     0     /* Jv field without demag/Zeeman (2d_i2/jtv.cu:87-97) */
+#define LLG_JV_FULL_FIELD    1     /* Jv field includes h_demag and h_app          */
+
+#define LLG_GS_AUTO          0     /* classical if neq < 500000 (2d_i2/2d_fft.cu:674) */
+#define LLG_GS_CLASSICAL     1
+#define LLG_GS_MODIFIED      2
+
+#define LLG_PREC_BLOCK_JACOBI 0
+#define LLG_PREC_LEARNED      1    /* learned stencil correction on top of block-Jacobi */
+
+/* ── problem parameters (one source of truth for f, Jv, P) ───────────── */
+typedef struct llg_params {
+  int32_t ng, ny;          /* cells in x and y (the reference's ng = NX_VAL/3)   */
+  int32_t exec_model;      /* LLG_EXEC_*                                          */
+  int32_t bc;              /* LLG_BC_*                                            */
+  int32_t norm_kind;       /* LLG_NORM_*                                          */
+  int32_t aniso_kind;      /* LLG_ANISO_*                                         */
+  int32_t demag_mode;      /* LLG_DEMAG_*                                         */
+  int32_t demag_precision; /* LLG_DEMAG_FP64 | LLG_DEMAG_MIXED                    */
+  int32_t windowed;        /* 1: per-cell window w + per-cell msk/nsk (polycrystal) */
+  int32_t jv_mode;         /* LLG_JV_*                                            */
+  int32_t precond_kind;    /* LLG_PREC_*                                          */
+  int32_t reserved0;
+  double  norm_eps;        /* LLG_NORM_REG epsilon (reference 1e-3)               */
+  double  che;             /* exchange coupling                                   */
+  double  chk;             /* anisotropy constant                                 */
+  double  cha;             /* linear-anisotropy offset                            */
+  double  chb;             /* DMI strength                                        */
+  double  alpha;           /* Gilbert damping                                     */
+  double  chg;             /* gyromagnetic prefactor                              */
+  double  msk[3];          /* easy axis (uniform; per-cell when windowed)         */
+  double  nsk[3];          /* DMI direction (uniform; per-cell when windowed)     */
+  double  happ[3];         /* uniform applied field                               */
+  double  demag_strength;  /* DEMAG_STRENGTH                                      */
+  double  demag_thick;     /* DEMAG_THICK                                         */
+} llg_params;
+
+/* ── integrator options ───────────────────────────────────────────────── */
+typedef struct llg_solver_opts {
+  double  rtol;            /* RTOL_VAL                                            */
+  double  atol;            /* ATOL_VAL (scalar; SV tolerances with one value)     */
+  int32_t maxl;            /* KRYLOV_DIM (<=0 → 5, the SPGMR default)             */
+  int32_t maxord;          /* MAX_BDF_ORDER (1..5)                                */
+  int32_t gs_type;         /* LLG_GS_*                                            */
+  int32_t mxstep;          /* max internal steps per llg_integrate call (500)     */
+  int32_t device_resident; /* 1: whole step loop on the device (CUDA graph)       */
+  int32_t reserved0;
+} llg_solver_opts;
+
+/* counters, same meaning as PrintFinalStats (2d_i2/2d_fft.cu:414-435) */
+typedef struct llg_stats {
+  int64_t nst, nfe, nsetups, nni, ncfn, netf, nli, nlcf, njvevals, npsolves, npe;
+  int64_t nfe_demag;       /* RHS calls that ran the demag chain                  */
+  int32_t qlast, qcur;
+  double  hlast, hcur, tcur;
+} llg_stats;
+
+typedef struct llg_ctx llg_ctx;
+
+/* ── lifecycle ────────────────────────────────────────────────────────── */
+/* Fill p with the physics of BASELINE config 0 (A=1, k=0.1 along +x, …). */
+int  llg_default_params(llg_params* p);
+int  llg_default_solver_opts(llg_solver_opts* o);
+int  llg_create(const llg_params* p, llg_ctx** out);
+void llg_destroy(llg_ctx* ctx);
+/* All work of ctx is issued on this stream (a cudaStream_t; NULL = legacy default). */
+int  llg_set_stream(llg_ctx* ctx, void* cuda_stream);
+const char* llg_last_error(void);
+
+/* ── geometry upload (host arrays, copied once) ──────────────────────── */
+/* EXEC_YMSK: reference SoA mask ymsk[3*ncell], entries 0 or 1, equal across
+ * the three components (2d_i2/2d_fft.cu:538-566).                          */
+int  llg_set_mask(llg_ctx* ctx, const double* h_ymsk3);
+/* EXEC_COMPACT: active / inactive cell lists (2d_i6/2d_i6.cu:462-533).    */
+int  llg_set_active_ids(llg_ctx* ctx, const int32_t* h_active, int32_t n_active,
+                        const int32_t* h_inactive, int32_t n_inactive);
+/* windowed (polycrystal): w[ncell], msk[3*ncell], nsk[3*ncell]
+ * (2d_i3/2d_fft.cu:317-387).                                               */
+int  llg_set_window(llg_ctx* ctx, const double* h_w, const double* h_msk3,
+                    const double* h_nsk3);
+
+/* ── operator callbacks (device pointers, SoA, length 3*ncell) ───────── */
+/* f: normalise y in place (norm_kind), demag → h_demag, RHS → ydot.        */
+int  llg_rhs(llg_ctx* ctx, double t, double* d_y, double* d_ydot);
+/* Jv = J(y)·v, analytic (exchange + anisotropy + DMI; demag excluded).     */
+int  llg_jtv(llg_ctx* ctx, const double* d_v, double* d_Jv, double t,
+             const double* d_y, const double* d_fy);
+/* Build the 3×3 block-Jacobi inverse (I − γJ)^-1 at y using the demag field
+ * of the last llg_rhs call; always rebuilds and sets *jcur = 1.            */
+int  llg_psetup(llg_ctx* ctx, double t, const double* d_y, const double* d_fy,
+                int jok, int* jcur, double gamma);
+/* z = P^-1 r, masked.                                                        */
+int  llg_psolve(llg_ctx* ctx, double t, const double* d_y, const double* d_fy,
+                const double* d_r, double* d_z, double gamma, double delta, int lr);
+/* In-place normalisation kernel alone (the first stage of llg_rhs).        */
+int  llg_normalize(llg_ctx* ctx, double* d_y);
+/* Demag field h = strength · N ⊛ (w·m), overwriting d_h (3*ncell).          */
+int  llg_demag_apply(llg_ctx* ctx, const double* d_y, double* d_h);
+/* N(0)·strength diagonal (Demag_GetSelfCoupling, 2d_i2/demag_fft.cu:365-377). */
+int  llg_demag_self_coupling(llg_ctx* ctx, double out3[3]);
+/* Unscaled Newell tensor component c (0..8 = xx,xy,xz,yx,yy,yz,zx,zy,zz) at
+ * displacement (dx, dy) on the demag grid, host copy (for checks).          */
+int  llg_demag_tensor_host(llg_ctx* ctx, int comp, int dx, int dy, double* out);
+/* Device pointer of the demag field written by the last llg_rhs call.      */
+const double* llg_hdemag_device(llg_ctx* ctx);
+
+/* ── fused vector ops (deterministic: fixed reduction order, no atomics) ── */
+/* out[k] = x · Y[k], k < nvec ≤ 16, one launch; h_out is host memory.       */
+int  llg_dot_multi(llg_ctx* ctx, int nvec, const double* d_x,
+                   const double* const* d_Y, double* h_out);
+/* z = Σ_k c[k] X[k], nvec ≤ 16, one pass.                                   */
+int  llg_linear_combination(llg_ctx* ctx, int nvec, const double* c,
+                            const double* const* d_X, double* d_z);
+/* sqrt(mean((x·w)^2)), host result.                                          */
+int  llg_wrms_norm(llg_ctx* ctx, const double* d_x, const double* d_w, double* h_out);
+
+/* ── integrator: BDF (orders 1..5, Nordsieck) + Newton + SPGMR ───────── */
+int  llg_integrator_init(llg_ctx* ctx, double t0, const double* d_y0,
+                         const llg_solver_opts* opts);
+/* Advance to tout (CV_NORMAL: may step past tout, returns y(tout) by
+ * interpolation).  d_yout: device, 3*ncell.                                */
+int  llg_integrate(llg_ctx* ctx, double tout, double* d_yout, double* tret);
+int  llg_get_stats(llg_ctx* ctx, llg_stats* st);
+
+/* ── instrumentation ──────────────────────────────────────────────────── */
+/* Kernel families, in this order: RHS, JTV, ARNOLDI (fused Krylov operator),
+ * PSETUP, PSOLVE, NORM, DEMAG_ROWS_FWD, DEMAG_COLS, DEMAG_ROWS_INV, REDUCE,
+ * ELEMWISE, LEARNED, OTHER.  Counts are process-wide launch counts.        */
+#define LLG_KERNEL_FAMILIES 13
+int  llg_kernel_counts(int64_t* out, int n);
+void llg_reset_kernel_counts(void);
+/* Average device time of one launch of family kernel_id (CUDA events on the
+ * context's stream), measured on the live integrator buffers.              */
+int  llg_time_kernel(llg_ctx* ctx, int kernel_id, int iters, double* avg_ms);
+
+/* ── geometry / initial-condition builders (host) ────────────────────── */
+#define LLG_GEOM_BULK         0   /* sim_config.h GEOMETRY_BULK          */
+#define LLG_GEOM_HOLE_SQUARE  1   /* GEOMETRY_HOLE_SQUARE (2d_i2)          */
+#define LLG_GEOM_RING         2   /* GEOMETRY_RING: outer rect − inner rect */
+#define LLG_GEOM_POLYCRYSTAL  3   /* GEOMETRY_POLYCRYSTAL (2d_i3)          */
+#define LLG_GEOM_CUSTOM       4   /* caller builds the arrays              */
+#define LLG_GEOM_ELLIPSE      5   /* GEOMETRY_ELLIPSE (2d_i6)              */
+#define LLG_GEOM_ANNULUS      6   /* circular ring r_in..r_out (no reference twin) */
+
+#define LLG_IC_UNIFORM        0   /* IC_UNIFORM                            */
+#define LLG_IC_HEAD_ON_STRIPES 1  /* IC_HEAD_ON_STRIPES (2d_i1)            */
+#define LLG_IC_TWO_DOMAIN     2   /* IC_TWO_DOMAIN (2d_i4)                 */
+#define LLG_IC_GRAIN_BUMPS    3   /* IC_GRAIN_BUMPS (2d_i3)                */
+#define LLG_IC_CUSTOM         4
+#define LLG_IC_TWO_DOMAIN_X   5   /* +x left half, −x right half (no reference twin) */
+#define LLG_IC_VORTEX         6   /* (−y, x, 0.1)/norm about the centre (no reference twin) */
+
+typedef struct llg_geom_spec {
+  int32_t ng, ny;
+  int32_t geometry_kind;          /* LLG_GEOM_*                              */
+  int32_t ic_kind;                /* LLG_IC_*                                */
+  /* square hole */
+  double  hole_center_x_frac, hole_center_y_frac, hole_radius_frac_y;
+  /* rectangular ring */
+  double  outer_w_frac, outer_h_frac, inner_w_frac_of_outer, inner_h_frac_of_outer;
+  /* ellipse */
+  double  active_rx_frac, active_ry_frac;
+  /* annulus (radii as fractions of min(ng, ny)) */
+  double  annulus_r_in_frac, annulus_r_out_frac;
+  /* polycrystal */
+  int32_t num_grains;
+  uint32_t hole_seed;
+  double  dead_grain_frac, mask_eps_cells, grain_z_bias;
+  /* initial condition */
+  double  init_m[3];
+  uint32_t init_random_seed;
+  int32_t reserved0;
+  double  init_random_eps;        /* stripes: my, mz amplitude (2d_i1)       */
+  double  stripe_left_frac, stripe_right_frac;
+  double  two_domain_split_frac, two_domain_tail_my;
+  double  ic_core_mz;
+  double  ic_jitter_eps;          /* U(±eps) on every component, then |m|=1  */
+} llg_geom_spec;
+
+int llg_default_geom_spec(llg_geom_spec* g);
+/* Fills the arrays that are non-NULL:
+ *   active[ncell] (1 active / 0 hole), w[ncell], msk3[3*ncell], nsk3[3*ncell],
+ *   grain_id[ncell], y0[3*ncell].  Returns the number of active cells (≥0)
+ *   or a negative LLG_ERR_*.  Uses the C library srand/rand in the
+ *   reference's call order.                                                 */
+int llg_build_geometry(const llg_geom_spec* g, uint8_t* active, double* w,
+                       double* msk3, double* nsk3, int32_t* grain_id, double* y0);
+
+/* KEY=VALUE parser using the sim_config.h / params.mk knob names
+ * (configs/sim_config.h); lines or whitespace separated; '#' comments.     */
+int llg_parse_config(const char* text, llg_params* p, llg_geom_spec* g,
+                     llg_solver_opts* o);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LLG_H */
