@@ -15,9 +15,12 @@
 //                 inverse FFT along y → S (only the data rows are kept).
 //   K3 rows_inv : inverse real FFT along x → h, × strength/(Px·Py) folded into
 //                 the tensor, written SoA for the first ng columns only.
-// Every transform runs in shared memory as in-place mixed-radix DIT (digit-
-// reversed load) or DIF (digit-reversed store) passes, radices 8/4/2/3/5 and a
-// generic odd radix; HBM sees each element of y, S and h once per kernel.
+// Every transform is a Stockham autosort FFT in shared memory (natural order
+// in and out, no reordering tables): each pass stages the thread's radix-R
+// butterflies (R = 8/4/2/3/5; any other prime through a generic path) in
+// registers, synchronises, and scatters the results in place.  A CTA row of
+// threads owns one transform; HBM sees each element of y, S and h once per
+// kernel.
 // The tensor is stored wrapped at displacement d mod P (d in [-P/2, P-1-P/2]),
 // which equals the reference's centring + output shift; the open-boundary
 // tensor has its unused d = -P/2 lines zeroed, so its spectra are real.  Only
@@ -36,11 +39,13 @@ namespace {
 
 constexpr int MAXR = 24;  // passes
 
+// Stockham plan for one transform length n.  Radices in pass order
+// (8/4/2 first so every power-of-two pass sees a power-of-two span Ns, then
+// 3, 5 and any other prime).  tx = threads per transform.
 struct FftPlan {
-  int n, nr;
-  int radix[MAXR];
-  const double2* tw;   // tw[k] = exp(-2 pi i k / n)
-  const int* revinv;   // natural index -> DIT position
+  int n, nr, tx;
+  const int4* pass;  // per pass: (radix R, span Ns before the pass, log2 Ns or -1, 0)
+  const double2* tw; // tw[k] = exp(-2 pi i k / n)
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -48,7 +53,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-// multiply by -i*SIGN... : rot(v) = v * (SIGN < 0 ? -i : +i)
+// v * (SIGN < 0 ? -i : +i)
 template <int SIGN>
 __device__ __forceinline__ double2 rot90(double2 v) {
   return (SIGN < 0) ? make_double2(v.y, -v.x) : make_double2(-v.y, v.x);
@@ -98,7 +103,6 @@ __device__ __forceinline__ void dft5(double2* v) {
   const double2 b1 = make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
   const double2 b2 = make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
   v[0] = make_double2(v[0].x + t1.x + t2.x, v[0].y + t1.y + t2.y);
-  // multiply b by i
   v[1] = make_double2(a1.x - b1.y, a1.y + b1.x);
   v[4] = make_double2(a1.x + b1.y, a1.y - b1.x);
   v[2] = make_double2(a2.x - b2.y, a2.y + b2.x);
@@ -107,12 +111,10 @@ __device__ __forceinline__ void dft5(double2* v) {
 template <int SIGN>
 __device__ __forceinline__ void dft8(double2* v) {
   const double h = 0.70710678118654752440;
-  // radix-2 split: even / odd
   double2 e[4] = {v[0], v[2], v[4], v[6]};
   double2 o[4] = {v[1], v[3], v[5], v[7]};
   dft4<SIGN>(e);
   dft4<SIGN>(o);
-  // twiddles w8^k for k=0..3 (SIGN)
   const double2 o1 = make_double2(h * (o[1].x - SIGN * o[1].y), h * (o[1].y + SIGN * o[1].x));
   const double2 o2 = rot90<SIGN>(o[2]);
   const double2 o3 = make_double2(-h * (o[3].x + SIGN * o[3].y), h * (SIGN * o[3].x - o[3].y));
@@ -125,7 +127,6 @@ __device__ __forceinline__ void dft8(double2* v) {
   v[3] = cadd(e[3], o3);
   v[7] = csub(e[3], o3);
 }
-
 template <int R, int SIGN>
 __device__ __forceinline__ void dft_fixed(double2* v) {
   if constexpr (R == 2) dft2<SIGN>(v);
@@ -135,101 +136,89 @@ __device__ __forceinline__ void dft_fixed(double2* v) {
   else if constexpr (R == 8) dft8<SIGN>(v);
 }
 
-// one pass over all butterflies of nbatch transforms held in buf
-template <int R, int SIGN, bool DIF>
-__device__ __forceinline__ void pass_fixed(double2* buf, int nbatch, const FftPlan& pl, int S) {
-  const int nb = pl.n / R;
-  const int total = nb * nbatch;
-  const int tstride = pl.n / (S * R);
-  for (int bf = threadIdx.x; bf < total; bf += blockDim.x) {
-    const int b = bf / nb, k = bf - b * nb;
-    const int g = k / S, j = k - g * S;
-    double2* base = buf + b * pl.n + g * S * R + j;
-    double2 v[R];
+// One Stockham pass of one transform held in buf[0..n).  All threads of the
+// row stage their butterflies in registers, the block synchronises, then
+// twiddle + DFT_R + scatter to (j / Ns)·Ns·R + j % Ns + r·Ns.
+// A row of tx threads covers n/R butterflies with at most MB each
+// (tx >= n/EPT is guaranteed by the plan).
+template <int R, int SIGN, int EPT>
+__device__ __forceinline__ void stockham_pass(double2* buf, const FftPlan& pl, int4 ps) {
+  constexpr int MB = (EPT + R - 1) / R;
+  const int n = pl.n, nb = n / R, Ns = ps.y, lg = ps.z;
+  const int tstride = n / (Ns * R);
+  double2 v[MB][R];
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = base[r * S];
-    if (!DIF) {
+  for (int u = 0; u < MB; u++) {
+    const int j = threadIdx.x + u * blockDim.x;
+    if (j < nb) {
 #pragma unroll
-      for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<SIGN>(pl, j * r * tstride));
+      for (int r = 0; r < R; r++) v[u][r] = buf[j + r * nb];
     }
-    dft_fixed<R, SIGN>(v);
-    if (DIF) {
-#pragma unroll
-      for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<SIGN>(pl, j * r * tstride));
-    }
-#pragma unroll
-    for (int r = 0; r < R; r++) base[r * S] = v[r];
   }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < MB; u++) {
+    const int j = threadIdx.x + u * blockDim.x;
+    if (j < nb) {
+      int q, jm;
+      if (lg >= 0) { q = j >> lg; jm = j & (Ns - 1); }
+      else { q = j / Ns; jm = j - q * Ns; }
+#pragma unroll
+      for (int r = 1; r < R; r++) v[u][r] = cmul(v[u][r], twid<SIGN>(pl, jm * r * tstride));
+      dft_fixed<R, SIGN>(v[u]);
+      const int ob = q * Ns * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; r++) buf[ob + r * Ns] = v[u][r];
+    }
+  }
+  __syncthreads();
 }
 
-// generic odd radix (small primes beyond 5), O(R^2), registers spill to local
-template <int SIGN, bool DIF>
-__device__ void pass_generic(double2* buf, int nbatch, const FftPlan& pl, int S, int R) {
-  const int nb = pl.n / R;
-  const int total = nb * nbatch;
-  const int tstride = pl.n / (S * R);
-  const int rstride = pl.n / R;
-  for (int bf = threadIdx.x; bf < total; bf += blockDim.x) {
-    const int b = bf / nb, k = bf - b * nb;
-    const int g = k / S, j = k - g * S;
-    double2* base = buf + b * pl.n + g * S * R + j;
-    double2 v[64], o[64];
-    for (int r = 0; r < R; r++) {
-      v[r] = base[r * S];
-      if (!DIF && r > 0) v[r] = cmul(v[r], twid<SIGN>(pl, j * r * tstride));
-    }
-    for (int q = 0; q < R; q++) {
+// Any other radix (small primes, test sizes only): one butterfly per thread
+// (the plan sizes tx >= n/R), R <= 64, O(R^2).
+template <int SIGN>
+__device__ void stockham_pass_generic(double2* buf, const FftPlan& pl, int4 ps) {
+  const int R = ps.x;
+  const int n = pl.n, nb = n / R, Ns = ps.y;
+  const int tstride = n / (Ns * R), rstride = n / R;
+  const int j = threadIdx.x;
+  double2 v[64];
+  if (j < nb) {
+    for (int r = 0; r < R; r++) v[r] = buf[j + r * nb];
+  }
+  __syncthreads();
+  if (j < nb) {
+    const int q = j / Ns, jm = j - q * Ns;
+    for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<SIGN>(pl, jm * r * tstride));
+    const int ob = q * Ns * R + jm;
+    for (int k = 0; k < R; k++) {
       double2 acc = v[0];
-      for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid<SIGN>(pl, ((r * q) % R) * rstride)));
-      o[q] = acc;
-    }
-    for (int q = 0; q < R; q++) {
-      double2 w = o[q];
-      if (DIF && q > 0) w = cmul(w, twid<SIGN>(pl, j * q * tstride));
-      base[q * S] = w;
+      for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid<SIGN>(pl, ((r * k) % R) * rstride)));
+      buf[ob + k * Ns] = acc;
     }
   }
+  __syncthreads();
 }
 
-template <int SIGN, bool DIF>
-__device__ __forceinline__ void run_pass(double2* buf, int nbatch, const FftPlan& pl, int S, int R) {
-  switch (R) {
-    case 2: pass_fixed<2, SIGN, DIF>(buf, nbatch, pl, S); break;
-    case 3: pass_fixed<3, SIGN, DIF>(buf, nbatch, pl, S); break;
-    case 4: pass_fixed<4, SIGN, DIF>(buf, nbatch, pl, S); break;
-    case 5: pass_fixed<5, SIGN, DIF>(buf, nbatch, pl, S); break;
-    case 8: pass_fixed<8, SIGN, DIF>(buf, nbatch, pl, S); break;
-    default: pass_generic<SIGN, DIF>(buf, nbatch, pl, S, R); break;
-  }
-}
-
-// natural-order output from digit-reversed input
-template <int SIGN>
-__device__ void fft_dit(double2* buf, int nbatch, const FftPlan& pl) {
-  int S = 1;
-  for (int p = 0; p < pl.nr; p++) {
-    const int R = pl.radix[p];
-    run_pass<SIGN, false>(buf, nbatch, pl, S, R);
-    __syncthreads();
-    S *= R;
-  }
-}
-// digit-reversed output from natural-order input
-template <int SIGN>
-__device__ void fft_dif(double2* buf, int nbatch, const FftPlan& pl) {
-  int S = pl.n;
-  for (int p = pl.nr - 1; p >= 0; p--) {
-    const int R = pl.radix[p];
-    S /= R;
-    run_pass<SIGN, true>(buf, nbatch, pl, S, R);
-    __syncthreads();
-  }
+// Natural-order in, natural-order out, in place in buf (this row's transform).
+// Every thread of the block must call it (it synchronises).  The passes run
+// as straight-line regions in factorisation order (8s, one 4, one 2, 3s, 5s,
+// other primes): a runtime switch over radices inside one loop makes the
+// register allocator keep every variant's state live at once.
+template <int SIGN, int EPT>
+__device__ void fft_stockham(double2* buf, const FftPlan& pl) {
+  int p = 0;
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<8, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
+  if (p < pl.nr && __ldg(&pl.pass[p].x) == 4) { stockham_pass<4, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  if (p < pl.nr && __ldg(&pl.pass[p].x) == 2) { stockham_pass<2, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<3, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<5, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pl.nr; p++) stockham_pass_generic<SIGN>(buf, pl, __ldg(&pl.pass[p]));
 }
 
 // ── K1: forward real transform of data rows along x ─────────────────────
-// CTA = (component c, group of 2*NB rows); NB complex transforms of length n.
-// in: comp c row r at in + c*comp_stride + r*row_len, valid i < row_len.
-template <int NB>
+// CTA = (component c, 2*NB rows); threadIdx.y = packed transform (rows ya, ya+1).
+template <int NB, int EPT>
 __global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long comp_stride, int row_len,
                            int nrows, const double* __restrict__ w, double2* __restrict__ S, int ld,
                            int Hx) {
@@ -237,10 +226,11 @@ __global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long 
   const int c = blockIdx.y;
   const int y0 = blockIdx.x * (2 * NB);
   const int n = pl.n;
+  const int b = threadIdx.y;
+  double2* buf = sm + b * n;
   const double* src = in + (long long)c * comp_stride;
-  for (int e = threadIdx.x; e < NB * n; e += blockDim.x) {
-    const int b = e / n, i = e - b * n;
-    const int ya = y0 + 2 * b, yb = ya + 1;
+  const int ya = y0 + 2 * b, yb = ya + 1;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double va = 0.0, vb = 0.0;
     if (i < row_len) {
       if (ya < nrows) {
@@ -252,18 +242,18 @@ __global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long 
         vb = src[q] * (w ? w[q] : 1.0);
       }
     }
-    sm[b * n + pl.revinv[i]] = make_double2(va, vb);
+    buf[i] = make_double2(va, vb);
   }
   __syncthreads();
-  fft_dit<-1>(sm, NB, pl);
-  // split the packed spectrum into the two real rows' half spectra
-  for (int e = threadIdx.x; e < Hx * 2 * NB; e += blockDim.x) {
+  fft_stockham<-1, EPT>(buf, pl);
+  const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int e = tid; e < Hx * 2 * NB; e += T) {
     const int kx = e / (2 * NB), r = e - kx * (2 * NB);
-    const int b = r >> 1, which = r & 1;
+    const int bb = r >> 1, which = r & 1;
     const int y = y0 + r;
     if (y >= nrows) continue;
-    const double2 zk = sm[b * n + kx];
-    const double2 zm = sm[b * n + ((n - kx) % n)];
+    const double2 zk = sm[bb * n + kx];
+    const double2 zm = sm[bb * n + ((n - kx) % n)];
     double2 out;
     if (!which) out = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
     else out = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
@@ -272,22 +262,23 @@ __global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long 
 }
 
 // ── K2: column transform + tensor multiply + inverse column transform ─────
+// CTA = one x-frequency column; threadIdx.y = component.
+template <int EPT>
 __global__ void k_cols_conv(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx,
                             const double* __restrict__ txx, const double* __restrict__ tyy,
                             const double* __restrict__ tzz, const double2* __restrict__ txy) {
   extern __shared__ double2 sm[];
   const int kx = blockIdx.x;
   const int n = pl.n;
-  for (int e = threadIdx.x; e < 3 * n; e += blockDim.x) {
-    const int c = e / n, yy = e - c * n;
-    double2 v = make_double2(0.0, 0.0);
-    if (yy < nrows) v = S[((long long)c * Hx + kx) * ld + yy];
-    sm[c * n + pl.revinv[yy]] = v;
-  }
+  const int c = threadIdx.y;
+  double2* buf = sm + c * n;
+  double2* col = S + ((long long)c * Hx + kx) * ld;
+  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) buf[yy] = (yy < nrows) ? col[yy] : make_double2(0.0, 0.0);
   __syncthreads();
-  fft_dit<-1>(sm, 3, pl);
+  fft_stockham<-1, EPT>(buf, pl);
   const long long tb = (long long)kx * n;
-  for (int ky = threadIdx.x; ky < n; ky += blockDim.x) {
+  const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int ky = tid; ky < n; ky += T) {
     const double2 mx = sm[ky], my = sm[n + ky], mz = sm[2 * n + ky];
     const double a = __ldg(&txx[tb + ky]), b = __ldg(&tyy[tb + ky]), d = __ldg(&tzz[tb + ky]);
     const double2 xy = __ldg(&txy[tb + ky]);
@@ -297,54 +288,50 @@ __global__ void k_cols_conv(FftPlan pl, double2* __restrict__ S, int ld, int nro
     sm[2 * n + ky] = make_double2(d * mz.x, d * mz.y);
   }
   __syncthreads();
-  fft_dif<+1>(sm, 3, pl);
-  for (int e = threadIdx.x; e < 3 * nrows; e += blockDim.x) {
-    const int c = e / nrows, yy = e - c * nrows;
-    S[((long long)c * Hx + kx) * ld + yy] = sm[c * n + pl.revinv[yy]];
-  }
+  fft_stockham<+1, EPT>(buf, pl);
+  for (int yy = threadIdx.x; yy < nrows; yy += blockDim.x) col[yy] = buf[yy];
 }
 
 // forward column transform only (tensor spectra at init)
+template <int EPT>
 __global__ void k_cols_fwd(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx) {
   extern __shared__ double2 sm[];
   const int kx = blockIdx.x;
   const int n = pl.n;
-  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) {
-    double2 v = make_double2(0.0, 0.0);
-    if (yy < nrows) v = S[(long long)kx * ld + yy];
-    sm[pl.revinv[yy]] = v;
-  }
+  double2* col = S + (long long)kx * ld;
+  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) sm[yy] = (yy < nrows) ? col[yy] : make_double2(0.0, 0.0);
   __syncthreads();
-  fft_dit<-1>(sm, 1, pl);
-  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) S[(long long)kx * ld + yy] = sm[yy];
+  fft_stockham<-1, EPT>(sm, pl);
+  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) col[yy] = sm[yy];
 }
 
 // ── K3: inverse real transform along x, scatter to SoA h ─────────────────
-template <int NB>
+template <int NB, int EPT>
 __global__ void k_rows_inv(FftPlan pl, const double2* __restrict__ S, int ld, int nrows, int Hx,
                            double* __restrict__ h, long long comp_stride, int ng) {
   extern __shared__ double2 sm[];
   const int c = blockIdx.y;
   const int y0 = blockIdx.x * (2 * NB);
   const int n = pl.n;
+  const int b = threadIdx.y;
   const bool even = (n % 2) == 0;
-  for (int e = threadIdx.x; e < n * 2 * NB; e += blockDim.x) {
-    const int k = e / (2 * NB), r = e - k * (2 * NB);
-    if (r & 1) continue;  // one thread builds both rows of a packed pair
-    const int b = r >> 1;
-    const int ya = y0 + 2 * b, yb = ya + 1;
+  const int ya = y0 + 2 * b, yb = ya + 1;
+  double2* buf = sm + b * n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
     const int kk = (k < Hx) ? k : n - k;
     double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
-    if (ya < nrows) A = S[((long long)c * Hx + kk) * ld + ya];
-    if (yb < nrows) B = S[((long long)c * Hx + kk) * ld + yb];
+    const double2* col = S + ((long long)c * Hx + kk) * ld;
+    if (ya < nrows) A = col[ya];
+    if (yb < nrows) B = col[yb];
     if (kk == 0 || (even && kk == n / 2)) { A.y = 0.0; B.y = 0.0; }
     if (k >= Hx) { A.y = -A.y; B.y = -B.y; }
-    sm[b * n + pl.revinv[k]] = make_double2(A.x - B.y, A.y + B.x);
+    buf[k] = make_double2(A.x - B.y, A.y + B.x);
   }
   __syncthreads();
-  fft_dit<+1>(sm, NB, pl);
+  fft_stockham<+1, EPT>(buf, pl);
   double* dst = h + (long long)c * comp_stride;
-  for (int e = threadIdx.x; e < NB * 2 * ng; e += blockDim.x) {
+  const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int e = tid; e < NB * 2 * ng; e += T) {
     const int r = e / ng, i = e - r * ng;
     const int y = y0 + r;
     if (y >= nrows) continue;
@@ -496,18 +483,20 @@ __global__ void k_tensor_finish(const double2* __restrict__ Sxx, const double2* 
 }  // namespace
 
 // ── host side ───────────────────────────────────────────────────────────
+static constexpr int kRowsNB = 2;  // packed transforms per row-CTA (4 real rows)
+
 struct HostFft {
-  int n = 0;
+  int n = 0, tx = 32, ept = 8;
   std::vector<int> radix;
   double2* d_tw = nullptr;
-  int* d_revinv = nullptr;
+  int4* d_pass = nullptr;
   FftPlan dev() const {
     FftPlan p{};
     p.n = n;
     p.nr = (int)radix.size();
-    for (int i = 0; i < p.nr; i++) p.radix[i] = radix[i];
+    p.tx = tx;
+    p.pass = d_pass;
     p.tw = d_tw;
-    p.revinv = d_revinv;
     return p;
   }
 };
@@ -548,52 +537,46 @@ static int factorize(int n, std::vector<int>& rad) {
     }
   }
   if ((int)rad.size() > MAXR) return -1;
-  if (rad.empty()) rad.push_back(1);
   return 0;
 }
 
-static int fft_init(HostFft& f, int n) {
+static int fft_init(HostFft& f, int n, int batch) {
   f.n = n;
   if (factorize(n, f.radix) != 0) {
     llg_set_error("FFT length " + std::to_string(n) + " has a prime factor > 64");
     return LLG_ERR_NOTSUP;
   }
-  if (f.radix.size() == 1 && f.radix[0] == 1) f.radix.clear();
+  // threads per transform: n/16 covers the fixed radices (<= 16/R butterflies
+  // per thread); a generic radix R needs one thread per butterfly (n/R).
+  f.ept = (((n + 7) / 8 + 31) / 32 * 32 * batch <= 1024) ? 8 : 16;
+  int need = (n + f.ept - 1) / f.ept;
+  for (int r : f.radix)
+    if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) need = std::max(need, n / r);
+  f.tx = ((std::max(need, 32) + 31) / 32) * 32;
   std::vector<double2> tw(n);
   for (int k = 0; k < n; k++) {
-    // exp(-2 pi i k/n) using octant-reduced arguments for accuracy
     const long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
     tw[k] = make_double2((double)cosl(ang), (double)-sinl(ang));
   }
-  // digit reversal: position p (digits r_1.. LSD first, radices in pass order)
-  std::vector<int> revinv(n);
-  const int k = (int)f.radix.size();
-  for (int p = 0; p < n; p++) {
-    int rem = p;
-    std::vector<int> dig(k);
-    for (int s = 0; s < k; s++) { dig[s] = rem % f.radix[s]; rem /= f.radix[s]; }
-    int x = 0;
-    for (int s = 0; s < k; s++) x = x * f.radix[s] + dig[s];
-    // x = r_k + R_k (r_{k-1} + ...): build from MSD = r_1
-    revinv[x] = p;
-  }
   LLG_CUDA_TRY(cudaMalloc(&f.d_tw, sizeof(double2) * n));
-  LLG_CUDA_TRY(cudaMalloc(&f.d_revinv, sizeof(int) * n));
   LLG_CUDA_TRY(cudaMemcpy(f.d_tw, tw.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
-  LLG_CUDA_TRY(cudaMemcpy(f.d_revinv, revinv.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  std::vector<int4> ps(std::max<size_t>(f.radix.size(), 1));
+  int ns = 1;
+  for (size_t i = 0; i < f.radix.size(); i++) {
+    ps[i] = make_int4(f.radix[i], ns, ((ns & (ns - 1)) == 0) ? __builtin_ctz((unsigned)ns) : -1, 0);
+    ns *= f.radix[i];
+  }
+  LLG_CUDA_TRY(cudaMalloc(&f.d_pass, sizeof(int4) * ps.size()));
+  LLG_CUDA_TRY(cudaMemcpy(f.d_pass, ps.data(), sizeof(int4) * ps.size(), cudaMemcpyHostToDevice));
   return 0;
 }
 
 static void fft_free(HostFft& f) {
   cudaFree(f.d_tw);
-  cudaFree(f.d_revinv);
+  cudaFree(f.d_pass);
   f.d_tw = nullptr;
-  f.d_revinv = nullptr;
+  f.d_pass = nullptr;
 }
-
-static constexpr int kRowsNB = 2;     // complex transforms per row-CTA (4 real rows)
-static constexpr int kRowThreads = 256;
-static constexpr int kColThreads = 256;
 
 void demag_destroy(DemagPlan* d) {
   if (!d) return;
@@ -615,6 +598,54 @@ static int set_smem(const void* fn, size_t bytes) {
   return 0;
 }
 
+// ── launch helpers (elements-per-thread dispatch) ─────────────────────────
+static int launch_rows_fwd(const DemagPlan* d, cudaStream_t s, const double* in, long long cs, int row_len,
+                           int nrows, const double* w, double2* S, int ld, int ncomp) {
+  const FftPlan pl = d->fx.dev();
+  const dim3 g((nrows + 2 * kRowsNB - 1) / (2 * kRowsNB), ncomp), b(d->fx.tx, kRowsNB);
+  if (d->fx.ept == 8)
+    k_rows_fwd<kRowsNB, 8><<<g, b, d->smem_rows, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
+  else
+    k_rows_fwd<kRowsNB, 16><<<g, b, d->smem_rows, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, double* h, long long cs) {
+  const FftPlan pl = d->fx.dev();
+  const dim3 g((d->ny + 2 * kRowsNB - 1) / (2 * kRowsNB), 3), b(d->fx.tx, kRowsNB);
+  if (d->fx.ept == 8)
+    k_rows_inv<kRowsNB, 8><<<g, b, d->smem_rows, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, h, cs, d->ng);
+  else
+    k_rows_inv<kRowsNB, 16><<<g, b, d->smem_rows, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, h, cs, d->ng);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+static int launch_cols_conv(const DemagPlan* d, cudaStream_t s) {
+  const FftPlan pl = d->fy.dev();
+  const dim3 b(d->fy.tx, 3);
+  if (d->fy.ept == 8)
+    k_cols_conv<8><<<d->hx, b, d->smem_cols, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy, d->d_tzz,
+                                                  d->d_txy);
+  else
+    k_cols_conv<16><<<d->hx, b, d->smem_cols, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy, d->d_tzz,
+                                                   d->d_txy);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+static int launch_cols_fwd(const DemagPlan* d, cudaStream_t s, double2* S) {
+  const FftPlan pl = d->fy.dev();
+  const size_t sm = sizeof(double2) * (size_t)d->py;
+  if (d->fy.ept == 8)
+    k_cols_fwd<8><<<d->hx, dim3(d->fy.tx, 1), sm, s>>>(pl, S, d->py, d->py, d->hx);
+  else
+    k_cols_fwd<16><<<d->hx, dim3(d->fy.tx, 1), sm, s>>>(pl, S, d->py, d->py, d->hx);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
 int demag_create(llg_ctx* c) {
   const llg_params& p = c->p;
   DemagPlan* d = new DemagPlan();
@@ -625,20 +656,25 @@ int demag_create(llg_ctx* c) {
   d->py = d->open ? 2 * p.ny : p.ny;
   d->hx = d->px / 2 + 1;
   d->strength = p.demag_strength;
-  int rc = fft_init(d->fx, d->px);
-  if (!rc) rc = fft_init(d->fy, d->py);
+  int rc = fft_init(d->fx, d->px, kRowsNB);
+  if (!rc) rc = fft_init(d->fy, d->py, 3);
   if (rc) { demag_destroy(d); return rc; }
   d->smem_rows = sizeof(double2) * (size_t)kRowsNB * d->px;
   d->smem_cols = sizeof(double2) * 3 * (size_t)d->py;
-  if (d->smem_rows > 227 * 1024 || d->smem_cols > 227 * 1024) {
+  if (d->smem_rows > 227 * 1024 || d->smem_cols > 227 * 1024 || d->fx.tx * kRowsNB > 1024 ||
+      d->fy.tx * 3 > 1024) {
     llg_set_error("demag grid too large for the shared-memory transform");
     demag_destroy(d);
     return LLG_ERR_NOTSUP;
   }
-  if ((rc = set_smem((const void*)k_rows_fwd<kRowsNB>, d->smem_rows)) ||
-      (rc = set_smem((const void*)k_rows_inv<kRowsNB>, d->smem_rows)) ||
-      (rc = set_smem((const void*)k_cols_conv, d->smem_cols)) ||
-      (rc = set_smem((const void*)k_cols_fwd, sizeof(double2) * (size_t)d->py))) {
+  if ((rc = set_smem((const void*)k_rows_fwd<kRowsNB, 8>, d->smem_rows)) ||
+      (rc = set_smem((const void*)k_rows_fwd<kRowsNB, 16>, d->smem_rows)) ||
+      (rc = set_smem((const void*)k_rows_inv<kRowsNB, 8>, d->smem_rows)) ||
+      (rc = set_smem((const void*)k_rows_inv<kRowsNB, 16>, d->smem_rows)) ||
+      (rc = set_smem((const void*)k_cols_conv<8>, d->smem_cols)) ||
+      (rc = set_smem((const void*)k_cols_conv<16>, d->smem_cols)) ||
+      (rc = set_smem((const void*)k_cols_fwd<8>, sizeof(double2) * (size_t)d->py)) ||
+      (rc = set_smem((const void*)k_cols_fwd<16>, sizeof(double2) * (size_t)d->py))) {
     demag_destroy(d);
     return rc;
   }
@@ -666,14 +702,13 @@ int demag_create(llg_ctx* c) {
   // spectra of all 9 components (real 2-D FFT: rows then columns)
   double2* spec = nullptr;
   LLG_CUDA_TRY(cudaMalloc(&spec, sizeof(double2) * 9 * (size_t)nspec));
-  const FftPlan fxp = d->fx.dev(), fyp = d->fy.dev();
   for (int k = 0; k < 9; k++) {
-    dim3 g1((d->py + 2 * kRowsNB - 1) / (2 * kRowsNB), 1);
-    k_rows_fwd<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, d->d_T + k * np, 0, d->px, d->py, nullptr,
-                                                              spec + k * nspec, d->py, d->hx);
-    LLG_CUDA_TRY(cudaPeekAtLastError());
-    k_cols_fwd<<<d->hx, kColThreads, sizeof(double2) * d->py, s>>>(fyp, spec + k * nspec, d->py, d->py, d->hx);
-    LLG_CUDA_TRY(cudaPeekAtLastError());
+    if ((rc = launch_rows_fwd(d, s, d->d_T + k * np, 0, d->px, d->py, nullptr, spec + k * nspec, d->py, 1)) ||
+        (rc = launch_cols_fwd(d, s, spec + k * nspec))) {
+      cudaFree(spec);
+      demag_destroy(d);
+      return rc;
+    }
   }
   const int nblk = 256;
   double* d_stats = nullptr;
@@ -716,46 +751,30 @@ int demag_apply_w(llg_ctx* c, const double* y, const double* w, double* h) {
     LLG_CUDA_TRY(cudaMemsetAsync(h, 0, sizeof(double) * 3 * (size_t)c->ncell, c->stream));
     return 0;
   }
-  cudaStream_t s = c->stream;
-  const FftPlan fxp = d->fx.dev(), fyp = d->fy.dev();
-  dim3 g1((d->ny + 2 * kRowsNB - 1) / (2 * kRowsNB), 3);
+  int rc;
   LLG_COUNT(KID_DEMAG_ROWS_FWD);
-  k_rows_fwd<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, y, (long long)c->ncell, d->ng, d->ny, w, d->d_S,
-                                                            d->ny, d->hx);
-  LLG_CUDA_TRY(cudaPeekAtLastError());
+  if ((rc = launch_rows_fwd(d, c->stream, y, (long long)c->ncell, d->ng, d->ny, w, d->d_S, d->ny, 3))) return rc;
   LLG_COUNT(KID_DEMAG_COLS);
-  k_cols_conv<<<d->hx, kColThreads, d->smem_cols, s>>>(fyp, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy,
-                                                       d->d_tzz, d->d_txy);
-  LLG_CUDA_TRY(cudaPeekAtLastError());
+  if ((rc = launch_cols_conv(d, c->stream))) return rc;
   LLG_COUNT(KID_DEMAG_ROWS_INV);
-  k_rows_inv<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, d->d_S, d->ny, d->ny, d->hx, h,
-                                                            (long long)c->ncell, d->ng);
-  LLG_CUDA_TRY(cudaPeekAtLastError());
-  return 0;
+  return launch_rows_inv(d, c->stream, h, (long long)c->ncell);
 }
 
 // one stage of the chain alone (profiling): 0 rows_fwd, 1 cols_conv, 2 rows_inv
 int demag_stage(llg_ctx* c, int stage, const double* y, double* h) {
   DemagPlan* d = c->demag;
   if (!d) return LLG_ERR_STATE;
-  cudaStream_t s = c->stream;
-  const FftPlan fxp = d->fx.dev(), fyp = d->fy.dev();
-  dim3 g1((d->ny + 2 * kRowsNB - 1) / (2 * kRowsNB), 3);
   if (stage == 0) {
     LLG_COUNT(KID_DEMAG_ROWS_FWD);
-    k_rows_fwd<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, y, (long long)c->ncell, d->ng, d->ny,
-                                                              c->p.windowed ? c->d_w : nullptr, d->d_S, d->ny, d->hx);
-  } else if (stage == 1) {
-    LLG_COUNT(KID_DEMAG_COLS);
-    k_cols_conv<<<d->hx, kColThreads, d->smem_cols, s>>>(fyp, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy,
-                                                         d->d_tzz, d->d_txy);
-  } else {
-    LLG_COUNT(KID_DEMAG_ROWS_INV);
-    k_rows_inv<kRowsNB><<<g1, kRowThreads, d->smem_rows, s>>>(fxp, d->d_S, d->ny, d->ny, d->hx, h,
-                                                              (long long)c->ncell, d->ng);
+    return launch_rows_fwd(d, c->stream, y, (long long)c->ncell, d->ng, d->ny, c->p.windowed ? c->d_w : nullptr,
+                           d->d_S, d->ny, 3);
   }
-  LLG_CUDA_TRY(cudaPeekAtLastError());
-  return 0;
+  if (stage == 1) {
+    LLG_COUNT(KID_DEMAG_COLS);
+    return launch_cols_conv(d, c->stream);
+  }
+  LLG_COUNT(KID_DEMAG_ROWS_INV);
+  return launch_rows_inv(d, c->stream, h, (long long)c->ncell);
 }
 
 int demag_dims(llg_ctx* c, int out[4]) {

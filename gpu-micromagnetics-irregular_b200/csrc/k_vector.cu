@@ -254,15 +254,20 @@ __global__ void k_scale_add_multi(int nv, CoefPack a, const double* __restrict__
     for (int k = 0; k < nv; k++) Z.p[k][i] = a.c[k] * xi + Y.p[k][i];
   }
 }
-// Pascal triangle (sign +1: predictor, -1: restore) over zn[0..q]
-__global__ void k_nordsieck(int q, MPtrPack zn, int sign, long long n) {
+// Pascal triangle (sign +1: predictor, -1: restore) over zn[0..Q], in registers
+template <int Q>
+__global__ void k_nordsieck(MPtrPack zn, int sign, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    double v[6];
-    for (int j = 0; j <= q; j++) v[j] = zn.p[j][i];
-    for (int k = 1; k <= q; k++)
-      for (int j = q; j >= k; j--) v[j - 1] = (sign > 0) ? v[j - 1] + v[j] : v[j - 1] - v[j];
-    for (int j = 0; j < q; j++) zn.p[j][i] = v[j];
+    double v[Q + 1];
+#pragma unroll
+    for (int j = 0; j <= Q; j++) v[j] = zn.p[j][i];
+#pragma unroll
+    for (int k = 1; k <= Q; k++)
+#pragma unroll
+      for (int j = Q; j >= k; j--) v[j - 1] = (sign > 0) ? v[j - 1] + v[j] : v[j - 1] - v[j];
+#pragma unroll
+    for (int j = 0; j < Q; j++) zn.p[j][i] = v[j];
   }
 }
 // zn[j] *= f_j for j = 1..q
@@ -404,7 +409,14 @@ int vnordsieck_shift(llg_ctx* c, int q, double* const* zn, int sign) {
   MPtrPack zp{};
   for (int j = 0; j <= q; j++) zp.p[j] = zn[j];
   LLG_COUNT(KID_ELEMWISE);
-  k_nordsieck<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(q, zp, sign, c->neq);
+  const int g = ew_grid(c, c->neq);
+  switch (q) {
+    case 1: k_nordsieck<1><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
+    case 2: k_nordsieck<2><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
+    case 3: k_nordsieck<3><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
+    case 4: k_nordsieck<4><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
+    default: k_nordsieck<5><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
+  }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

@@ -146,6 +146,8 @@ def test_demag_matches_oracle(oracle_lib, gpu, mode, ng, ny):
     assert rel_err(dh.cpu().numpy(), o.demag(y)) < 1e-11
     assert rel_err(np.array(ctx.demag_self_coupling()), np.array(o.demag_self())) < 1e-13
     for comp, dx, dyy in ((0, 0, 0), (4, 3, -2), (1, 2, 1), (8, -1, 0)):
+        if mode == llg.DEMAG_OPEN and (abs(dx) >= ng or abs(dyy) >= ny):
+            continue  # padding lines: never touched by the linear convolution
         assert abs(ctx.demag_tensor(comp, dx, dyy) - o.tensor(comp, dx, dyy)) < 1e-13
 
 
