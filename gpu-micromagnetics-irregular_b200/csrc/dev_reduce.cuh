@@ -1,0 +1,106 @@
+// dev_reduce.cuh — deterministic block/grid reductions shared by the vector
+// kernels (k_vector.cu) and the fused integrator kernels (k_fused.cu).
+// The block partition depends only on the vector length; blocks reduce with
+// warp shuffles in a fixed tree; the last block (atomic ticket) sums the
+// per-block partials in block order.
+#pragma once
+#include <math.h>
+#include "llg_internal.h"
+
+namespace {
+
+constexpr int RT = 256;         // threads per reduction block
+constexpr int RMAXB = 1024;     // max reduction blocks
+
+int red_blocks(long long n) {
+  long long b = (n + RT * 8 - 1) / (RT * 8);
+  if (b > RMAXB) b = RMAXB;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// block sum of K values per thread; result valid in thread 0
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* sm /* [K][RT/32] */) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const double s = warp_sum(v[k]);
+    if (lane == 0) sm[k * (RT / 32) + wid] = s;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double s = (lane < RT / 32) ? sm[k * (RT / 32) + lane] : 0.0;
+      s = warp_sum(s);
+      v[k] = s;
+    }
+  }
+}
+
+// Last-block finalisation: partials[k*nb + b]; out[k] = sum_b partials (fixed tree).
+template <int K>
+__device__ __forceinline__ void finalize(double* partials, int nb, unsigned int* counter, double* out,
+                                         int mode /*0 sum, 1 wrms with n, 2 max*/, double nrm,
+                                         const double (&mine)[K]) {
+  __shared__ bool last;
+  __shared__ double sm[K * (RT / 32)];
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) partials[k * nb + blockIdx.x] = mine[k];
+    __threadfence();
+    const unsigned int t = atomicAdd(counter, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    double s = (mode == 2) ? 0.0 : 0.0;
+    for (int b = threadIdx.x; b < nb; b += RT) {
+      const double pv = ((volatile double*)partials)[k * nb + b];
+      s = (mode == 2) ? fmax(s, pv) : s + pv;
+    }
+    v[k] = s;
+  }
+  if (mode == 2) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const double s = warp_max(v[k]);
+      if (lane == 0) sm[k * (RT / 32) + wid] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        double s = (lane < RT / 32) ? sm[k * (RT / 32) + lane] : 0.0;
+        v[k] = warp_max(s);
+      }
+    }
+  } else {
+    block_sum<K>(v, sm);
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) out[k] = (mode == 1) ? sqrt(v[k] / nrm) : v[k];
+    *counter = 0u;
+  }
+}
+
+
+}  // namespace

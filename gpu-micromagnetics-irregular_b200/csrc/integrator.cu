@@ -11,10 +11,14 @@
 //
 // All vectors live in HBM; every vector update is one kernel on the
 // context's stream.  Scalars (norms, Gram–Schmidt coefficients) come back
-// through one pinned 8-byte copy per decision point.  The Arnoldi step
+// through one pinned copy per decision point.  The Arnoldi step
 // (ewt-scaling, Jv, subtraction, block-Jacobi solve, rescaling) is one fused
 // kernel (launch_arnoldi_op) instead of the five separate passes of the
-// reference's SPGMR + callbacks.
+// reference's SPGMR + callbacks; the Newton residual, the first Krylov
+// vector, the Gram–Schmidt update, the correction update and the
+// tolerance weights each carry their norm in the same pass (k_fused.cu).
+// The Newton correction starts as an implicit zero (ycor_zero) instead of a
+// cleared vector.
 #include <float.h>
 #include <math.h>
 #include <string.h>
@@ -56,9 +60,8 @@ struct Integrator {
   int qmax = 5, maxl = 5, classical_gs = 1, mxstep = 500;
   double rtol = 1e-4, atol = 1e-6;
   double* zn[QMAXL + 1] = {};
-  double *ewt = nullptr, *acor = nullptr, *y = nullptr, *tempv = nullptr, *ftemp = nullptr, *delta = nullptr;
+  double *ewt = nullptr, *acor = nullptr, *y = nullptr, *tempv = nullptr, *delta = nullptr;
   double* V[MAXLL + 1] = {};
-  double *xcor = nullptr, *vtemp = nullptr;
   double Hes[MAXLL + 1][MAXLL] = {}, givens[2 * MAXLL] = {}, yg[MAXLL + 1] = {};
   double tn = 0, h = 0, hscale = 0, hprime = 0, next_h = 0, eta = 1, etamax = ETAMX1, hu = 0, hmin = 0,
          hmax_inv = 0;
@@ -70,6 +73,7 @@ struct Integrator {
   long long nst = 0, nfe = 0, nsetups = 0, nni = 0, ncfn = 0, netf = 0, nli = 0, nlcf = 0, njv = 0, nps = 0,
             npe = 0, nstlp = 0, nstlj = 0, nscon = 0;
   int err = 0;  // sticky CUDA/launch failure
+  bool ycor_zero = false;  // acor holds the zero vector implicitly (not yet written)
 
   // ── helpers ──
   bool ok(int rc) {
@@ -80,6 +84,11 @@ struct Integrator {
     double r = 0.0;
     if (ok(vwrms_dev(c, x, ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 1, &r));
     return r;
+  }
+  // sqrt(s/neq) of raw sums: the same arithmetic as the device-side wrms
+  double wrms_of(double s) const { return sqrt(s / (double)neq); }
+  void materialise_acor() {
+    if (ycor_zero) { ok(vconst(c, 0.0, acor)); ycor_zero = false; }
   }
   double dot(const double* x, const double* yv) {
     double r = 0.0;
@@ -112,15 +121,16 @@ struct Integrator {
       cf[0] = 1.0;
       X[0] = V[k];
       for (int i = 0; i < k; i++) { Hes[i][k - 1] = dots[i]; cf[i + 1] = -dots[i]; X[i + 1] = V[i]; }
-      ok(vlincomb(c, k + 1, cf, X, V[k]));
-      double nrm = sqrt(dot(V[k], V[k]));
+      double ss = 0.0;
+      if (ok(fused_lincomb_norm(c, k + 1, cf, X, V[k], SLOT_DOTS))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
+      double nrm = sqrt(ss);
       if (GS_FACTOR * nrm < vk_norm) {
         if (ok(vdot_multi_dev(c, k, V[k], Y.data(), SLOT_DOTS))) ok(fetch_scalars(c, SLOT_DOTS, k, dots));
         cf[0] = 1.0;
         X[0] = V[k];
         for (int i = 0; i < k; i++) { Hes[i][k - 1] += dots[i]; cf[i + 1] = -dots[i]; X[i + 1] = V[i]; }
-        ok(vlincomb(c, k + 1, cf, X, V[k]));
-        nrm = sqrt(dot(V[k], V[k]));
+        if (ok(fused_lincomb_norm(c, k + 1, cf, X, V[k], SLOT_DOTS))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
+        nrm = sqrt(ss);
       }
       return nrm;
     }
@@ -189,12 +199,12 @@ struct Integrator {
     const int lmax = maxl;
     int nl = 0, krydim = 0, converged = 0;
     nps++;
-    if (!ok(launch_psolve(c, rhs, vtemp))) return LS_CONV_FAIL;
-    ok(vprod(c, ewt, vtemp, V[0]));
-    const double beta = sqrt(dot(V[0], V[0]));
+    double ss = 0.0;
+    if (!ok(fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A))) return LS_CONV_FAIL;
+    ok(fetch_scalars(c, SLOT_A, 1, &ss));
+    const double beta = sqrt(ss);
     double rnorm = beta, rho = beta;
     if (rnorm <= delta_tol) { ok(vconst(c, 0.0, rhs)); return LS_SUCCESS; }
-    ok(vconst(c, 0.0, xcor));
     for (int i = 0; i <= lmax; i++)
       for (int j = 0; j < lmax; j++) Hes[i][j] = 0.0;
     double rot = 1.0;
@@ -216,16 +226,12 @@ struct Integrator {
     yg[0] = rnorm;
     for (int i = 1; i <= krydim; i++) yg[i] = 0.0;
     if (qr_sol(krydim, yg) != 0) return LS_QRSOL_FAIL;
-    {
-      double cf[MAXLL + 1];
-      const double* X[MAXLL + 1];
-      cf[0] = 1.0;
-      X[0] = xcor;
-      for (int k = 0; k < krydim; k++) { cf[k + 1] = yg[k]; X[k + 1] = V[k]; }
-      ok(vlincomb(c, krydim + 1, cf, X, xcor));
-    }
     if (converged || rho < beta) {
-      ok(vdiv(c, xcor, ewt, rhs));
+      // x = 0 + sum_k yg_k V_k, then x / ewt; 0 + a*b is a*b exactly, so the
+      // zero initial guess needs no pass of its own
+      const double* X[MAXLL + 1];
+      for (int k = 0; k < krydim; k++) X[k] = V[k];
+      ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs));
       return converged ? LS_SUCCESS : LS_RES_REDUCED;
     }
     return LS_CONV_FAIL;
@@ -347,14 +353,16 @@ struct Integrator {
     rescale();
   }
 
-  int nls_residual(const double* ycor, double* res) {
-    ok(vlin(c, 1.0, zn[0], 1.0, ycor, y));
-    const int r = call_f(tn, y, ftemp);
-    if (r < 0) return LLG_CV_RHSFUNC_FAIL;
-    if (r > 0) return 1;
-    ok(vlin(c, rl1, zn[1], 1.0, ycor, res));
-    ok(vlin(c, -gamma, ftemp, 1.0, res, res));
-    return err ? LLG_CV_RHSFUNC_FAIL : 0;
+  // y = zn0 + ycor, f(y) (normalising y in place), and the NEGATED Newton
+  // residual  -(rl1 zn1 + ycor - gamma f(y))  in the RHS kernel's epilogue.
+  int nls_residual(const double* ycor, double* negres) {
+    nfe++;
+    const double* yc = ycor_zero ? nullptr : ycor;
+    int r = fused_lin_normalize(c, zn[0], yc, y);
+    if (!r) r = fused_field(c, y);
+    if (!r) r = fused_resid(c, y, zn[1], yc, rl1, gamma, negres);
+    if (r) { err = r; return LLG_CV_RHSFUNC_FAIL; }
+    return 0;
   }
   int nls_lsetup(int jbad) {
     if (jbad) convfail = CV_FAIL_BAD_J;
@@ -383,15 +391,16 @@ struct Integrator {
     if (r == LS_RES_REDUCED) return (ls_curiter == 0) ? 0 : 1;
     return 1;
   }
-  int nls_ctest(const double* ycor, const double* del, double tol, int m) {
-    const double dn = wrms(del);
+  // s[0], s[1]: raw weighted sums of squares of del and of the updated ycor
+  int nls_ctest(const double s[2], double tol, int m) {
+    const double dn = wrms_of(s[0]);
     if (m > 0) {
       const double r = dn / delp;
       crate = (CRDOWN * crate > r) ? CRDOWN * crate : r;
     }
     const double dcon = dn * (crate < 1.0 ? crate : 1.0) / tol;
     if (dcon <= 1.0) {
-      acnrm = (m == 0) ? dn : wrms(ycor);
+      acnrm = (m == 0) ? dn : wrms_of(s[1]);
       return 0;
     }
     if ((m >= 1) && (dn > RDIV * delp)) return NLS_CONV_RECVR;
@@ -412,12 +421,13 @@ struct Integrator {
       int m = 0;
       for (;;) {
         nni++;
-        ok(vscale(c, -1.0, del, del));
         ls_curiter = m;
         retval = nls_lsolve(del);
         if (retval != 0) break;
-        ok(vlin(c, 1.0, ycor, 1.0, del, ycor));
-        retval = nls_ctest(ycor, del, tq[4], m);
+        double s[2] = {0.0, 0.0};
+        if (ok(fused_update_wrms2(c, ycor_zero, ycor, del, ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 2, s));
+        ycor_zero = false;
+        retval = nls_ctest(s, tq[4], m);
         if (err) return LLG_CV_LSOLVE_FAIL;
         if (retval == 0) { jcur_nls = 0; return 0; }
         if (retval != NLS_CONTINUE) break;
@@ -429,7 +439,7 @@ struct Integrator {
       if (retval > 0 && !jcur_nls) {
         call_setup = 1;
         jbad = 1;
-        ok(vconst(c, 0.0, ycor));
+        ycor_zero = true;
         continue;
       }
       break;
@@ -440,10 +450,10 @@ struct Integrator {
     convfail = ((nflag == FIRST_CALL) || (nflag == PREV_ERR_FAIL)) ? CV_NO_FAILURES : CV_FAIL_OTHER;
     const int call_setup = (nflag == PREV_CONV_FAIL) || (nflag == PREV_ERR_FAIL) || (nst == 0) ||
                            (nst >= nstlp + MSBP) || (fabs(gamrat - 1.0) > DGMAX);
-    ok(vconst(c, 0.0, acor));
+    ycor_zero = true;
     const int flag = newton(call_setup);
-    ok(vlin(c, 1.0, zn[0], 1.0, acor, y));
-    if (flag != 0) return flag;
+    // (CVODE also forms y = zn0 + acor here; nothing in this integrator reads it)
+    if (flag != 0) { materialise_acor(); return flag; }
     jcur = 0;
     return 0;
   }
@@ -574,8 +584,19 @@ struct Integrator {
       return;
     }
     qwait = 2;
-    etaqm1 = eta_qm1();
-    etaqp1 = eta_qp1();
+    if (q > 1 && q != qmax && saved_tq5 != 0.0) {
+      // both order-change norms in one pass
+      const double cquot = (tq[5] / saved_tq5) * powi(h / tau[2], L);
+      double s[2] = {0.0, 0.0};
+      if (ok(fused_wrms2(c, zn[q], -cquot, zn[qmax], 1.0, acor, ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 2, s));
+      const double ddn = wrms_of(s[0]) * tq[1];
+      etaqm1 = 1.0 / (powr(BIAS1 * ddn, 1.0 / q) + ADDON);
+      const double dup = wrms_of(s[1]) * tq[3];
+      etaqp1 = 1.0 / (powr(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
+    } else {
+      etaqm1 = eta_qm1();
+      etaqp1 = eta_qp1();
+    }
     choose_eta();
     set_eta();
   }
@@ -600,7 +621,7 @@ struct Integrator {
     complete_step();
     prepare_next(dsm);
     etamax = (nst <= SMALL_NST) ? ETAMX2 : ETAMX3;
-    ok(vscale(c, tq[2], acor, acor));
+    // (CVODE scales acor by tq[2] here for CVodeGetEstLocalErrors; not exposed)
     return err ? LLG_CV_RHSFUNC_FAIL : 0;
   }
   int get_dky(double t, double* dky) {
@@ -696,12 +717,17 @@ struct Integrator {
     for (;;) {
       next_h = h;
       next_q = q;
+      double nrm = 0.0;
       if (nst > 0) {
-        if (set_ewt(zn[0]) != 0) {
+        // new weights and ||zn0|| in one pass
+        double s[2] = {0.0, 0.0};
+        if (ok(fused_ewt_wrms(c, rtol, atol, zn[0], ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 2, s));
+        if (s[0] != 0.0) {
           cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
           *tret = tn;
           return LLG_CV_ILL_INPUT;
         }
+        nrm = wrms_of(s[1]);
       }
       if ((mxstep > 0) && (nstloc >= mxstep)) {
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
@@ -709,7 +735,7 @@ struct Integrator {
         llg_set_error("mxstep reached before tout");
         return LLG_CV_TOO_MUCH_WORK;
       }
-      const double nrm = wrms(zn[0]);
+      if (nst == 0) nrm = wrms(zn[0]);
       if (err) return LLG_CV_RHSFUNC_FAIL;
       if (!isfinite(nrm)) {
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
@@ -744,7 +770,7 @@ struct Integrator {
   void free_all() {
     for (auto& p : zn) { cudaFree(p); p = nullptr; }
     for (auto& p : V) { cudaFree(p); p = nullptr; }
-    double** vs[] = {&ewt, &acor, &y, &tempv, &ftemp, &delta, &xcor, &vtemp};
+    double** vs[] = {&ewt, &acor, &y, &tempv, &delta};
     for (auto pp : vs) { cudaFree(*pp); *pp = nullptr; }
   }
 };
@@ -769,7 +795,7 @@ int integrator_create(llg_ctx* c, double t0, const double* y0, const llg_solver_
   int rc = 0;
   for (int j = 0; j <= b->qmax && !rc; j++) rc = alloc(&b->zn[j]);
   for (int j = 0; j <= b->maxl && !rc; j++) rc = alloc(&b->V[j]);
-  double** vs[] = {&b->ewt, &b->acor, &b->y, &b->tempv, &b->ftemp, &b->delta, &b->xcor, &b->vtemp};
+  double** vs[] = {&b->ewt, &b->acor, &b->y, &b->tempv, &b->delta};
   for (auto pp : vs)
     if (!rc) rc = alloc(pp);
   if (rc) { b->free_all(); delete b; return rc; }

@@ -163,8 +163,16 @@ __device__ __forceinline__ void stockham_pass(double2* buf, const FftPlan& pl, i
       int q, jm;
       if (lg >= 0) { q = j >> lg; jm = j & (Ns - 1); }
       else { q = j / Ns; jm = j - q * Ns; }
+      if (Ns > 1 && jm != 0) {
+        // one table load per butterfly; higher powers in registers
+        const double2 w1 = twid<SIGN>(pl, jm * tstride);
+        double2 wr = w1;
 #pragma unroll
-      for (int r = 1; r < R; r++) v[u][r] = cmul(v[u][r], twid<SIGN>(pl, jm * r * tstride));
+        for (int r = 1; r < R; r++) {
+          v[u][r] = cmul(v[u][r], wr);
+          if (r + 1 < R) wr = cmul(wr, w1);
+        }
+      }
       dft_fixed<R, SIGN>(v[u]);
       const int ob = q * Ns * R + jm;
 #pragma unroll
@@ -262,8 +270,19 @@ __global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long 
 }
 
 // ── K2: column transform + tensor multiply + inverse column transform ─────
-// CTA = one x-frequency column; threadIdx.y = component.
-template <int EPT>
+// CTA = one x-frequency column; threadIdx.y = component.  The three spectrum
+// columns and (STAGE) this column's tensor spectra are fetched with
+// asynchronous 16-byte copies (cp.async) at entry, so the 40n-byte tensor
+// read overlaps the forward transform instead of stalling the multiply.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int EPT, bool STAGE>
 __global__ void k_cols_conv(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx,
                             const double* __restrict__ txx, const double* __restrict__ tyy,
                             const double* __restrict__ tzz, const double2* __restrict__ txy) {
@@ -273,15 +292,38 @@ __global__ void k_cols_conv(FftPlan pl, double2* __restrict__ S, int ld, int nro
   const int c = threadIdx.y;
   double2* buf = sm + c * n;
   double2* col = S + ((long long)c * Hx + kx) * ld;
-  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) buf[yy] = (yy < nrows) ? col[yy] : make_double2(0.0, 0.0);
+  const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const long long tb = (long long)kx * n;
+  double* sxx = reinterpret_cast<double*>(sm + 3 * n);
+  double* syy = sxx + n;
+  double* szz = syy + n;
+  double2* sxy = reinterpret_cast<double2*>(szz + n);
+  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) {
+    if (yy < nrows) cp_async16(&buf[yy], &col[yy]);
+    else buf[yy] = make_double2(0.0, 0.0);
+  }
+  cp_async_commit();
+  if (STAGE) {
+    const int h = n / 2;  // n even when staging: 16-byte pairs of doubles
+    for (int e = tid; e < 3 * h + n; e += T) {
+      if (e < h) cp_async16(&sxx[2 * e], &txx[tb + 2 * e]);
+      else if (e < 2 * h) cp_async16(&syy[2 * (e - h)], &tyy[tb + 2 * (e - h)]);
+      else if (e < 3 * h) cp_async16(&szz[2 * (e - 2 * h)], &tzz[tb + 2 * (e - 2 * h)]);
+      else cp_async16(&sxy[e - 3 * h], &txy[tb + (e - 3 * h)]);
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<1>();
   __syncthreads();
   fft_stockham<-1, EPT>(buf, pl);
-  const long long tb = (long long)kx * n;
-  const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+  cp_async_wait<0>();
+  __syncthreads();
   for (int ky = tid; ky < n; ky += T) {
     const double2 mx = sm[ky], my = sm[n + ky], mz = sm[2 * n + ky];
-    const double a = __ldg(&txx[tb + ky]), b = __ldg(&tyy[tb + ky]), d = __ldg(&tzz[tb + ky]);
-    const double2 xy = __ldg(&txy[tb + ky]);
+    double a, b, d;
+    double2 xy;
+    if (STAGE) { a = sxx[ky]; b = syy[ky]; d = szz[ky]; xy = sxy[ky]; }
+    else { a = __ldg(&txx[tb + ky]); b = __ldg(&tyy[tb + ky]); d = __ldg(&tzz[tb + ky]); xy = __ldg(&txy[tb + ky]); }
     const double2 hxy = cmul(xy, my), hyx = cmul(xy, mx);
     sm[ky] = make_double2(a * mx.x + hxy.x, a * mx.y + hxy.y);
     sm[n + ky] = make_double2(hyx.x + b * my.x, hyx.y + b * my.y);
@@ -483,7 +525,7 @@ __global__ void k_tensor_finish(const double2* __restrict__ Sxx, const double2* 
 }  // namespace
 
 // ── host side ───────────────────────────────────────────────────────────
-static constexpr int kRowsNB = 2;  // packed transforms per row-CTA (4 real rows)
+static constexpr int kRowsNB = 1;  // packed transforms per row-CTA (2 real rows)
 
 struct HostFft {
   int n = 0, tx = 32, ept = 8;
@@ -513,7 +555,8 @@ struct DemagPlan {
   double* d_tzz = nullptr;
   double2* d_txy = nullptr;
   double* d_T = nullptr;         // 9 real tensor components (kept for host queries)
-  size_t smem_rows = 0, smem_cols = 0;
+  size_t smem_rows = 0, smem_cols = 0, smem_cols_staged = 0;
+  bool stage_tensor = false;     // tensor column prefetched into shared memory
 };
 
 static int factorize(int n, std::vector<int>& rad) {
@@ -625,12 +668,15 @@ static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, double* h, long l
 static int launch_cols_conv(const DemagPlan* d, cudaStream_t s) {
   const FftPlan pl = d->fy.dev();
   const dim3 b(d->fy.tx, 3);
-  if (d->fy.ept == 8)
-    k_cols_conv<8><<<d->hx, b, d->smem_cols, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy, d->d_tzz,
-                                                  d->d_txy);
-  else
-    k_cols_conv<16><<<d->hx, b, d->smem_cols, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy, d->d_tzz,
-                                                   d->d_txy);
+  const size_t sm = d->stage_tensor ? d->smem_cols_staged : d->smem_cols;
+#define COLS_LAUNCH(E, ST) \
+  k_cols_conv<E, ST><<<d->hx, b, sm, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy)
+  if (d->fy.ept == 8) {
+    if (d->stage_tensor) COLS_LAUNCH(8, true); else COLS_LAUNCH(8, false);
+  } else {
+    if (d->stage_tensor) COLS_LAUNCH(16, true); else COLS_LAUNCH(16, false);
+  }
+#undef COLS_LAUNCH
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -661,6 +707,8 @@ int demag_create(llg_ctx* c) {
   if (rc) { demag_destroy(d); return rc; }
   d->smem_rows = sizeof(double2) * (size_t)kRowsNB * d->px;
   d->smem_cols = sizeof(double2) * 3 * (size_t)d->py;
+  d->smem_cols_staged = d->smem_cols + (size_t)40 * d->py;
+  d->stage_tensor = (d->py % 2 == 0) && d->smem_cols_staged <= 200 * 1024;
   if (d->smem_rows > 227 * 1024 || d->smem_cols > 227 * 1024 || d->fx.tx * kRowsNB > 1024 ||
       d->fy.tx * 3 > 1024) {
     llg_set_error("demag grid too large for the shared-memory transform");
@@ -671,8 +719,10 @@ int demag_create(llg_ctx* c) {
       (rc = set_smem((const void*)k_rows_fwd<kRowsNB, 16>, d->smem_rows)) ||
       (rc = set_smem((const void*)k_rows_inv<kRowsNB, 8>, d->smem_rows)) ||
       (rc = set_smem((const void*)k_rows_inv<kRowsNB, 16>, d->smem_rows)) ||
-      (rc = set_smem((const void*)k_cols_conv<8>, d->smem_cols)) ||
-      (rc = set_smem((const void*)k_cols_conv<16>, d->smem_cols)) ||
+      (rc = set_smem((const void*)k_cols_conv<8, false>, d->smem_cols)) ||
+      (rc = set_smem((const void*)k_cols_conv<16, false>, d->smem_cols)) ||
+      (d->stage_tensor && (rc = set_smem((const void*)k_cols_conv<8, true>, d->smem_cols_staged))) ||
+      (d->stage_tensor && (rc = set_smem((const void*)k_cols_conv<16, true>, d->smem_cols_staged))) ||
       (rc = set_smem((const void*)k_cols_fwd<8>, sizeof(double2) * (size_t)d->py)) ||
       (rc = set_smem((const void*)k_cols_fwd<16>, sizeof(double2) * (size_t)d->py))) {
     demag_destroy(d);

@@ -1,0 +1,342 @@
+// k_fused.cu — integrator-specific fused passes, sm_100a.
+//
+// CVODE drives the reference's callbacks through chains of N_Vector calls
+// (linear sums, scalings, dot products; src/irregular/2d_fft/2d_i2/2d_fft.cu
+// :648-724 and the SUNDIALS NVECTOR_CUDA kernels that show up as ~45 % of its
+// kernel time).  Each function here is one HBM pass that applies, element by
+// element, the same operations as a chain of those calls:
+//
+//   fused_ewt_wrms        ewt = 1/(rtol|y|+atol)  +  ||y||_wrms(ewt)
+//   fused_lin_normalize   y = zn0 + ycor, then the RHS's normalisation
+//   fused_field           the RHS's demag field for y (or zero)
+//   fused_resid           RHS f(y) and the Newton residual
+//                         −(−γ f + (rl1 zn1 + ycor)) in the epilogue
+//   fused_psolve_scale_dot  V0 = ewt ⊙ P⁻¹ r  +  V0·V0
+//   fused_lincomb_norm    z = Σ c_k X_k  +  z·z           (classical GS)
+//   fused_lincomb_div     z = (Σ c_k X_k) / w             (GMRES correction)
+//   fused_update_wrms2    ycor += del  +  ||del||, ||ycor|| (Newton test)
+//   fused_wrms2           ||x1||  and  ||a x2 + b x3||     (order selection)
+//
+// Reductions use the deterministic partition of dev_reduce.cuh; results land
+// in c->d_scal as raw sums (the host takes sqrt(s/neq)).
+#include <math.h>
+
+#include "dev_physics.cuh"
+#include "dev_reduce.cuh"
+#include "llg_internal.h"
+
+namespace {
+
+constexpr int FV = 17;
+struct CPack {
+  double c[FV];
+};
+struct XPack {
+  const double* p[FV];
+};
+
+int cell_blocks(int ncell) { return red_blocks(ncell); }
+
+__global__ void __launch_bounds__(RT) k_ewt_wrms(double rtol, double atol, const double* __restrict__ y,
+                                                 double* __restrict__ ewt, long long n, double* partials,
+                                                 unsigned int* counter, double* out) {
+  __shared__ double sm[2 * (RT / 32)];
+  double acc[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
+    const double yi = y[i];
+    const double t = rtol * fabs(yi) + atol;
+    if (!(t > 0.0)) acc[0] += 1.0;
+    const double w = 1.0 / t;
+    ewt[i] = w;
+    const double p = yi * w;
+    acc[1] += p * p;
+  }
+  block_sum<2>(acc, sm);
+  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
+// A null ycor stands for the zero vector (the Newton iteration's first
+// iterate); 1*x + 1*0 is x exactly, so the result is the same either way.
+__device__ __forceinline__ double ycor_at(const double* ycor, int i) { return ycor ? ycor[i] : 0.0; }
+
+__global__ void k_lin_normalize(const double* __restrict__ zn0, const double* __restrict__ ycor,
+                                double* __restrict__ y, int n, int kind, double eps) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double m1 = 1.0 * zn0[k] + 1.0 * ycor_at(ycor, k);
+    const double m2 = 1.0 * zn0[n + k] + 1.0 * ycor_at(ycor, n + k);
+    const double m3 = 1.0 * zn0[2 * n + k] + 1.0 * ycor_at(ycor, 2 * n + k);
+    double o1 = m1, o2 = m2, o3 = m3;
+    if (kind != LLG_NORM_NONE) {
+      const double ymp = sqrt(m1 * m1 + m2 * m2 + m3 * m3);
+      if (kind == LLG_NORM_REG) {
+        const double inv = 1.0 / (ymp + eps);
+        o1 = m1 * inv; o2 = m2 * inv; o3 = m3 * inv;
+      } else if (ymp > 1.0e-30) {
+        const double inv = 1.0 / ymp;
+        o1 = m1 * inv; o2 = m2 * inv; o3 = m3 * inv;
+      }
+    }
+    y[k] = o1; y[n + k] = o2; y[2 * n + k] = o3;
+  }
+}
+
+// RHS at y with the Newton residual epilogue; writes −res (the Newton
+// iteration's negated right-hand side) and no ydot.
+__global__ void __launch_bounds__(TX * TY) k_rhs_resid_tile(DevProblem P, const double* __restrict__ y,
+                                                            const double* __restrict__ hd,
+                                                            const double* __restrict__ zn1,
+                                                            const double* __restrict__ ycor, double rl1,
+                                                            double gamma, double* __restrict__ negres) {
+  __shared__ Tile<1> T;
+  const double* f[1] = {y};
+  load_tile<1>(P, T, f);
+  const int gi = blockIdx.x * TX + threadIdx.x, gj = blockIdx.y * TY + threadIdx.y;
+  if (gi >= P.ng || gj >= P.ny) return;
+  const int n = P.ncell, cell = gj * P.ng + gi;
+  const double m[3] = {y[cell], y[n + cell], y[2 * n + cell]};
+  double msk[3], nsk[3];
+  cell_axes(P, cell, msk, nsk);
+  double h[3];
+  tile_field(P, T.v[0], threadIdx.x + 1, threadIdx.y + 1, m, msk, nsk, h);
+#pragma unroll
+  for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+  double o[3];
+  llg_torque(P, m, h, gate_of(P, cell), o);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int i = a * n + cell;
+    const double t = rl1 * zn1[i] + 1.0 * ycor_at(ycor, i);
+    const double r = (-gamma) * o[a] + 1.0 * t;
+    negres[i] = -1.0 * r;
+  }
+}
+
+__global__ void k_rhs_resid_compact(DevProblem P, const double* __restrict__ y, const double* __restrict__ hd,
+                                    const int32_t* __restrict__ act_ids, int na,
+                                    const int32_t* __restrict__ inact_ids, int ni,
+                                    const double* __restrict__ zn1, const double* __restrict__ ycor, double rl1,
+                                    double gamma, double* __restrict__ negres) {
+  const int n = P.ncell;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na + ni; t += gridDim.x * blockDim.x) {
+    double o[3] = {0.0, 0.0, 0.0};
+    int cell;
+    if (t >= na) {
+      cell = inact_ids[t - na];
+    } else {
+      cell = act_ids[t];
+      const int gi = cell % P.ng, gj = cell / P.ng;
+      const double m[3] = {y[cell], y[n + cell], y[2 * n + cell]};
+      double msk[3], nsk[3];
+      cell_axes(P, cell, msk, nsk);
+      double h[3];
+      gather_field(P, y, gi, gj, m, msk, nsk, h);
+#pragma unroll
+      for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+      llg_torque(P, m, h, 1.0, o);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int i = a * n + cell;
+      const double tt = rl1 * zn1[i] + 1.0 * ycor_at(ycor, i);
+      const double r = (-gamma) * o[a] + 1.0 * tt;
+      negres[i] = -1.0 * r;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const double* __restrict__ pm,
+                                                         const double* __restrict__ ph,
+                                                         const double* __restrict__ r,
+                                                         const double* __restrict__ ewt, double* __restrict__ v0,
+                                                         double gamma, double* partials, unsigned int* counter,
+                                                         double* out) {
+  __shared__ double sm[RT / 32];
+  double acc[1] = {0.0};
+  const int n = P.ncell;
+  for (int k = blockIdx.x * RT + threadIdx.x; k < n; k += gridDim.x * RT) {
+    const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
+    const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
+    const double rr[3] = {r[k], r[n + k], r[2 * n + k]};
+    double msk[3], nsk[3];
+    cell_axes(P, k, msk, nsk);
+    const double ws = P.windowed ? P.w[k] : 1.0;
+    double Pi[9];
+    block_inverse(P, m, h, msk, ws, gamma, Pi);
+    double g = 1.0;
+    if (!P.windowed && P.act) g = P.act[k] ? 1.0 : 0.0;
+    const double z0 = g * (Pi[0] * rr[0] + Pi[1] * rr[1] + Pi[2] * rr[2]);
+    const double z1 = g * (Pi[3] * rr[0] + Pi[4] * rr[1] + Pi[5] * rr[2]);
+    const double z2 = g * (Pi[6] * rr[0] + Pi[7] * rr[1] + Pi[8] * rr[2]);
+    const double a0 = ewt[k] * z0, a1 = ewt[n + k] * z1, a2 = ewt[2 * n + k] * z2;
+    v0[k] = a0; v0[n + k] = a1; v0[2 * n + k] = a2;
+    acc[0] += a0 * a0;
+    acc[0] += a1 * a1;
+    acc[0] += a2 * a2;
+  }
+  block_sum<1>(acc, sm);
+  finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
+// z = c0 X0; z = c_k X_k + z (z may alias X0), and sum z^2
+__global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, double* z, long long n,
+                                                     double* partials, unsigned int* counter, double* out) {
+  __shared__ double sm[RT / 32];
+  double acc[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
+    double s = c.c[0] * X.p[0][i];
+    for (int k = 1; k < nv; k++) s = c.c[k] * X.p[k][i] + s;
+    z[i] = s;
+    acc[0] += s * s;
+  }
+  block_sum<1>(acc, sm);
+  finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
+__global__ void k_lincomb_div(int nv, CPack c, XPack X, const double* __restrict__ w, double* __restrict__ z,
+                              long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double s = c.c[0] * X.p[0][i];
+    for (int k = 1; k < nv; k++) s = c.c[k] * X.p[k][i] + s;
+    z[i] = s / w[i];
+  }
+}
+
+// ycor = 1*ycor + 1*del (ycor_in null: zero); sums (del*w)^2 and (ycor*w)^2
+__global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, double* ycor, const double* __restrict__ del,
+                                                     const double* __restrict__ w, long long n, double* partials,
+                                                     unsigned int* counter, double* out) {
+  __shared__ double sm[2 * (RT / 32)];
+  double acc[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
+    const double d = del[i];
+    const double yc = 1.0 * (ycor_in ? ycor_in[i] : 0.0) + 1.0 * d;
+    ycor[i] = yc;
+    const double wi = w[i];
+    const double p = d * wi, q = yc * wi;
+    acc[0] += p * p;
+    acc[1] += q * q;
+  }
+  block_sum<2>(acc, sm);
+  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
+// sums (x1*w)^2 and ((a x2 + b x3)*w)^2
+__global__ void __launch_bounds__(RT) k_wrms2(const double* __restrict__ x1, double a, const double* __restrict__ x2,
+                                              double b, const double* __restrict__ x3, const double* __restrict__ w,
+                                              long long n, double* partials, unsigned int* counter, double* out) {
+  __shared__ double sm[2 * (RT / 32)];
+  double acc[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
+    const double wi = w[i];
+    const double p = x1[i] * wi;
+    const double v = a * x2[i] + b * x3[i];
+    const double q = v * wi;
+    acc[0] += p * p;
+    acc[1] += q * q;
+  }
+  block_sum<2>(acc, sm);
+  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
+int ew_blocks(const llg_ctx* c, long long n) {
+  long long g = (n + 255) / 256;
+  const long long cap = (long long)c->num_sms * 8;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+}  // namespace
+
+int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot) {
+  LLG_COUNT(KID_REDUCE);
+  k_ewt_wrms<<<red_blocks(c->neq), RT, 0, c->stream>>>(rtol, atol, y, ewt, c->neq, c->d_red, c->d_counter,
+                                                       c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor, double* y) {
+  LLG_COUNT(KID_NORM);
+  k_lin_normalize<<<ew_blocks(c, c->ncell), 256, 0, c->stream>>>(zn0, ycor, y, c->ncell, c->p.norm_kind,
+                                                                c->p.norm_eps);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_field(llg_ctx* c, const double* y) {
+  if (c->demag) {
+    const int rc = demag_apply(c, y, c->d_hd);
+    if (rc) return rc;
+    c->nfe_demag++;
+    return 0;
+  }
+  LLG_CUDA_TRY(cudaMemsetAsync(c->d_hd, 0, sizeof(double) * 3 * (size_t)c->ncell, c->stream));
+  return 0;
+}
+
+int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* ycor, double rl1, double gamma,
+                double* negres) {
+  LLG_COUNT(KID_RHS);
+  if (c->p.exec_model == LLG_EXEC_COMPACT) {
+    const int tot = c->n_active + c->n_inactive;
+    k_rhs_resid_compact<<<ew_blocks(c, tot), 256, 0, c->stream>>>(c->dp, y, c->d_hd, c->d_active_ids, c->n_active,
+                                                                   c->d_inactive_ids, c->n_inactive, zn1, ycor, rl1,
+                                                                   gamma, negres);
+  } else {
+    dim3 g((c->p.ng + TX - 1) / TX, (c->p.ny + TY - 1) / TY);
+    k_rhs_resid_tile<<<g, dim3(TX, TY), 0, c->stream>>>(c->dp, y, c->d_hd, zn1, ycor, rl1, gamma, negres);
+  }
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot) {
+  if (!c->have_setup) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
+  LLG_COUNT(KID_PSOLVE);
+  k_psolve_scale_dot<<<cell_blocks(c->ncell), RT, 0, c->stream>>>(c->dp, c->d_pm, c->d_ph, r, ewt, v0,
+                                                                  c->gamma_setup, c->d_red, c->d_counter,
+                                                                  c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot) {
+  if (nv < 1 || nv > FV) { llg_set_error("lincomb_norm: bad nvec"); return LLG_ERR_ARG; }
+  CPack cp{};
+  XPack xp{};
+  for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
+  LLG_COUNT(KID_REDUCE);
+  k_lincomb_norm<<<red_blocks(c->neq), RT, 0, c->stream>>>(nv, cp, xp, z, c->neq, c->d_red, c->d_counter,
+                                                           c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z) {
+  if (nv < 1 || nv > FV) { llg_set_error("lincomb_div: bad nvec"); return LLG_ERR_ARG; }
+  CPack cp{};
+  XPack xp{};
+  for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
+  LLG_COUNT(KID_ELEMWISE);
+  k_lincomb_div<<<ew_blocks(c, c->neq), 256, 0, c->stream>>>(nv, cp, xp, w, z, c->neq);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot) {
+  LLG_COUNT(KID_REDUCE);
+  k_update_wrms2<<<red_blocks(c->neq), RT, 0, c->stream>>>(ycor_zero ? nullptr : ycor, ycor, del, w, c->neq, c->d_red, c->d_counter,
+                                                           c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double b, const double* x3,
+                const double* w, int slot) {
+  LLG_COUNT(KID_REDUCE);
+  k_wrms2<<<red_blocks(c->neq), RT, 0, c->stream>>>(x1, a, x2, b, x3, w, c->neq, c->d_red, c->d_counter,
+                                                    c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}

@@ -148,3 +148,16 @@ int vscale_columns(llg_ctx* c, int q, double eta, double* const* zn);
 int vset_ewt(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot);
 int vhin_bound(llg_ctx* c, double rtol, double atol, const double* y0, const double* f0,
                double* tmp);
+
+// fused integrator passes (k_fused.cu); reductions leave raw sums in d_scal[slot..]
+int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot);
+int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor /* null: zero */, double* y);
+int fused_field(llg_ctx* c, const double* y);
+int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* ycor /* null: zero */, double rl1,
+                double gamma, double* negres);
+int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot);
+int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot);
+int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z);
+int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot);
+int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double b, const double* x3,
+                const double* w, int slot);
