@@ -1,0 +1,121 @@
+// dev_tc.cuh — thin inline-PTX helpers for the 5th-generation tensor cores
+// (tcgen05: MMA from shared-memory descriptors into tensor memory, TMEM
+// allocation and loads) and mbarriers, sm_100a only.
+//
+// Shared-memory operand layout (no swizzle): an operand is tiled into "core
+// matrices" of 8 x 16 bytes stored as 128 contiguous bytes.  K-major: the 8
+// rows are 8 M (or N) indices, each 16-byte row holds 8 consecutive K
+// elements.  MN-major: the 8 rows are 8 K indices, each holding 8
+// consecutive M elements.  LBO = byte distance between core matrices along
+// K, SBO = along M/N.  For 16-bit elements:
+//   K-major  (r, k): (r/8)*SBO + (k/8)*LBO + (r%8)*16 + (k%8)*2
+//   MN-major (m, k): (m/8)*SBO + (k/8)*LBO + (k%8)*16 + (m%8)*2
+#pragma once
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace {
+
+__host__ __device__ constexpr uint32_t off_kmajor(int r, int k, int lbo, int sbo) {
+  return (uint32_t)((r >> 3) * sbo + (k >> 3) * lbo + (r & 7) * 16 + (k & 7) * 2);
+}
+__host__ __device__ constexpr uint32_t off_mnmajor(int m, int k, int lbo, int sbo) {
+  return (uint32_t)((m >> 3) * sbo + (k >> 3) * lbo + (k & 7) * 16 + (m & 7) * 2);
+}
+
+// shared-memory matrix descriptor: start address, LBO, SBO (all >> 4),
+// version 1 (bits 46-47), base offset 0, no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor, kind::f16: D f32 (bits 4-5 = 1), A and B f16
+// (bits 7-9, 10-12 = 0), A/B major (bits 15, 16), N>>3 (bits 17-22),
+// M>>4 (bits 24-28)
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N, int a_mn_major, int b_mn_major) {
+  return (1u << 4) | ((uint32_t)a_mn_major << 15) | ((uint32_t)b_mn_major << 16) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// ── TMEM allocation (one full warp) ──
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(slot_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// D[tmem] (+)= A[smem desc] * B[smem desc]^T, issued by one thread
+__device__ __forceinline__ void tc_mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// arrive on the mbarrier once all previously issued MMAs of this thread complete
+__device__ __forceinline__ void tc_commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+// 32 lanes x 16 consecutive 32-bit columns: thread i gets lane (base + i)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// ── mbarrier ──
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// bounded wait for the phase with the given parity; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit) {
+  const uint32_t a = smem_u32(mbar);
+  for (uint32_t it = 0; it < limit; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// FP32 -> FP16 hi + FP16 lo' with v ~ hi + 2^-11 lo' (to ~2^-22 relative).
+// The remainder is stored scaled up by 2^11 so it stays a normal FP16
+// number (an unscaled remainder of a value below ~0.1 would be subnormal).
+constexpr float LO_SCALE = 2048.f, LO_UNSCALE = 1.f / 2048.f;
+__device__ __forceinline__ void split_h(float v, __half& hi, __half& lo) {
+  hi = __float2half_rn(v);
+  lo = __float2half_rn((v - __half2float(hi)) * LO_SCALE);
+}
+
+}  // namespace

@@ -33,209 +33,37 @@
 #include <algorithm>
 #include <vector>
 
+#include "dev_fft.cuh"
 #include "llg_internal.h"
 
 namespace {
 
-constexpr int MAXR = 24;  // passes
+using FftPlan = FftPlanT<double>;
 
-// Stockham plan for one transform length n.  Radices in pass order
-// (8/4/2 first so every power-of-two pass sees a power-of-two span Ns, then
-// 3, 5 and any other prime).  tx = threads per transform.
-struct FftPlan {
-  int n, nr, tx;
-  const int4* pass;  // per pass: (radix R, span Ns before the pass, log2 Ns or -1, 0)
-  const double2* tw; // tw[k] = exp(-2 pi i k / n)
-};
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// 16-byte (cg) or 8-byte (ca) asynchronous global->shared copy
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (BYTES == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-// v * (SIGN < 0 ? -i : +i)
-template <int SIGN>
-__device__ __forceinline__ double2 rot90(double2 v) {
-  return (SIGN < 0) ? make_double2(v.y, -v.x) : make_double2(-v.y, v.x);
-}
-
-template <int SIGN>
-__device__ __forceinline__ double2 twid(const FftPlan& pl, int idx) {
-  double2 w = __ldg(&pl.tw[idx]);
-  if (SIGN > 0) w.y = -w.y;
-  return w;
-}
-
-// in-register DFTs, out[q] = sum_r v[r] exp(SIGN 2 pi i r q / R)
-template <int SIGN>
-__device__ __forceinline__ void dft2(double2* v) {
-  const double2 a = v[0], b = v[1];
-  v[0] = cadd(a, b);
-  v[1] = csub(a, b);
-}
-template <int SIGN>
-__device__ __forceinline__ void dft4(double2* v) {
-  const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-  const double2 b0 = cadd(v[1], v[3]), b1 = rot90<SIGN>(csub(v[1], v[3]));
-  v[0] = cadd(a0, b0);
-  v[2] = csub(a0, b0);
-  v[1] = cadd(a1, b1);
-  v[3] = csub(a1, b1);
-}
-template <int SIGN>
-__device__ __forceinline__ void dft3(double2* v) {
-  const double c = -0.5, s = SIGN * 0.86602540378443864676;  // sin(2pi/3)
-  const double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
-  const double2 a = make_double2(v[0].x + c * t1.x, v[0].y + c * t1.y);
-  const double2 b = make_double2(-s * t2.y, s * t2.x);  // i*s*t2
-  v[0] = cadd(v[0], t1);
-  v[1] = cadd(a, b);
-  v[2] = csub(a, b);
-}
-template <int SIGN>
-__device__ __forceinline__ void dft5(double2* v) {
-  const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-  const double s1 = SIGN * 0.95105651629515357212, s2 = SIGN * 0.58778525229247312917;
-  const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-  const double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-  const double2 a1 = make_double2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
-  const double2 a2 = make_double2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
-  const double2 b1 = make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
-  const double2 b2 = make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
-  v[0] = make_double2(v[0].x + t1.x + t2.x, v[0].y + t1.y + t2.y);
-  v[1] = make_double2(a1.x - b1.y, a1.y + b1.x);
-  v[4] = make_double2(a1.x + b1.y, a1.y - b1.x);
-  v[2] = make_double2(a2.x - b2.y, a2.y + b2.x);
-  v[3] = make_double2(a2.x + b2.y, a2.y - b2.x);
-}
-template <int SIGN>
-__device__ __forceinline__ void dft8(double2* v) {
-  const double h = 0.70710678118654752440;
-  double2 e[4] = {v[0], v[2], v[4], v[6]};
-  double2 o[4] = {v[1], v[3], v[5], v[7]};
-  dft4<SIGN>(e);
-  dft4<SIGN>(o);
-  const double2 o1 = make_double2(h * (o[1].x - SIGN * o[1].y), h * (o[1].y + SIGN * o[1].x));
-  const double2 o2 = rot90<SIGN>(o[2]);
-  const double2 o3 = make_double2(-h * (o[3].x + SIGN * o[3].y), h * (SIGN * o[3].x - o[3].y));
-  v[0] = cadd(e[0], o[0]);
-  v[4] = csub(e[0], o[0]);
-  v[1] = cadd(e[1], o1);
-  v[5] = csub(e[1], o1);
-  v[2] = cadd(e[2], o2);
-  v[6] = csub(e[2], o2);
-  v[3] = cadd(e[3], o3);
-  v[7] = csub(e[3], o3);
-}
-template <int R, int SIGN>
-__device__ __forceinline__ void dft_fixed(double2* v) {
-  if constexpr (R == 2) dft2<SIGN>(v);
-  else if constexpr (R == 3) dft3<SIGN>(v);
-  else if constexpr (R == 4) dft4<SIGN>(v);
-  else if constexpr (R == 5) dft5<SIGN>(v);
-  else if constexpr (R == 8) dft8<SIGN>(v);
-}
-
-// One Stockham pass of one transform held in buf[0..n).  All threads of the
-// row stage their butterflies in registers, the block synchronises, then
-// twiddle + DFT_R + scatter to (j / Ns)·Ns·R + j % Ns + r·Ns.
-// A row of tx threads covers n/R butterflies with at most MB each
-// (tx >= n/EPT is guaranteed by the plan).
-template <int R, int SIGN, int EPT>
-__device__ __forceinline__ void stockham_pass(double2* buf, const FftPlan& pl, int4 ps) {
-  constexpr int MB = (EPT + R - 1) / R;
-  const int n = pl.n, nb = n / R, Ns = ps.y, lg = ps.z;
-  const int tstride = n / (Ns * R);
-  double2 v[MB][R];
-#pragma unroll
-  for (int u = 0; u < MB; u++) {
-    const int j = threadIdx.x + u * blockDim.x;
-    if (j < nb) {
-#pragma unroll
-      for (int r = 0; r < R; r++) v[u][r] = buf[j + r * nb];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int u = 0; u < MB; u++) {
-    const int j = threadIdx.x + u * blockDim.x;
-    if (j < nb) {
-      int q, jm;
-      if (lg >= 0) { q = j >> lg; jm = j & (Ns - 1); }
-      else { q = j / Ns; jm = j - q * Ns; }
-      if (Ns > 1 && jm != 0) {
-        // one table load per butterfly; higher powers in registers
-        const double2 w1 = twid<SIGN>(pl, jm * tstride);
-        double2 wr = w1;
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-          v[u][r] = cmul(v[u][r], wr);
-          if (r + 1 < R) wr = cmul(wr, w1);
-        }
-      }
-      dft_fixed<R, SIGN>(v[u]);
-      const int ob = q * Ns * R + jm;
-#pragma unroll
-      for (int r = 0; r < R; r++) buf[ob + r * Ns] = v[u][r];
-    }
-  }
-  __syncthreads();
-}
-
-// Any other radix (small primes, test sizes only): one butterfly per thread
-// (the plan sizes tx >= n/R), R <= 64, O(R^2).
-template <int SIGN>
-__device__ void stockham_pass_generic(double2* buf, const FftPlan& pl, int4 ps) {
-  const int R = ps.x;
-  const int n = pl.n, nb = n / R, Ns = ps.y;
-  const int tstride = n / (Ns * R), rstride = n / R;
-  const int j = threadIdx.x;
-  double2 v[64];
-  if (j < nb) {
-    for (int r = 0; r < R; r++) v[r] = buf[j + r * nb];
-  }
-  __syncthreads();
-  if (j < nb) {
-    const int q = j / Ns, jm = j - q * Ns;
-    for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<SIGN>(pl, jm * r * tstride));
-    const int ob = q * Ns * R + jm;
-    for (int k = 0; k < R; k++) {
-      double2 acc = v[0];
-      for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid<SIGN>(pl, ((r * k) % R) * rstride)));
-      buf[ob + k * Ns] = acc;
-    }
-  }
-  __syncthreads();
-}
-
-// Natural-order in, natural-order out, in place in buf (this row's transform).
-// Every thread of the block must call it (it synchronises).  The passes run
-// as straight-line regions in factorisation order (8s, one 4, one 2, 3s, 5s,
-// other primes): a runtime switch over radices inside one loop makes the
-// register allocator keep every variant's state live at once.
-template <int SIGN, int EPT>
-__device__ void fft_stockham(double2* buf, const FftPlan& pl) {
-  int p = 0;
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<8, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
-  if (p < pl.nr && __ldg(&pl.pass[p].x) == 4) { stockham_pass<4, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  if (p < pl.nr && __ldg(&pl.pass[p].x) == 2) { stockham_pass<2, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<3, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<5, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pl.nr; p++) stockham_pass_generic<SIGN>(buf, pl, __ldg(&pl.pass[p]));
-}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // ── K1: forward real transform of data rows along x ─────────────────────
 // CTA = (component c, 2*NB rows); threadIdx.y = packed transform (rows ya, ya+1).
-template <int NB, int EPT>
-__global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long comp_stride, int row_len,
-                           int nrows, const double* __restrict__ w, double2* __restrict__ S, int ld,
-                           int Hx) {
-  extern __shared__ double2 sm[];
+// The FP64 input is rounded to R on load (R = float: mixed chain).
+template <typename R, int NB, int EPT>
+__global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long long comp_stride, int row_len,
+                           int nrows, const double* __restrict__ w, cx_t<R>* __restrict__ S, int ld, int Hx) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx_t<R>* sm = reinterpret_cast<cx_t<R>*>(smraw);
   const int c = blockIdx.y;
   const int y0 = blockIdx.x * (2 * NB);
   const int n = pl.n;
   const int b = threadIdx.y;
-  double2* buf = sm + b * n;
+  cx_t<R>* buf = sm + b * n;
   const double* src = in + (long long)c * comp_stride;
   const int ya = y0 + 2 * b, yb = ya + 1;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -250,21 +78,21 @@ __global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long 
         vb = src[q] * (w ? w[q] : 1.0);
       }
     }
-    buf[i] = make_double2(va, vb);
+    buf[i] = mk<R>((R)va, (R)vb);
   }
   __syncthreads();
-  fft_stockham<-1, EPT>(buf, pl);
+  fft_stockham<R, -1, EPT>(buf, pl);
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int e = tid; e < Hx * 2 * NB; e += T) {
     const int kx = e / (2 * NB), r = e - kx * (2 * NB);
     const int bb = r >> 1, which = r & 1;
     const int y = y0 + r;
     if (y >= nrows) continue;
-    const double2 zk = sm[bb * n + kx];
-    const double2 zm = sm[bb * n + ((n - kx) % n)];
-    double2 out;
-    if (!which) out = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
-    else out = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+    const cx_t<R> zk = sm[bb * n + kx];
+    const cx_t<R> zm = sm[bb * n + ((n - kx) % n)];
+    cx_t<R> out;
+    if (!which) out = mk<R>(R(0.5) * (zk.x + zm.x), R(0.5) * (zk.y - zm.y));
+    else out = mk<R>(R(0.5) * (zk.y + zm.y), R(-0.5) * (zk.x - zm.x));
     S[((long long)c * Hx + kx) * ld + y] = out;
   }
 }
@@ -272,113 +100,111 @@ __global__ void k_rows_fwd(FftPlan pl, const double* __restrict__ in, long long 
 // ── K2: column transform + tensor multiply + inverse column transform ─────
 // CTA = one x-frequency column; threadIdx.y = component.  The three spectrum
 // columns and (STAGE) this column's tensor spectra are fetched with
-// asynchronous 16-byte copies (cp.async) at entry, so the 40n-byte tensor
-// read overlaps the forward transform instead of stalling the multiply.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-template <int EPT, bool STAGE>
-__global__ void k_cols_conv(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx,
-                            const double* __restrict__ txx, const double* __restrict__ tyy,
-                            const double* __restrict__ tzz, const double2* __restrict__ txy) {
-  extern __shared__ double2 sm[];
+// asynchronous copies (cp.async) at entry, so the tensor read overlaps the
+// forward transform instead of stalling the multiply.
+template <typename R, int EPT, bool STAGE>
+__global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
+                            const R* __restrict__ txx, const R* __restrict__ tyy, const R* __restrict__ tzz,
+                            const cx_t<R>* __restrict__ txy) {
+  using C = cx_t<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
   const int kx = blockIdx.x;
   const int n = pl.n;
   const int c = threadIdx.y;
-  double2* buf = sm + c * n;
-  double2* col = S + ((long long)c * Hx + kx) * ld;
+  C* buf = sm + c * n;
+  C* col = S + ((long long)c * Hx + kx) * ld;
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   const long long tb = (long long)kx * n;
-  double* sxx = reinterpret_cast<double*>(sm + 3 * n);
-  double* syy = sxx + n;
-  double* szz = syy + n;
-  double2* sxy = reinterpret_cast<double2*>(szz + n);
+  R* sxx = reinterpret_cast<R*>(sm + 3 * n);
+  R* syy = sxx + n;
+  R* szz = syy + n;
+  C* sxy = reinterpret_cast<C*>(szz + n);
   for (int yy = threadIdx.x; yy < n; yy += blockDim.x) {
-    if (yy < nrows) cp_async16(&buf[yy], &col[yy]);
-    else buf[yy] = make_double2(0.0, 0.0);
+    if (yy < nrows) cp_async<sizeof(C)>(&buf[yy], &col[yy]);
+    else buf[yy] = mk<R>(R(0), R(0));
   }
   cp_async_commit();
   if (STAGE) {
-    const int h = n / 2;  // n even when staging: 16-byte pairs of doubles
-    for (int e = tid; e < 3 * h + n; e += T) {
-      if (e < h) cp_async16(&sxx[2 * e], &txx[tb + 2 * e]);
-      else if (e < 2 * h) cp_async16(&syy[2 * (e - h)], &tyy[tb + 2 * (e - h)]);
-      else if (e < 3 * h) cp_async16(&szz[2 * (e - 2 * h)], &tzz[tb + 2 * (e - 2 * h)]);
-      else cp_async16(&sxy[e - 3 * h], &txy[tb + (e - 3 * h)]);
+    constexpr int PR = 16 / sizeof(R), PC = 16 / sizeof(C);  // elements per 16-byte copy
+    const int hr = n / PR, hc = n / PC;
+    for (int e = tid; e < 3 * hr + hc; e += T) {
+      if (e < hr) cp_async<16>(&sxx[PR * e], &txx[tb + PR * e]);
+      else if (e < 2 * hr) cp_async<16>(&syy[PR * (e - hr)], &tyy[tb + PR * (e - hr)]);
+      else if (e < 3 * hr) cp_async<16>(&szz[PR * (e - 2 * hr)], &tzz[tb + PR * (e - 2 * hr)]);
+      else cp_async<16>(&sxy[PC * (e - 3 * hr)], &txy[tb + PC * (e - 3 * hr)]);
     }
   }
   cp_async_commit();
   cp_async_wait<1>();
   __syncthreads();
-  fft_stockham<-1, EPT>(buf, pl);
+  fft_stockham<R, -1, EPT>(buf, pl);
   cp_async_wait<0>();
   __syncthreads();
   for (int ky = tid; ky < n; ky += T) {
-    const double2 mx = sm[ky], my = sm[n + ky], mz = sm[2 * n + ky];
-    double a, b, d;
-    double2 xy;
+    const C mx = sm[ky], my = sm[n + ky], mz = sm[2 * n + ky];
+    R a, b, d;
+    C xy;
     if (STAGE) { a = sxx[ky]; b = syy[ky]; d = szz[ky]; xy = sxy[ky]; }
     else { a = __ldg(&txx[tb + ky]); b = __ldg(&tyy[tb + ky]); d = __ldg(&tzz[tb + ky]); xy = __ldg(&txy[tb + ky]); }
-    const double2 hxy = cmul(xy, my), hyx = cmul(xy, mx);
-    sm[ky] = make_double2(a * mx.x + hxy.x, a * mx.y + hxy.y);
-    sm[n + ky] = make_double2(hyx.x + b * my.x, hyx.y + b * my.y);
-    sm[2 * n + ky] = make_double2(d * mz.x, d * mz.y);
+    const C hxy = cmul<R>(xy, my), hyx = cmul<R>(xy, mx);
+    sm[ky] = mk<R>(a * mx.x + hxy.x, a * mx.y + hxy.y);
+    sm[n + ky] = mk<R>(hyx.x + b * my.x, hyx.y + b * my.y);
+    sm[2 * n + ky] = mk<R>(d * mz.x, d * mz.y);
   }
   __syncthreads();
-  fft_stockham<+1, EPT>(buf, pl);
+  fft_stockham<R, +1, EPT>(buf, pl);
   for (int yy = threadIdx.x; yy < nrows; yy += blockDim.x) col[yy] = buf[yy];
 }
 
-// forward column transform only (tensor spectra at init)
+// forward column transform only (tensor spectra at init, FP64)
 template <int EPT>
 __global__ void k_cols_fwd(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx) {
-  extern __shared__ double2 sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* sm = reinterpret_cast<double2*>(smraw);
   const int kx = blockIdx.x;
   const int n = pl.n;
   double2* col = S + (long long)kx * ld;
   for (int yy = threadIdx.x; yy < n; yy += blockDim.x) sm[yy] = (yy < nrows) ? col[yy] : make_double2(0.0, 0.0);
   __syncthreads();
-  fft_stockham<-1, EPT>(sm, pl);
+  fft_stockham<double, -1, EPT>(sm, pl);
   for (int yy = threadIdx.x; yy < n; yy += blockDim.x) col[yy] = sm[yy];
 }
 
-// ── K3: inverse real transform along x, scatter to SoA h ─────────────────
-template <int NB, int EPT>
-__global__ void k_rows_inv(FftPlan pl, const double2* __restrict__ S, int ld, int nrows, int Hx,
+// ── K3: inverse real transform along x, scatter to SoA h (FP64) ──────────
+template <typename R, int NB, int EPT>
+__global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
                            double* __restrict__ h, long long comp_stride, int ng) {
-  extern __shared__ double2 sm[];
+  using C = cx_t<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
   const int c = blockIdx.y;
   const int y0 = blockIdx.x * (2 * NB);
   const int n = pl.n;
   const int b = threadIdx.y;
   const bool even = (n % 2) == 0;
   const int ya = y0 + 2 * b, yb = ya + 1;
-  double2* buf = sm + b * n;
+  C* buf = sm + b * n;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
     const int kk = (k < Hx) ? k : n - k;
-    double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
-    const double2* col = S + ((long long)c * Hx + kk) * ld;
+    C A = mk<R>(R(0), R(0)), B = mk<R>(R(0), R(0));
+    const C* col = S + ((long long)c * Hx + kk) * ld;
     if (ya < nrows) A = col[ya];
     if (yb < nrows) B = col[yb];
-    if (kk == 0 || (even && kk == n / 2)) { A.y = 0.0; B.y = 0.0; }
+    if (kk == 0 || (even && kk == n / 2)) { A.y = R(0); B.y = R(0); }
     if (k >= Hx) { A.y = -A.y; B.y = -B.y; }
-    buf[k] = make_double2(A.x - B.y, A.y + B.x);
+    buf[k] = mk<R>(A.x - B.y, A.y + B.x);
   }
   __syncthreads();
-  fft_stockham<+1, EPT>(buf, pl);
+  fft_stockham<R, +1, EPT>(buf, pl);
   double* dst = h + (long long)c * comp_stride;
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int e = tid; e < NB * 2 * ng; e += T) {
     const int r = e / ng, i = e - r * ng;
     const int y = y0 + r;
     if (y >= nrows) continue;
-    const double2 z = sm[(r >> 1) * n + i];
-    dst[(long long)y * ng + i] = (r & 1) ? z.y : z.x;
+    const C z = sm[(r >> 1) * n + i];
+    dst[(long long)y * ng + i] = (double)((r & 1) ? z.y : z.x);
   }
 }
 
@@ -531,14 +357,17 @@ struct HostFft {
   int n = 0, tx = 32, ept = 8;
   std::vector<int> radix;
   double2* d_tw = nullptr;
+  float2* d_twf = nullptr;   // FP32 twiddles (mixed chain)
   int4* d_pass = nullptr;
-  FftPlan dev() const {
-    FftPlan p{};
+  template <typename R>
+  FftPlanT<R> dev() const {
+    FftPlanT<R> p{};
     p.n = n;
     p.nr = (int)radix.size();
     p.tx = tx;
     p.pass = d_pass;
-    p.tw = d_tw;
+    if constexpr (sizeof(R) == 8) p.tw = d_tw;
+    else p.tw = d_twf;
     return p;
   }
 };
@@ -557,6 +386,16 @@ struct DemagPlan {
   double* d_T = nullptr;         // 9 real tensor components (kept for host queries)
   size_t smem_rows = 0, smem_cols = 0, smem_cols_staged = 0;
   bool stage_tensor = false;     // tensor column prefetched into shared memory
+  // mixed-precision chain (LLG_DEMAG_MIXED): FP32 spectrum and tensor spectra
+  int mixed = 0;
+  float2* d_Sf = nullptr;
+  float* d_txxf = nullptr;
+  float* d_tyyf = nullptr;
+  float* d_tzzf = nullptr;
+  float2* d_txyf = nullptr;
+  size_t smem_rows_f = 0, smem_cols_f = 0, smem_cols_staged_f = 0;
+  bool stage_tensor_f = false;
+  DemagTc* tc = nullptr;         // tensor-core column stage (k_demag_tc.cu), when the shape allows
 };
 
 static int factorize(int n, std::vector<int>& rad) {
@@ -597,12 +436,16 @@ static int fft_init(HostFft& f, int n, int batch) {
     if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) need = std::max(need, n / r);
   f.tx = ((std::max(need, 32) + 31) / 32) * 32;
   std::vector<double2> tw(n);
+  std::vector<float2> twf(n);
   for (int k = 0; k < n; k++) {
     const long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
     tw[k] = make_double2((double)cosl(ang), (double)-sinl(ang));
+    twf[k] = make_float2((float)cosl(ang), (float)-sinl(ang));
   }
   LLG_CUDA_TRY(cudaMalloc(&f.d_tw, sizeof(double2) * n));
   LLG_CUDA_TRY(cudaMemcpy(f.d_tw, tw.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+  LLG_CUDA_TRY(cudaMalloc(&f.d_twf, sizeof(float2) * n));
+  LLG_CUDA_TRY(cudaMemcpy(f.d_twf, twf.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
   std::vector<int4> ps(std::max<size_t>(f.radix.size(), 1));
   int ns = 1;
   for (size_t i = 0; i < f.radix.size(); i++) {
@@ -616,7 +459,9 @@ static int fft_init(HostFft& f, int n, int batch) {
 
 static void fft_free(HostFft& f) {
   cudaFree(f.d_tw);
+  cudaFree(f.d_twf);
   cudaFree(f.d_pass);
+  f.d_twf = nullptr;
   f.d_tw = nullptr;
   f.d_pass = nullptr;
 }
@@ -631,6 +476,12 @@ void demag_destroy(DemagPlan* d) {
   cudaFree(d->d_tzz);
   cudaFree(d->d_txy);
   cudaFree(d->d_T);
+  cudaFree(d->d_Sf);
+  cudaFree(d->d_txxf);
+  cudaFree(d->d_tyyf);
+  cudaFree(d->d_tzzf);
+  cudaFree(d->d_txyf);
+  demag_tc_destroy(d->tc);
   delete d;
 }
 
@@ -642,39 +493,46 @@ static int set_smem(const void* fn, size_t bytes) {
 }
 
 // ── launch helpers (elements-per-thread dispatch) ─────────────────────────
+template <typename R>
 static int launch_rows_fwd(const DemagPlan* d, cudaStream_t s, const double* in, long long cs, int row_len,
-                           int nrows, const double* w, double2* S, int ld, int ncomp) {
-  const FftPlan pl = d->fx.dev();
+                           int nrows, const double* w, cx_t<R>* S, int ld, int ncomp) {
+  const FftPlanT<R> pl = d->fx.dev<R>();
+  const size_t sm = (sizeof(R) == 8) ? d->smem_rows : d->smem_rows_f;
   const dim3 g((nrows + 2 * kRowsNB - 1) / (2 * kRowsNB), ncomp), b(d->fx.tx, kRowsNB);
   if (d->fx.ept == 8)
-    k_rows_fwd<kRowsNB, 8><<<g, b, d->smem_rows, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
+    k_rows_fwd<R, kRowsNB, 8><<<g, b, sm, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
   else
-    k_rows_fwd<kRowsNB, 16><<<g, b, d->smem_rows, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
+    k_rows_fwd<R, kRowsNB, 16><<<g, b, sm, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
-static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, double* h, long long cs) {
-  const FftPlan pl = d->fx.dev();
+template <typename R>
+static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, const cx_t<R>* S, double* h, long long cs) {
+  const FftPlanT<R> pl = d->fx.dev<R>();
+  const size_t sm = (sizeof(R) == 8) ? d->smem_rows : d->smem_rows_f;
   const dim3 g((d->ny + 2 * kRowsNB - 1) / (2 * kRowsNB), 3), b(d->fx.tx, kRowsNB);
   if (d->fx.ept == 8)
-    k_rows_inv<kRowsNB, 8><<<g, b, d->smem_rows, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, h, cs, d->ng);
+    k_rows_inv<R, kRowsNB, 8><<<g, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, h, cs, d->ng);
   else
-    k_rows_inv<kRowsNB, 16><<<g, b, d->smem_rows, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, h, cs, d->ng);
+    k_rows_inv<R, kRowsNB, 16><<<g, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, h, cs, d->ng);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
-static int launch_cols_conv(const DemagPlan* d, cudaStream_t s) {
-  const FftPlan pl = d->fy.dev();
+template <typename R>
+static int launch_cols_conv(const DemagPlan* d, cudaStream_t s, cx_t<R>* S, const R* txx, const R* tyy,
+                            const R* tzz, const cx_t<R>* txy) {
+  const FftPlanT<R> pl = d->fy.dev<R>();
   const dim3 b(d->fy.tx, 3);
-  const size_t sm = d->stage_tensor ? d->smem_cols_staged : d->smem_cols;
-#define COLS_LAUNCH(E, ST) \
-  k_cols_conv<E, ST><<<d->hx, b, sm, s>>>(pl, d->d_S, d->ny, d->ny, d->hx, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy)
+  const bool stage = (sizeof(R) == 8) ? d->stage_tensor : d->stage_tensor_f;
+  const size_t sm = (sizeof(R) == 8) ? (stage ? d->smem_cols_staged : d->smem_cols)
+                                     : (stage ? d->smem_cols_staged_f : d->smem_cols_f);
+#define COLS_LAUNCH(E, ST) k_cols_conv<R, E, ST><<<d->hx, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy)
   if (d->fy.ept == 8) {
-    if (d->stage_tensor) COLS_LAUNCH(8, true); else COLS_LAUNCH(8, false);
+    if (stage) COLS_LAUNCH(8, true); else COLS_LAUNCH(8, false);
   } else {
-    if (d->stage_tensor) COLS_LAUNCH(16, true); else COLS_LAUNCH(16, false);
+    if (stage) COLS_LAUNCH(16, true); else COLS_LAUNCH(16, false);
   }
 #undef COLS_LAUNCH
   LLG_CUDA_TRY(cudaPeekAtLastError());
@@ -682,7 +540,7 @@ static int launch_cols_conv(const DemagPlan* d, cudaStream_t s) {
 }
 
 static int launch_cols_fwd(const DemagPlan* d, cudaStream_t s, double2* S) {
-  const FftPlan pl = d->fy.dev();
+  const FftPlan pl = d->fy.dev<double>();
   const size_t sm = sizeof(double2) * (size_t)d->py;
   if (d->fy.ept == 8)
     k_cols_fwd<8><<<d->hx, dim3(d->fy.tx, 1), sm, s>>>(pl, S, d->py, d->py, d->hx);
@@ -690,6 +548,35 @@ static int launch_cols_fwd(const DemagPlan* d, cudaStream_t s, double2* S) {
     k_cols_fwd<16><<<d->hx, dim3(d->fy.tx, 1), sm, s>>>(pl, S, d->py, d->py, d->hx);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
+}
+
+template <typename R>
+static int set_smem_all(const DemagPlan* d, size_t rows, size_t cols, size_t cols_staged, bool stage) {
+  int rc;
+  if ((rc = set_smem((const void*)k_rows_fwd<R, kRowsNB, 8>, rows)) ||
+      (rc = set_smem((const void*)k_rows_fwd<R, kRowsNB, 16>, rows)) ||
+      (rc = set_smem((const void*)k_rows_inv<R, kRowsNB, 8>, rows)) ||
+      (rc = set_smem((const void*)k_rows_inv<R, kRowsNB, 16>, rows)) ||
+      (rc = set_smem((const void*)k_cols_conv<R, 8, false>, cols)) ||
+      (rc = set_smem((const void*)k_cols_conv<R, 16, false>, cols)) ||
+      (stage && (rc = set_smem((const void*)k_cols_conv<R, 8, true>, cols_staged))) ||
+      (stage && (rc = set_smem((const void*)k_cols_conv<R, 16, true>, cols_staged))))
+    return rc;
+  (void)d;
+  return 0;
+}
+
+// FP64 tensor spectra -> FP32 copies for the mixed chain
+__global__ void k_tensor_to_f32(const double* __restrict__ a, const double* __restrict__ b,
+                                const double* __restrict__ c, const double2* __restrict__ xy, long long n,
+                                float* __restrict__ af, float* __restrict__ bf, float* __restrict__ cf,
+                                float2* __restrict__ xyf) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    af[e] = (float)a[e];
+    bf[e] = (float)b[e];
+    cf[e] = (float)c[e];
+    xyf[e] = make_float2((float)xy[e].x, (float)xy[e].y);
+  }
 }
 
 int demag_create(llg_ctx* c) {
@@ -715,14 +602,14 @@ int demag_create(llg_ctx* c) {
     demag_destroy(d);
     return LLG_ERR_NOTSUP;
   }
-  if ((rc = set_smem((const void*)k_rows_fwd<kRowsNB, 8>, d->smem_rows)) ||
-      (rc = set_smem((const void*)k_rows_fwd<kRowsNB, 16>, d->smem_rows)) ||
-      (rc = set_smem((const void*)k_rows_inv<kRowsNB, 8>, d->smem_rows)) ||
-      (rc = set_smem((const void*)k_rows_inv<kRowsNB, 16>, d->smem_rows)) ||
-      (rc = set_smem((const void*)k_cols_conv<8, false>, d->smem_cols)) ||
-      (rc = set_smem((const void*)k_cols_conv<16, false>, d->smem_cols)) ||
-      (d->stage_tensor && (rc = set_smem((const void*)k_cols_conv<8, true>, d->smem_cols_staged))) ||
-      (d->stage_tensor && (rc = set_smem((const void*)k_cols_conv<16, true>, d->smem_cols_staged))) ||
+  d->mixed = (p.demag_precision == LLG_DEMAG_MIXED);
+  d->smem_rows_f = sizeof(float2) * (size_t)kRowsNB * d->px;
+  d->smem_cols_f = sizeof(float2) * 3 * (size_t)d->py;
+  d->smem_cols_staged_f = d->smem_cols_f + (size_t)20 * d->py;
+  d->stage_tensor_f = (d->py % 4 == 0) && d->smem_cols_staged_f <= 200 * 1024;
+  if ((rc = set_smem_all<double>(d, d->smem_rows, d->smem_cols, d->smem_cols_staged, d->stage_tensor)) ||
+      (d->mixed &&
+       (rc = set_smem_all<float>(d, d->smem_rows_f, d->smem_cols_f, d->smem_cols_staged_f, d->stage_tensor_f))) ||
       (rc = set_smem((const void*)k_cols_fwd<8>, sizeof(double2) * (size_t)d->py)) ||
       (rc = set_smem((const void*)k_cols_fwd<16>, sizeof(double2) * (size_t)d->py))) {
     demag_destroy(d);
@@ -753,7 +640,8 @@ int demag_create(llg_ctx* c) {
   double2* spec = nullptr;
   LLG_CUDA_TRY(cudaMalloc(&spec, sizeof(double2) * 9 * (size_t)nspec));
   for (int k = 0; k < 9; k++) {
-    if ((rc = launch_rows_fwd(d, s, d->d_T + k * np, 0, d->px, d->py, nullptr, spec + k * nspec, d->py, 1)) ||
+    if ((rc = launch_rows_fwd<double>(d, s, d->d_T + k * np, 0, d->px, d->py, nullptr, spec + k * nspec, d->py,
+                                      1)) ||
         (rc = launch_cols_fwd(d, s, spec + k * nspec))) {
       cudaFree(spec);
       demag_destroy(d);
@@ -787,8 +675,44 @@ int demag_create(llg_ctx* c) {
     c->demag = d;
     return LLG_ERR_NOTSUP;
   }
+  if (d->mixed) {
+    LLG_CUDA_TRY(cudaMalloc(&d->d_Sf, sizeof(float2) * 3 * (size_t)d->hx * d->ny));
+    LLG_CUDA_TRY(cudaMalloc(&d->d_txxf, sizeof(float) * nspec));
+    LLG_CUDA_TRY(cudaMalloc(&d->d_tyyf, sizeof(float) * nspec));
+    LLG_CUDA_TRY(cudaMalloc(&d->d_tzzf, sizeof(float) * nspec));
+    LLG_CUDA_TRY(cudaMalloc(&d->d_txyf, sizeof(float2) * nspec));
+    k_tensor_to_f32<<<c->num_sms * 4, 256, 0, s>>>(d->d_txx, d->d_tyy, d->d_tzz, d->d_txy, nspec, d->d_txxf,
+                                                   d->d_tyyf, d->d_tzzf, d->d_txyf);
+    LLG_CUDA_TRY(cudaPeekAtLastError());
+    // tensor-core column stage where the column shape allows it (else FP32 Stockham columns)
+    if ((rc = demag_tc_create(c, d->px, d->py, d->hx, d->ny, d->d_txxf, d->d_tyyf, d->d_tzzf, d->d_txyf, &d->tc))) {
+      c->demag = d;
+      return rc;
+    }
+  }
   c->demag = d;
   return 0;
+}
+
+// stage 0 rows_fwd, 1 column convolution, 2 rows_inv; FP64 or mixed chain
+static int demag_run_stage(llg_ctx* c, DemagPlan* d, int stage, const double* y, const double* w, double* h) {
+  const long long cs = (long long)c->ncell;
+  if (stage == 0) {
+    LLG_COUNT(KID_DEMAG_ROWS_FWD);
+    if (d->mixed) return launch_rows_fwd<float>(d, c->stream, y, cs, d->ng, d->ny, w, d->d_Sf, d->ny, 3);
+    return launch_rows_fwd<double>(d, c->stream, y, cs, d->ng, d->ny, w, d->d_S, d->ny, 3);
+  }
+  if (stage == 1) {
+    LLG_COUNT(KID_DEMAG_COLS);
+    if (d->mixed) {
+      if (d->tc) return demag_tc_cols(c, d->tc, d->d_Sf);
+      return launch_cols_conv<float>(d, c->stream, d->d_Sf, d->d_txxf, d->d_tyyf, d->d_tzzf, d->d_txyf);
+    }
+    return launch_cols_conv<double>(d, c->stream, d->d_S, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy);
+  }
+  LLG_COUNT(KID_DEMAG_ROWS_INV);
+  if (d->mixed) return launch_rows_inv<float>(d, c->stream, d->d_Sf, h, cs);
+  return launch_rows_inv<double>(d, c->stream, d->d_S, h, cs);
 }
 
 int demag_apply(llg_ctx* c, const double* y, double* h) {
@@ -802,29 +726,24 @@ int demag_apply_w(llg_ctx* c, const double* y, const double* w, double* h) {
     return 0;
   }
   int rc;
-  LLG_COUNT(KID_DEMAG_ROWS_FWD);
-  if ((rc = launch_rows_fwd(d, c->stream, y, (long long)c->ncell, d->ng, d->ny, w, d->d_S, d->ny, 3))) return rc;
-  LLG_COUNT(KID_DEMAG_COLS);
-  if ((rc = launch_cols_conv(d, c->stream))) return rc;
-  LLG_COUNT(KID_DEMAG_ROWS_INV);
-  return launch_rows_inv(d, c->stream, h, (long long)c->ncell);
+  for (int stage = 0; stage < 3; stage++)
+    if ((rc = demag_run_stage(c, d, stage, y, w, h))) return rc;
+  return 0;
 }
 
 // one stage of the chain alone (profiling): 0 rows_fwd, 1 cols_conv, 2 rows_inv
 int demag_stage(llg_ctx* c, int stage, const double* y, double* h) {
   DemagPlan* d = c->demag;
   if (!d) return LLG_ERR_STATE;
-  if (stage == 0) {
-    LLG_COUNT(KID_DEMAG_ROWS_FWD);
-    return launch_rows_fwd(d, c->stream, y, (long long)c->ncell, d->ng, d->ny, c->p.windowed ? c->d_w : nullptr,
-                           d->d_S, d->ny, 3);
+  return demag_run_stage(c, d, stage, y, c->p.windowed ? c->d_w : nullptr, h);
+}
+
+int demag_check(llg_ctx* c) {
+  if (c->demag && c->demag->tc && demag_tc_failed(c, c->demag->tc)) {
+    llg_set_error("demag: a tensor-core completion wait ran out (results invalid)");
+    return LLG_ERR_TIMEOUT;
   }
-  if (stage == 1) {
-    LLG_COUNT(KID_DEMAG_COLS);
-    return launch_cols_conv(d, c->stream);
-  }
-  LLG_COUNT(KID_DEMAG_ROWS_INV);
-  return launch_rows_inv(d, c->stream, h, (long long)c->ncell);
+  return 0;
 }
 
 int demag_dims(llg_ctx* c, int out[4]) {

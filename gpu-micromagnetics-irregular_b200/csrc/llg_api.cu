@@ -57,6 +57,7 @@ static int validate(const llg_params* p) {
   if (p->aniso_kind != LLG_ANISO_LINEAR && p->aniso_kind != LLG_ANISO_CUBIC) { llg_set_error("bad aniso_kind"); return LLG_ERR_ARG; }
   if (p->demag_mode < LLG_DEMAG_OFF || p->demag_mode > LLG_DEMAG_OPEN) { llg_set_error("bad demag_mode"); return LLG_ERR_ARG; }
   if (p->demag_mode != LLG_DEMAG_OFF && !(p->demag_thick > 0.0)) { llg_set_error("demag_thick must be > 0"); return LLG_ERR_ARG; }
+  if (p->demag_precision != LLG_DEMAG_FP64 && p->demag_precision != LLG_DEMAG_MIXED) { llg_set_error("bad demag_precision"); return LLG_ERR_ARG; }
   if (p->windowed && p->exec_model != LLG_EXEC_YMSK) { llg_set_error("windowed runs use the full-grid execution model"); return LLG_ERR_ARG; }
   if (p->jv_mode != LLG_JV_REFERENCE && p->jv_mode != LLG_JV_FULL_FIELD) { llg_set_error("bad jv_mode"); return LLG_ERR_ARG; }
   const double vals[] = {p->che, p->chk, p->cha, p->chb, p->alpha, p->chg, p->demag_strength};
@@ -287,7 +288,8 @@ int llg_demag_apply(llg_ctx* c, const double* d_y, double* d_h) {
   int rc = ready(c);
   if (rc) return rc;
   if (!d_y || !d_h) return LLG_ERR_ARG;
-  return demag_apply(c, d_y, d_h) ? LLG_ERR_LAUNCH : 0;
+  if (demag_apply(c, d_y, d_h)) return LLG_ERR_LAUNCH;
+  return demag_check(c);
 }
 
 int llg_demag_self_coupling(llg_ctx* c, double out3[3]) {
@@ -335,7 +337,9 @@ int llg_integrator_init(llg_ctx* c, double t0, const double* d_y0, const llg_sol
 
 int llg_integrate(llg_ctx* c, double tout, double* d_yout, double* tret) {
   if (!c || !d_yout || !tret) return LLG_ERR_ARG;
-  return integrator_run(c, tout, d_yout, tret);
+  const int rc = integrator_run(c, tout, d_yout, tret);
+  const int dc = demag_check(c);
+  return dc ? dc : rc;
 }
 
 int llg_get_stats(llg_ctx* c, llg_stats* st) {

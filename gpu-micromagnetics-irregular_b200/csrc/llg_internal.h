@@ -63,6 +63,7 @@ struct DevProblem {
 };
 
 struct DemagPlan;   // k_demag.cu
+struct DemagTc;     // k_demag_tc.cu
 struct Integrator;  // integrator.cu
 struct Learned;     // k_learned.cu
 
@@ -124,6 +125,15 @@ int demag_self(llg_ctx* c, double out3[3]);
 int demag_stage(llg_ctx* c, int stage, const double* y, double* h);
 int demag_dims(llg_ctx* c, int out[4]);
 int demag_tensor_host(llg_ctx* c, int comp, int dx, int dy, double* out);
+// tensor-core (tcgen05, FP16 hi+lo split, FP32 accumulation) column stage of the
+// mixed chain; *out stays null when the column shape is not supported
+int demag_tc_create(llg_ctx* c, int px, int py, int hx, int ny, const float* txx, const float* tyy,
+                    const float* tzz, const float2* txy, DemagTc** out);
+void demag_tc_destroy(DemagTc* t);
+int demag_tc_cols(llg_ctx* c, DemagTc* t, float2* Sf);
+int demag_tc_failed(llg_ctx* c, DemagTc* t);
+// LLG_ERR_TIMEOUT if a bounded tensor-core wait of the demag chain ran out
+int demag_check(llg_ctx* c);
 
 // ── vector ops (k_vector.cu) ───────────────────────────────────────────
 int reductions_init(llg_ctx* c);

@@ -193,6 +193,7 @@ def load(path: str | None = None):
         "llg_default_geom_spec": (I, [P(GeomSpec)]),
         "llg_build_geometry": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
         "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
+        "llg_selftest_tcgen05": (I, [I, P(D)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -334,6 +335,15 @@ class Context:
         st = Stats()
         _check(self.lib.llg_get_stats(self.h, C.byref(st)), "llg_get_stats")
         return st.as_dict()
+
+
+def selftest_tcgen05(flags: int) -> float:
+    """One tensor-core GEMM (tcgen05, FP16 in, FP32 accumulate) against a
+    host FP64 product; returns the max error relative to sum |a b|."""
+    lib = load()
+    err = C.c_double()
+    _check(lib.llg_selftest_tcgen05(int(flags), C.byref(err)), "llg_selftest_tcgen05")
+    return err.value
 
 
 def build_geometry(spec: GeomSpec, want=("active", "w", "msk3", "nsk3", "grain_id", "y0")):

@@ -232,6 +232,12 @@ void llg_reset_kernel_counts(void);
 /* Average device time of one launch of family kernel_id (CUDA events on the
  * context's stream), measured on the live integrator buffers.              */
 int  llg_time_kernel(llg_ctx* ctx, int kernel_id, int iters, double* avg_ms);
+/* Known-answer check of the tensor-core path the mixed demag chain uses
+ * (no counterpart in the reference): one 128x64x64 FP16 GEMM into tensor
+ * memory against a host FP64 product; *max_rel_err = max |D - ref| /
+ * sum |a b|.  flags bit 0: A operand MN-major (else K-major); bit 1: A
+ * values in the FP16 subnormal range (shows whether the MMA keeps them).   */
+int  llg_selftest_tcgen05(int flags, double* max_rel_err);
 
 /* ── geometry / initial-condition builders (host) ────────────────────── */
 #define LLG_GEOM_BULK         0   /* sim_config.h GEOMETRY_BULK          */
