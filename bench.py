@@ -12,6 +12,13 @@ llg_integrate at the reference's 0.1 output cadence.  value = K*dt / device
 time of K steps (CUDA events on the library's stream, max over ranks);
 the state (>= 20 vectors of 18.9 MB) exceeds L2, so no flush is needed.
 
+Forms (--form): "plain" is the reference method in FP64; "mixed" runs the
+demag transforms in reduced precision (FP32 rows, tensor-core FP16 hi+lo
+column DFT stages with FP32 accumulation).  By default the best form built
+is timed and then a plain FP64 instance of the same workload is timed the
+same way; the line reports both throughputs, their ratio and the max |dm|
+between the two final states.
+
 --impl reference runs the CPU restatement of the reference path (the oracle;
 the reference itself needs SUNDIALS, which is absent) on all host cores.
 Multi-GPU: independent replicas (one instance per rank, no collective in
@@ -47,11 +54,12 @@ def workload(ng=1536, ny=512, seed=12345):
     return p, g, o
 
 
-def algorithmic_bytes(kid, ng, ny, dims):
-    """Compulsory HBM bytes of one launch of kernel family kid (FP64)."""
+def algorithmic_bytes(kid, ng, ny, dims, mixed=False):
+    """Compulsory HBM bytes of one launch of kernel family kid (FP64 state;
+    the mixed demag chain keeps its spectra and tensor spectra in FP32)."""
     n = ng * ny
     px, py, hx, nrows = dims
-    S = 3 * hx * nrows * 16
+    S = 3 * hx * nrows * (8 if mixed else 16)
     if kid == 0:   # rhs: y, hd, mask in; ydot out
         return 24 * n + 24 * n + n + 24 * n
     if kid == 1:   # jtv: y, v, mask in; Jv out
@@ -65,7 +73,7 @@ def algorithmic_bytes(kid, ng, ny, dims):
     if kid == 6:   # rows forward: y in; row spectra out
         return 24 * n + S
     if kid == 7:   # columns: spectra in/out + tensor (xx,yy,zz real, xy complex)
-        return 2 * S + hx * py * 40
+        return 2 * S + hx * py * (20 if mixed else 40)
     if kid == 8:   # rows inverse: spectra in; h out
         return S + 24 * n
     if kid == 9:   # dot_multi of 6 vectors: 7 vectors read
@@ -153,25 +161,39 @@ def make_ctx(p, g):
     return ctx, geo
 
 
-def run_ours(args, world, rank, local):
+# Forms of the same workload.  "plain" is the reference method in FP64; the
+# others change only the demag transform precision and the preconditioner.
+FORMS = {
+    "plain": dict(demag_precision=llg.DEMAG_FP64,
+                  desc="plain FP64 (block-Jacobi, FP64 FFT demag)"),
+    "mixed": dict(demag_precision=llg.DEMAG_MIXED,
+                  desc="mixed-precision demag (FP32 row FFTs, tcgen05 FP16 hi+lo column DFT stages with FP32 "
+                       "accumulation), block-Jacobi; FP64 state, norms, Newton update, Gram-Schmidt"),
+}
+BEST_FORM = "mixed"
+
+
+def form_params(form, seed):
+    p, g, o = workload(seed=seed)
+    p.demag_precision = FORMS[form]["demag_precision"]
+    return p, g, o
+
+
+def timed_run(args, form, world, rank, local, lib, clocks=True):
+    """Warm-up W steps, then K timed steps of one fresh instance of `form`."""
     import torch
-    torch.cuda.set_device(local)
-    lib = llg.load()
-    p, g, o = workload(seed=12345 + rank)
-    ng, ny = p.ng, p.ny
-    n = ng * ny
+    p, g, o = form_params(form, 12345 + rank)
     ctx, geo = make_ctx(p, g)
     y0 = torch.from_numpy(geo["y0"]).cuda()
     ctx.integrator_init(0.0, y0, o)
     yout = torch.zeros_like(y0)
-    t = 0.0
     sub = max(1, int(round(args.dt / 0.1)))
+    state = {"t": 0.0}
 
     def step():
-        nonlocal t
         for k in range(sub):
-            ctx.integrate(t + args.dt * (k + 1) / sub, yout)
-        t += args.dt
+            ctx.integrate(state["t"] + args.dt * (k + 1) / sub, yout)
+        state["t"] += args.dt
 
     for _ in range(args.warmup):
         step()
@@ -182,24 +204,29 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     dist_barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        e0.record()
-        for _ in range(args.steps):
-            step()
-        e1.record()
-        torch.cuda.synchronize()
-    ms_local = e0.elapsed_time(e1)
+    clk = Clocks(local) if clocks else None
+    if clk:
+        clk.__enter__()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    ms = dist_max(e0.elapsed_time(e1), world)
     dist_barrier(world)
-    ms = dist_max(ms_local, world)
     lib.llg_kernel_counts(counts1, 16)
     st1 = ctx.stats()
     launches = {KERNEL_NAMES[k]: int(counts1[k] - counts0[k]) for k in range(13)}
-    total_launches = sum(launches.values())
-    sim = args.steps * args.dt
-    value = world * sim / (ms / 1000.0)
+    dst = {k: st1[k] - st0[k] for k in ("nst", "nfe", "nni", "nli", "nsetups", "netf", "ncfn")}
+    return {"ctx": ctx, "p": p, "g": g, "o": o, "yout": yout, "t": state["t"], "ms": ms, "launches": launches,
+            "counters": dst, "value": world * args.steps * args.dt / (ms / 1000.0), "clocks": clk}
 
-    # per-family device time on live buffers → shares and the dominant kernel
-    dims = (C.c_int * 4)()
+
+def roofline_for(lib, run, ng, ny, mixed):
+    launches = run["launches"]
+    ctx = run["ctx"]
     fam_ms = {}
     for kid in (0, 1, 2, 3, 4, 6, 7, 8, 9, 10):
         if launches[KERNEL_NAMES[kid]] == 0 and kid not in (6, 7, 8):
@@ -218,74 +245,104 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    abytes = algorithmic_bytes(dom, ng, ny, dd)
+    peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    abytes = algorithmic_bytes(dom, ng, ny, dd, mixed)
     achieved = abytes / (fam_ms[dom] * 1e-3) / 1e9 if dom in fam_ms else None
     traffic = None
     try:
         with open(os.path.join(REPO, "profiles", "traffic_per_launch.json")) as f:
-            traffic = json.load(f).get(KERNEL_NAMES[dom])
+            traffic = json.load(f).get(("mixed:" if mixed else "") + KERNEL_NAMES[dom])
     except Exception:
         pass
+    return {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": fam_ms.get(dom),
+            "peak_source": f"{peak_src} hbm_gbs (burst copy)",
+            "kernel_avg_ms": {KERNEL_NAMES[k]: v for k, v in fam_ms.items()},
+            "kernel_share": {KERNEL_NAMES[k]: v / max(sum(share.values()), 1e-30) for k, v in share.items()}}
 
-    # end to end: host buffers in, host frames out, through the public API
-    e2e = None
-    if not args.no_e2e:
-        ctx2 = llg.Context(p)
-        geo2 = llg.build_geometry(g, want=("active", "y0"))
-        mask_h = torch.from_numpy(np.tile(geo2["active"].astype(np.float64), 3)).pin_memory()
-        y0_h = torch.from_numpy(geo2["y0"]).pin_memory()
-        frame_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
-        y0_d = torch.empty(3 * n, dtype=torch.float64, device="cuda")
-        yo_d = torch.empty_like(y0_d)
-        torch.cuda.synchronize()
-        dist_barrier(world)
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record()
-        ctx2.set_mask(mask_h.numpy())
-        y0_d.copy_(y0_h, non_blocking=True)
-        ctx2.integrator_init(0.0, y0_d, o)
-        tt = 0.0
-        for _ in range(args.steps):
-            for k in range(sub):
-                ctx2.integrate(tt + args.dt * (k + 1) / sub, yo_d)
-            tt += args.dt
-            frame_h.copy_(yo_d, non_blocking=True)
-        f1.record()
-        torch.cuda.synchronize()
-        ems = dist_max(f0.elapsed_time(f1), world)
-        e2e = {"value": world * args.steps * args.dt / (ems / 1000.0), "unit": UNIT,
-               "h2d_bytes_per_step": int((y0_h.numel() * 8 + mask_h.numel() * 8) / args.steps),
-               "d2h_bytes_per_step": int(frame_h.numel() * 8),
-               "note": "fresh instance from t=0: pinned y0 + mask uploaded once and amortised over the steps; "
-                       "one y(t) frame copied back per step; includes integrator start-up"}
-        ctx2.close()
 
+def e2e_run(args, form, world, rank):
+    """Same metric through the public API from host buffers: pinned y0 and
+    mask uploaded inside the timed region, one y(t) frame read back per step."""
+    import torch
+    p, g, o = form_params(form, 12345 + rank)
+    n = p.ng * p.ny
+    sub = max(1, int(round(args.dt / 0.1)))
+    ctx2 = llg.Context(p)
+    geo2 = llg.build_geometry(g, want=("active", "y0"))
+    mask_h = torch.from_numpy(np.tile(geo2["active"].astype(np.float64), 3)).pin_memory()
+    y0_h = torch.from_numpy(geo2["y0"]).pin_memory()
+    frame_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+    y0_d = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+    yo_d = torch.empty_like(y0_d)
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    ctx2.set_mask(mask_h.numpy())
+    y0_d.copy_(y0_h, non_blocking=True)
+    ctx2.integrator_init(0.0, y0_d, o)
+    tt = 0.0
+    for _ in range(args.steps):
+        for k in range(sub):
+            ctx2.integrate(tt + args.dt * (k + 1) / sub, yo_d)
+        tt += args.dt
+        frame_h.copy_(yo_d, non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    ems = dist_max(f0.elapsed_time(f1), world)
+    ctx2.close()
+    return {"value": world * args.steps * args.dt / (ems / 1000.0), "unit": UNIT,
+            "h2d_bytes_per_step": int((y0_h.numel() * 8 + mask_h.numel() * 8) / args.steps),
+            "d2h_bytes_per_step": int(frame_h.numel() * 8),
+            "note": "fresh instance from t=0: pinned y0 + mask uploaded once and amortised over the steps; "
+                    "one y(t) frame copied back per step; includes integrator start-up"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    lib = llg.load()
+    form = args.form or BEST_FORM
+    ng, ny = 1536, 512
+    main = timed_run(args, form, world, rank, local, lib)
+    roof = roofline_for(lib, main, ng, ny, FORMS[form]["demag_precision"] == llg.DEMAG_MIXED)
+    clk = main["clocks"].summary()
+    y_main = main["yout"].cpu().numpy()
+    main["ctx"].close()
+    compare = None
+    if form != "plain" and not args.no_compare:
+        plain = timed_run(args, "plain", world, rank, local, lib, clocks=False)
+        y_plain = plain["yout"].cpu().numpy()
+        plain["ctx"].close()
+        compare = {"plain_fp64_value": plain["value"], "plain_fp64_ms_per_step": plain["ms"] / args.steps,
+                   "ratio_vs_plain_fp64": main["value"] / plain["value"],
+                   "max_dm_vs_plain_fp64": float(np.abs(y_main - y_plain).max()),
+                   "dm_at_t": main["t"], "plain_counters": plain["counters"],
+                   "dm_note": "both forms integrated from the same state over [0, t]; at rtol 1e-4 they take a "
+                              "few different accepted steps, so the distance is at the integration-tolerance "
+                              "level and grows with the workload's physical instability"}
+    e2e = None if args.no_e2e else e2e_run(args, form, world, rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
-
-    dst = {k: st1[k] - st0[k] for k in ("nst", "nfe", "nni", "nli", "nsetups", "netf", "ncfn")}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry/IC builders)",
+        "metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": main["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded geometry/IC builders)",
         "config": {"workload": "1536x512 cells, square hole side 0.25*ny, open FFT demag strength 4 "
                                "(3072x1024 padded), A=1 k=0.1(+x) h=(0,0,0.05) alpha=0.02, free edges, "
-                               "rtol 1e-4 atol 1e-6, SPGMR(5)+block-Jacobi, classical GS, FP64",
-                   "form": "plain FP64 (block-Jacobi, FP64 demag)", "sim_time_per_step": args.dt,
+                               "rtol 1e-4 atol 1e-6, SPGMR(5), classical GS",
+                   "form": FORMS[form]["desc"], "sim_time_per_step": args.dt,
                    "output_interval": 0.1, "parallelism": f"replicas x{world}",
                    "l2": "state > 126 MB L2 (>= 20 vectors x 18.9 MB); no flush",
-                   "solver_counters_timed": dst},
-        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": fam_ms.get(dom),
-                     "peak_source": f"{peak_src} hbm_gbs (burst copy)",
-                     "kernel_avg_ms": {KERNEL_NAMES[k]: v for k, v in fam_ms.items()},
-                     "kernel_share": {KERNEL_NAMES[k]: v / max(sum(share.values()), 1e-30)
-                                      for k, v in share.items()}},
-        "e2e": e2e, "gpu_launches": total_launches, "launches_by_family": launches,
-        "clocks": clk.summary(), "cpu_baseline": cpu,
+                   "solver_counters_timed": main["counters"]},
+        "compare": compare,
+        "roofline": roof,
+        "e2e": e2e, "gpu_launches": sum(main["launches"].values()), "launches_by_family": main["launches"],
+        "clocks": clk, "cpu_baseline": cpu,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -370,6 +427,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", choices=sorted(FORMS), default=None,
+                    help="form to time (default: the best one built, compared against plain FP64)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
