@@ -164,18 +164,55 @@ def make_ctx(p, g):
 # Forms of the same workload.  "plain" is the reference method in FP64; the
 # others change only the demag transform precision and the preconditioner.
 FORMS = {
-    "plain": dict(demag_precision=llg.DEMAG_FP64,
+    "plain": dict(demag_precision=llg.DEMAG_FP64, learned=False,
                   desc="plain FP64 (block-Jacobi, FP64 FFT demag)"),
-    "mixed": dict(demag_precision=llg.DEMAG_MIXED,
+    "mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=False,
                   desc="mixed-precision demag (FP32 row FFTs, tcgen05 FP16 hi+lo column DFT stages with FP32 "
                        "accumulation), block-Jacobi; FP64 state, norms, Newton update, Gram-Schmidt"),
+    "learned+mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=True,
+                          desc="learned preconditioner (3-layer 3x3 conv, 16 channels, BF16 weights, FP32 "
+                               "accumulation, on top of block-Jacobi, trained on the GPU on this workload's own "
+                               "harvested SPGMR solves) + mixed-precision demag"),
 }
-BEST_FORM = "mixed"
+BEST_FORM = "learned+mixed"
+TRAIN = dict(t_harvest=1.0, max_samples=32, stride=2, iters=600, batch=16, patch=32, seed=5, lr=3e-3,
+             init_scale=0.05)
+_weights_cache = {}
+
+
+def train_weights(rank):
+    """Harvest block-Jacobi SPGMR solves of the workload over t in [0, 1] and
+    train the network on them (setup phase, outside every timed region)."""
+    import torch
+    if "w" in _weights_cache:
+        return _weights_cache["w"], _weights_cache["info"]
+    t0 = time.perf_counter()
+    p, g, o = workload(seed=12345 + rank)
+    p.demag_precision = llg.DEMAG_MIXED
+    ctx, geo = make_ctx(p, g)
+    ctx.learned_harvest(TRAIN["max_samples"], TRAIN["stride"])
+    y0 = torch.from_numpy(geo["y0"]).cuda()
+    ctx.integrator_init(0.0, y0, o)
+    yout = torch.zeros_like(y0)
+    for k in range(1, int(round(TRAIN["t_harvest"] / 0.1)) + 1):
+        ctx.integrate(0.1 * k, yout)
+    t1 = time.perf_counter()
+    l0, l1 = ctx.learned_train(iters=TRAIN["iters"], batch=TRAIN["batch"], patch=TRAIN["patch"],
+                               seed=TRAIN["seed"], lr=TRAIN["lr"], init_scale=TRAIN["init_scale"])
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    w = ctx.learned_get_weights()
+    info = {"samples": ctx.learned_num_samples(), "harvest_s": t1 - t0, "train_s": t2 - t1,
+            "loss_first": l0, "loss_last": l1, **{k: v for k, v in TRAIN.items()}}
+    ctx.close()
+    _weights_cache["w"], _weights_cache["info"] = w, info
+    return w, info
 
 
 def form_params(form, seed):
     p, g, o = workload(seed=seed)
     p.demag_precision = FORMS[form]["demag_precision"]
+    p.precond_kind = llg.PREC_LEARNED if FORMS[form]["learned"] else llg.PREC_BLOCK_JACOBI
     return p, g, o
 
 
@@ -184,6 +221,8 @@ def timed_run(args, form, world, rank, local, lib, clocks=True):
     import torch
     p, g, o = form_params(form, 12345 + rank)
     ctx, geo = make_ctx(p, g)
+    if FORMS[form]["learned"]:
+        ctx.learned_set_weights(train_weights(rank)[0])
     y0 = torch.from_numpy(geo["y0"]).cuda()
     ctx.integrator_init(0.0, y0, o)
     yout = torch.zeros_like(y0)
@@ -220,6 +259,8 @@ def timed_run(args, form, world, rank, local, lib, clocks=True):
     st1 = ctx.stats()
     launches = {KERNEL_NAMES[k]: int(counts1[k] - counts0[k]) for k in range(13)}
     dst = {k: st1[k] - st0[k] for k in ("nst", "nfe", "nni", "nli", "nsetups", "netf", "ncfn")}
+    if FORMS[form]["learned"]:
+        dst["learned_status"] = ctx.learned_status()
     return {"ctx": ctx, "p": p, "g": g, "o": o, "yout": yout, "t": state["t"], "ms": ms, "launches": launches,
             "counters": dst, "value": world * args.steps * args.dt / (ms / 1000.0), "clocks": clk}
 
@@ -270,6 +311,8 @@ def e2e_run(args, form, world, rank):
     n = p.ng * p.ny
     sub = max(1, int(round(args.dt / 0.1)))
     ctx2 = llg.Context(p)
+    if FORMS[form]["learned"]:
+        ctx2.learned_set_weights(train_weights(rank)[0])
     geo2 = llg.build_geometry(g, want=("active", "y0"))
     mask_h = torch.from_numpy(np.tile(geo2["active"].astype(np.float64), 3)).pin_memory()
     y0_h = torch.from_numpy(geo2["y0"]).pin_memory()
@@ -318,11 +361,18 @@ def run_ours(args, world, rank, local):
         plain["ctx"].close()
         compare = {"plain_fp64_value": plain["value"], "plain_fp64_ms_per_step": plain["ms"] / args.steps,
                    "ratio_vs_plain_fp64": main["value"] / plain["value"],
+                   "gmres_iters_per_newton": main["counters"]["nli"] / max(main["counters"]["nni"], 1),
+                   "plain_gmres_iters_per_newton": plain["counters"]["nli"] / max(plain["counters"]["nni"], 1),
                    "max_dm_vs_plain_fp64": float(np.abs(y_main - y_plain).max()),
                    "dm_at_t": main["t"], "plain_counters": plain["counters"],
                    "dm_note": "both forms integrated from the same state over [0, t]; at rtol 1e-4 they take a "
                               "few different accepted steps, so the distance is at the integration-tolerance "
                               "level and grows with the workload's physical instability"}
+        if FORMS[form]["learned"]:
+            mixed = timed_run(args, "mixed", world, rank, local, lib, clocks=False)
+            mixed["ctx"].close()
+            compare["mixed_only_value"] = mixed["value"]
+            compare["mixed_only_gmres_iters_per_newton"] = mixed["counters"]["nli"] / max(mixed["counters"]["nni"], 1)
     e2e = None if args.no_e2e else e2e_run(args, form, world, rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -340,6 +390,7 @@ def run_ours(args, world, rank, local):
                    "l2": "state > 126 MB L2 (>= 20 vectors x 18.9 MB); no flush",
                    "solver_counters_timed": main["counters"]},
         "compare": compare,
+        "training": _weights_cache.get("info") if FORMS[form]["learned"] else None,
         "roofline": roof,
         "e2e": e2e, "gpu_launches": sum(main["launches"].values()), "launches_by_family": main["launches"],
         "clocks": clk, "cpu_baseline": cpu,

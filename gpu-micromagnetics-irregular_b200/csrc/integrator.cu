@@ -200,7 +200,17 @@ struct Integrator {
     int nl = 0, krydim = 0, converged = 0;
     nps++;
     double ss = 0.0;
-    if (!ok(fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A))) return LS_CONV_FAIL;
+    const bool learned = learned_active(c);
+    const bool harvest = !learned && learned_harvest_wanted(c);
+    double* zb = (learned || harvest) ? learned_zbuf(c) : nullptr;
+    if ((learned || harvest) && !zb) return LS_CONV_FAIL;
+    if (harvest) ok(launch_psolve(c, rhs, zb));   // u = P_BJ^-1 r, kept with the solution
+    if (learned) {
+      // V0 = ewt (I + gamma Net) P_BJ^-1 r, and its norm
+      if (!ok(launch_psolve(c, rhs, zb)) || !ok(learned_apply(c, ewt, V[0], SLOT_A))) return LS_CONV_FAIL;
+    } else if (!ok(fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A))) {
+      return LS_CONV_FAIL;
+    }
     ok(fetch_scalars(c, SLOT_A, 1, &ss));
     const double beta = sqrt(ss);
     double rnorm = beta, rho = beta;
@@ -214,7 +224,12 @@ struct Integrator {
       krydim = l + 1;
       njv++;
       nps++;
-      ok(launch_arnoldi_op(c, V[l], ewt, V[l + 1], y, gamma));
+      if (learned) {
+        ok(launch_arnoldi_op(c, V[l], ewt, zb, y, gamma, 0));
+        ok(learned_apply(c, ewt, V[l + 1], -1));
+      } else {
+        ok(launch_arnoldi_op(c, V[l], ewt, V[l + 1], y, gamma));
+      }
       Hes[l + 1][l] = gram_schmidt(l + 1);
       if (qr_fact(krydim) != 0) { nli += nl; return LS_CONV_FAIL; }
       rot *= givens[2 * l + 1];
@@ -232,6 +247,7 @@ struct Integrator {
       const double* X[MAXLL + 1];
       for (int k = 0; k < krydim; k++) X[k] = V[k];
       ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs));
+      if (converged && harvest) ok(learned_harvest(c, zb, rhs, ewt, c->gamma_setup));
       return converged ? LS_SUCCESS : LS_RES_REDUCED;
     }
     return LS_CONV_FAIL;
@@ -384,8 +400,13 @@ struct Integrator {
   int nls_lsolve(double* del) {
     const double deltar = LS_EPLIN * tq[4];
     const double dtol = deltar * sqrt((double)neq);
+    const bool learned = learned_active(c);
     const int r = spgmr(del, dtol);
     if (err) return LLG_CV_LSOLVE_FAIL;
+    // GMRES convergence judges the learned preconditioner: a failed solve
+    // switches this context back to block-Jacobi (the Newton iteration then
+    // recovers as after any linear-solver failure)
+    if (learned && (r == LS_CONV_FAIL || r == LS_QRSOL_FAIL)) learned_fall_back(c);
     if (r != LS_SUCCESS) nlcf++;
     if (r == LS_SUCCESS) return 0;
     if (r == LS_RES_REDUCED) return (ls_curiter == 0) ? 0 : 1;

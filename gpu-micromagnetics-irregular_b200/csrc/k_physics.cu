@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(TX * TY) k_arnoldi_tile(DevProblem P, const do
                                                           const double* __restrict__ hd,
                                                           const double* __restrict__ pm,
                                                           const double* __restrict__ ph, double gamma,
-                                                          double gamma_p) {
+                                                          double gamma_p, int scale_out) {
   __shared__ Tile<2> T;
   // stage y and vt = in/s (windowed: w·) with halo
   {
@@ -273,9 +273,15 @@ __global__ void __launch_bounds__(TX * TY) k_arnoldi_tile(DevProblem P, const do
   const double z0 = gz * (Pi[0] * u[0] + Pi[1] * u[1] + Pi[2] * u[2]);
   const double z1 = gz * (Pi[3] * u[0] + Pi[4] * u[1] + Pi[5] * u[2]);
   const double z2 = gz * (Pi[6] * u[0] + Pi[7] * u[1] + Pi[8] * u[2]);
-  out[cell] = ss[0] * z0;
-  out[n + cell] = ss[1] * z1;
-  out[2 * n + cell] = ss[2] * z2;
+  if (scale_out) {
+    out[cell] = ss[0] * z0;
+    out[n + cell] = ss[1] * z1;
+    out[2 * n + cell] = ss[2] * z2;
+  } else {  // block-Jacobi output for a further preconditioning stage
+    out[cell] = z0;
+    out[n + cell] = z1;
+    out[2 * n + cell] = z2;
+  }
 }
 
 int grid_1d(const llg_ctx* c, long long work, int block) {
@@ -344,11 +350,11 @@ int launch_psolve(llg_ctx* c, const double* r, double* z) {
 }
 
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out, const double* y,
-                      double gamma) {
+                      double gamma, int scale_out) {
   if (!c->have_setup) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_ARNOLDI);
   k_arnoldi_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, in, ewt, out, y, c->d_hd, c->d_pm, c->d_ph,
-                                                               gamma, c->gamma_setup);
+                                                               gamma, c->gamma_setup, scale_out);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

@@ -112,8 +112,9 @@ int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y);
 int launch_psetup(llg_ctx* c, const double* y, double gamma);
 int launch_psolve(llg_ctx* c, const double* r, double* z);
 // fused Arnoldi operator:  out = s1 ⊙ P^-1 ( vt − γ J vt ),  vt = in / s2
+// (scale_out 0: out = P^-1 (...) without the s1 factor)
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out,
-                      const double* y, double gamma);
+                      const double* y, double gamma, int scale_out = 1);
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot);
 
 // ── demag (k_demag.cu) ─────────────────────────────────────────────────
@@ -134,6 +135,14 @@ int demag_tc_cols(llg_ctx* c, DemagTc* t, float2* Sf);
 int demag_tc_failed(llg_ctx* c, DemagTc* t);
 // LLG_ERR_TIMEOUT if a bounded tensor-core wait of the demag chain ran out
 int demag_check(llg_ctx* c);
+
+// ── learned preconditioner (k_learned.cu) ──────────────────────────────
+bool learned_active(llg_ctx* c);                 // LLG_PREC_LEARNED with weights, no fallback
+double* learned_zbuf(llg_ctx* c);                // 3N scratch for the block-Jacobi stage
+int learned_apply(llg_ctx* c, const double* ewt, double* out, int slot /* <0: no norm */);
+void learned_fall_back(llg_ctx* c);
+bool learned_harvest_wanted(llg_ctx* c);
+int learned_harvest(llg_ctx* c, const double* u, const double* x, const double* ewt, double gamma);
 
 // ── vector ops (k_vector.cu) ───────────────────────────────────────────
 int reductions_init(llg_ctx* c);

@@ -18,6 +18,8 @@ from __future__ import annotations
 import ctypes as C
 import os
 
+import numpy as np
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libllg.so")
 
@@ -59,6 +61,14 @@ class SolverOpts(C.Structure):
         ("gs_type", C.c_int32), ("mxstep", C.c_int32), ("device_resident", C.c_int32),
         ("reserved0", C.c_int32),
     ]
+
+
+class TrainOpts(C.Structure):
+    _fields_ = [("iters", C.c_int32), ("batch", C.c_int32), ("patch", C.c_int32), ("seed", C.c_int32),
+                ("lr", C.c_double), ("init_scale", C.c_double)]
+
+
+LEARNED_NWEIGHTS = 4032
 
 
 class Stats(C.Structure):
@@ -194,6 +204,14 @@ def load(path: str | None = None):
         "llg_build_geometry": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
         "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
         "llg_selftest_tcgen05": (I, [I, P(D)]),
+        "llg_learned_harvest": (I, [VP, C.c_int32, C.c_int32]),
+        "llg_learned_num_samples": (I, [VP]),
+        "llg_learned_train": (I, [VP, P(TrainOpts), P(D), P(D)]),
+        "llg_learned_set_weights": (I, [VP, P(C.c_float), C.c_int32]),
+        "llg_learned_get_weights": (I, [VP, P(C.c_float), C.c_int32]),
+        "llg_learned_status": (I, [VP, P(C.c_int32), P(C.c_int32), P(C.c_int64)]),
+        "llg_learned_loss_grad": (I, [P(C.c_float), C.c_int32, C.c_int32] + [P(C.c_float)] * 6
+                                  + [P(D), P(C.c_float), P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -335,6 +353,52 @@ class Context:
         st = Stats()
         _check(self.lib.llg_get_stats(self.h, C.byref(st)), "llg_get_stats")
         return st.as_dict()
+
+    # ── learned preconditioner ──
+    def learned_harvest(self, max_samples: int, stride: int = 1):
+        _check(self.lib.llg_learned_harvest(self.h, int(max_samples), int(stride)), "llg_learned_harvest")
+
+    def learned_num_samples(self) -> int:
+        return int(self.lib.llg_learned_num_samples(self.h))
+
+    def learned_train(self, iters=400, batch=16, patch=32, seed=1, lr=3e-3, init_scale=0.05):
+        o = TrainOpts(int(iters), int(batch), int(patch), int(seed), float(lr), float(init_scale))
+        l0, l1 = C.c_double(), C.c_double()
+        _check(self.lib.llg_learned_train(self.h, C.byref(o), C.byref(l0), C.byref(l1)), "llg_learned_train")
+        return l0.value, l1.value
+
+    def learned_set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(self.lib.llg_learned_set_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size),
+               "llg_learned_set_weights")
+
+    def learned_get_weights(self):
+        w = np.zeros(LEARNED_NWEIGHTS, dtype=np.float32)
+        _check(self.lib.llg_learned_get_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size),
+               "llg_learned_get_weights")
+        return w
+
+    def learned_status(self):
+        a, f, n = C.c_int32(), C.c_int32(), C.c_int64()
+        _check(self.lib.llg_learned_status(self.h, C.byref(a), C.byref(f), C.byref(n)), "llg_learned_status")
+        return {"active": a.value, "fell_back": f.value, "napply": n.value}
+
+
+def learned_loss_grad(w, u, m, mask, ewt, x, gamma, want_z=True):
+    """Loss, weight gradient (and output z) of the CUDA training kernels on
+    FP32 patches: u, m, ewt, x (nb, 3, P, P), mask (nb, P, P), gamma (nb,)."""
+    lib = load()
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+    w, u, m, mask, ewt, x, gamma = map(f32, (w, u, m, mask, ewt, x, gamma))
+    nb, _, P, _ = u.shape
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    loss = C.c_double()
+    grad = np.zeros(LEARNED_NWEIGHTS, dtype=np.float32)
+    z = np.zeros_like(u) if want_z else None
+    _check(lib.llg_learned_loss_grad(fp(w), nb, P, fp(u), fp(m), fp(mask), fp(ewt), fp(x), fp(gamma),
+                                     C.byref(loss), fp(grad), fp(z) if want_z else None),
+           "llg_learned_loss_grad")
+    return loss.value, grad, z
 
 
 def selftest_tcgen05(flags: int) -> float:

@@ -222,6 +222,39 @@ int  llg_integrator_init(llg_ctx* ctx, double t0, const double* d_y0,
 int  llg_integrate(llg_ctx* ctx, double tout, double* d_yout, double* tret);
 int  llg_get_stats(llg_ctx* ctx, llg_stats* st);
 
+/* ── learned preconditioner (no counterpart in the reference) ──────────── *
+ * z = (P_BJ^-1 r + gamma * Net(P_BJ^-1 r; m)) on active cells, Net a 3-layer
+ * 3x3 convolution 9 -> 16 -> 16 -> 3 channels without bias or activation
+ * (linear in r), inputs [u, m x u, m x (m x u)], BF16 weights at inference,
+ * FP32 accumulation.  Used by the integrator when params.precond_kind ==
+ * LLG_PREC_LEARNED and weights are set; a failed GMRES solve switches the
+ * context back to block-Jacobi for good (llg_learned_status).  Weights:
+ * 4032 floats, [W1 (16,9,3,3) | W2 (16,16,3,3) | W3 (3,16,3,3)] row-major.  */
+#define LLG_LEARNED_NWEIGHTS 4032
+typedef struct llg_train_opts {
+  int32_t iters;           /* Adam iterations                                     */
+  int32_t batch;           /* patches per iteration                               */
+  int32_t patch;           /* patch side (cells); 3-cell border excluded from loss */
+  int32_t seed;            /* patch sampling / initial weights                     */
+  double  lr;              /* Adam learning rate                                   */
+  double  init_scale;      /* initial weight scale (fresh weights only)            */
+} llg_train_opts;
+/* Record (P_BJ^-1 r, x, ewt, m, gamma) of every `stride`-th converged
+ * block-Jacobi SPGMR solve of the integrator, up to max_samples.           */
+int  llg_learned_harvest(llg_ctx* ctx, int32_t max_samples, int32_t stride);
+int  llg_learned_num_samples(llg_ctx* ctx);
+/* Train on the harvested samples with the library's forward/backward/Adam
+ * kernels; loss = mean over patches of sum (ewt (z - x))^2 / sum (ewt x)^2.  */
+int  llg_learned_train(llg_ctx* ctx, const llg_train_opts* o, double* loss_first, double* loss_last);
+int  llg_learned_set_weights(llg_ctx* ctx, const float* h_w, int32_t n);
+int  llg_learned_get_weights(llg_ctx* ctx, float* h_w, int32_t n);
+int  llg_learned_status(llg_ctx* ctx, int32_t* active, int32_t* fell_back, int64_t* napply);
+/* Loss, weight gradient and output z of the training kernels on host FP32
+ * patches [nb][3][P][P] (mask [nb][P][P], gamma [nb]); h_z may be NULL.     */
+int  llg_learned_loss_grad(const float* h_w, int32_t nb, int32_t P, const float* h_u, const float* h_m,
+                           const float* h_mask, const float* h_ewt, const float* h_x, const float* h_gamma,
+                           double* loss, float* h_grad, float* h_z);
+
 /* ── instrumentation ──────────────────────────────────────────────────── */
 /* Kernel families, in this order: RHS, JTV, ARNOLDI (fused Krylov operator),
  * PSETUP, PSOLVE, NORM, DEMAG_ROWS_FWD, DEMAG_COLS, DEMAG_ROWS_INV, REDUCE,

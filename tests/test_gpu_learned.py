@@ -1,0 +1,98 @@
+"""Learned preconditioner on the GPU, through the C ABI.
+
+1. The CUDA training kernels (forward, loss, backward) against the FP64
+   restatement oracle/learned_ref.py (itself pinned to finite differences in
+   tests/test_learned_oracle.py).  FP32 kernels vs FP64: rel 1e-4.
+2. Harvest -> train -> integrate: the network is trained on the solver's own
+   SPGMR solutions of a square-hole + open-demag film and then used as the
+   left preconditioner; it must lower the GMRES iterations per Newton
+   iteration against block-Jacobi on a fresh run of the same physics.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import llg
+from conftest import REPO
+
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+import learned_ref as L  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def test_training_kernels_match_fp64_oracle(gpu):
+    rng = np.random.default_rng(3)
+    theta = (rng.standard_normal(L.nparams()) * 0.1).astype(np.float32)
+    nb, P = 3, 20
+    batch = L.random_batch(rng, nb, P, P)
+    for s in batch:   # FP32-representable inputs for both sides
+        for k in ("u", "m", "mask", "ewt", "x"):
+            s[k] = s[k].astype(np.float32).astype(np.float64)
+        s["gamma"] = float(np.float32(s["gamma"]))
+    loss_ref, g_ref = L.loss_and_grad(theta.astype(np.float64), batch)
+    st = lambda k: np.stack([s[k] for s in batch])  # noqa: E731
+    loss, g, z = llg.learned_loss_grad(theta, st("u"), st("m"), st("mask"), st("ewt"), st("x"),
+                                       np.array([s["gamma"] for s in batch]))
+    z_ref = np.stack([L.forward(theta.astype(np.float64), s["u"], s["m"], s["mask"], s["gamma"])[0]
+                      for s in batch])
+    print("loss", loss, loss_ref, "grad rel", np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref))
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref)
+    assert np.linalg.norm(g - g_ref) <= 1e-4 * np.linalg.norm(g_ref)
+    assert np.abs(z - z_ref).max() <= 1e-4 * np.abs(z_ref).max()
+
+
+def _film(ng, ny, precond):
+    p = llg.default_params(ng, ny, demag_mode=llg.DEMAG_OPEN, demag_strength=4.0, norm_kind=llg.NORM_REG,
+                           precond_kind=precond)
+    g = llg.default_geom(ng, ny, geometry_kind=llg.GEOM_HOLE_SQUARE, hole_radius_frac_y=0.125, ic_jitter_eps=0.01)
+    return p, llg.build_geometry(g)
+
+
+def _integrate(torch, ctx, geo, t_end, opts):
+    y0 = torch.from_numpy(geo["y0"]).cuda()
+    ctx.integrator_init(0.0, y0, opts)
+    yout = torch.zeros_like(y0)
+    for k in range(1, int(round(t_end / 0.1)) + 1):
+        ctx.integrate(0.1 * k, yout)
+    torch.cuda.synchronize()
+    return yout.cpu().numpy(), ctx.stats()
+
+
+def test_trained_network_lowers_gmres_iterations(gpu):
+    import torch
+    ng, ny = 192, 128
+    opts = llg.default_solver_opts()
+    # harvest training pairs from a block-Jacobi run
+    p, geo = _film(ng, ny, llg.PREC_BLOCK_JACOBI)
+    act = np.tile(geo["active"].astype(np.float64), 3)
+    ch = llg.Context(p)
+    ch.set_mask(act)
+    ch.learned_harvest(48, 1)
+    _integrate(torch, ch, geo, 1.0, opts)
+    assert ch.learned_num_samples() > 8
+    l0, l1 = ch.learned_train(iters=600, batch=16, patch=32, seed=5, lr=3e-3, init_scale=0.05)
+    w = ch.learned_get_weights()
+    print(f"training loss {l0:.4e} -> {l1:.4e} on {ch.learned_num_samples()} harvested solves")
+    assert l1 < l0
+    # fresh runs of the same physics, block-Jacobi vs learned
+    _, base = _integrate(torch, _ctx(llg.PREC_BLOCK_JACOBI, ng, ny, act), geo, 2.0, opts)
+    cl = _ctx(llg.PREC_LEARNED, ng, ny, act)
+    cl.learned_set_weights(w)
+    _, lrn = _integrate(torch, cl, geo, 2.0, opts)
+    status = cl.learned_status()
+    it_b = base["nli"] / base["nni"]
+    it_l = lrn["nli"] / lrn["nni"]
+    print(f"GMRES iterations per Newton iteration: block-Jacobi {it_b:.3f} ({base}), learned {it_l:.3f} "
+          f"({lrn}), status {status}")
+    assert status["active"] == 1 and status["fell_back"] == 0 and status["napply"] > 0
+    assert it_l < it_b
+
+
+def _ctx(precond, ng, ny, act):
+    p, _ = _film(ng, ny, precond)
+    c = llg.Context(p)
+    c.set_mask(act)
+    return c
