@@ -171,8 +171,9 @@ FORMS = {
                        "accumulation), block-Jacobi; FP64 state, norms, Newton update, Gram-Schmidt"),
     "learned+mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=True,
                           desc="learned preconditioner (3-layer 3x3 conv, 16 channels, BF16 weights, FP32 "
-                               "accumulation, on top of block-Jacobi, trained on the GPU on this workload's own "
-                               "harvested SPGMR solves) + mixed-precision demag"),
+                               "accumulation, fused tcgen05 inference, on top of block-Jacobi, trained on the GPU on "
+                               "this workload's own harvested SPGMR solves; every 8th solve probes block-Jacobi and "
+                               "the learned path stays only while it pays for its cost) + mixed-precision demag"),
 }
 BEST_FORM = "learned+mixed"
 TRAIN = dict(t_harvest=1.0, max_samples=32, stride=2, iters=600, batch=16, patch=32, seed=5, lr=3e-3,

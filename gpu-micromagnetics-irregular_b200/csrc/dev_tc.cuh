@@ -38,6 +38,11 @@ __host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N, int a_mn_majo
          ((uint32_t)(M >> 4) << 24);
 }
 
+// kind::f16 with BF16 A and B (bits 7-9 = 1, 10-12 = 1), D f32
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, int a_mn_major, int b_mn_major) {
+  return idesc_f16_f32(M, N, a_mn_major, b_mn_major) | (1u << 7) | (1u << 10);
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void fence_proxy_async_smem() {

@@ -74,6 +74,13 @@ struct Integrator {
             npe = 0, nstlp = 0, nstlj = 0, nscon = 0;
   int err = 0;  // sticky CUDA/launch failure
   bool ycor_zero = false;  // acor holds the zero vector implicitly (not yet written)
+  // learned-preconditioner policy: every PROBE_EVERY-th solve runs block-
+  // Jacobi; once both sides have enough solves, the learned path stays only
+  // if its iterations are cheaper than block-Jacobi's at the measured cost
+  // ratio kappa = (learned application) / (fused Arnoldi operator)
+  static constexpr int PROBE_EVERY = 8, MIN_LEARNED = 24, MIN_PROBES = 4;
+  long long pol_solves = 0, nsl = 0, nil = 0, nsb = 0, nib = 0;
+  double kappa = -1.0;
 
   // ── helpers ──
   bool ok(int rc) {
@@ -195,12 +202,11 @@ struct Integrator {
     return code;
   }
 
-  int spgmr(double* rhs, double delta_tol) {
+  int spgmr(double* rhs, double delta_tol, bool learned) {
     const int lmax = maxl;
     int nl = 0, krydim = 0, converged = 0;
     nps++;
     double ss = 0.0;
-    const bool learned = learned_active(c);
     const bool harvest = !learned && learned_harvest_wanted(c);
     double* zb = (learned || harvest) ? learned_zbuf(c) : nullptr;
     if ((learned || harvest) && !zb) return LS_CONV_FAIL;
@@ -224,7 +230,22 @@ struct Integrator {
       krydim = l + 1;
       njv++;
       nps++;
-      if (learned) {
+      if (learned && kappa < 0.0) {
+        // one-time cost ratio of the learned application to the Arnoldi operator
+        cudaEvent_t e[3];
+        for (auto& ev : e) cudaEventCreate(&ev);
+        cudaEventRecord(e[0], c->stream);
+        ok(launch_arnoldi_op(c, V[l], ewt, zb, y, gamma, 0));
+        cudaEventRecord(e[1], c->stream);
+        ok(learned_apply(c, ewt, V[l + 1], -1));
+        cudaEventRecord(e[2], c->stream);
+        cudaEventSynchronize(e[2]);
+        float ta = 0.f, tl = 0.f;
+        cudaEventElapsedTime(&ta, e[0], e[1]);
+        cudaEventElapsedTime(&tl, e[1], e[2]);
+        for (auto& ev : e) cudaEventDestroy(ev);
+        kappa = (ta > 0.f) ? (double)tl / ta : 1.0;
+      } else if (learned) {
         ok(launch_arnoldi_op(c, V[l], ewt, zb, y, gamma, 0));
         ok(learned_apply(c, ewt, V[l + 1], -1));
       } else {
@@ -400,13 +421,31 @@ struct Integrator {
   int nls_lsolve(double* del) {
     const double deltar = LS_EPLIN * tq[4];
     const double dtol = deltar * sqrt((double)neq);
-    const bool learned = learned_active(c);
-    const int r = spgmr(del, dtol);
+    bool learned = learned_active(c);
+    bool probe = false;
+    if (learned && learned_policy_on(c) && (pol_solves++ % PROBE_EVERY) == PROBE_EVERY - 1) {
+      learned = false;
+      probe = true;
+    }
+    const long long nli0 = nli;
+    const int r = spgmr(del, dtol, learned);
     if (err) return LLG_CV_LSOLVE_FAIL;
+    if (learned) { nsl++; nil += nli - nli0; }
+    if (probe) { nsb++; nib += nli - nli0; }
+    if ((learned || probe) && nsl >= MIN_LEARNED && nsb >= MIN_PROBES && kappa >= 0.0) {
+      // per solve, in Arnoldi-operator units: each iteration costs the operator
+      // plus ~0.6 for Gram-Schmidt; the learned path adds kappa per application
+      // (one per iteration plus the first Krylov vector)
+      const double itl = (double)nil / nsl, itb = (double)nib / nsb;
+      const double cost_l = itl * 1.6 + (itl + 1.0) * kappa, cost_b = itb * 1.6;
+      learned_policy_record(c, itl, itb, kappa);
+      if (cost_l >= cost_b) learned_fall_back(c, 2);
+      nsl = nil = nsb = nib = 0;   // judge again on fresh counts if it stays
+    }
     // GMRES convergence judges the learned preconditioner: a failed solve
     // switches this context back to block-Jacobi (the Newton iteration then
     // recovers as after any linear-solver failure)
-    if (learned && (r == LS_CONV_FAIL || r == LS_QRSOL_FAIL)) learned_fall_back(c);
+    if (learned && (r == LS_CONV_FAIL || r == LS_QRSOL_FAIL)) learned_fall_back(c, 1);
     if (r != LS_SUCCESS) nlcf++;
     if (r == LS_SUCCESS) return 0;
     if (r == LS_RES_REDUCED) return (ls_curiter == 0) ? 0 : 1;

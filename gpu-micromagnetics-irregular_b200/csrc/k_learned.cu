@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "dev_reduce.cuh"
+#include "dev_tc.cuh"
 #include "llg_internal.h"
 
 namespace {
@@ -309,18 +310,224 @@ __global__ void k_round_bf16(const float* __restrict__ w, float* __restrict__ wq
 
 dim3 conv_grid(int H, int W, int B) { return dim3((W + TW - 1) / TW, (H + TH - 1) / TH, B); }
 
+// ── fused inference on the tensor cores (tcgen05, BF16 operands, FP32 accumulation) ──
+// One CTA computes a 32x16 tile of outputs.  The three layers run over the
+// tile's 38x22 input region (3-cell halo) held in shared memory as BF16
+// activations, laid out [channel chunk of 8][pixel] with one 16-byte row per
+// pixel and chunk; that is the K-major operand layout (8-pixel core matrices,
+// SBO = 128 B, LBO = one chunk), so the operand of 3x3 tap (dy, dx) for 128
+// consecutive pixels is the same layout started dy*38 + dx pixels later: each
+// layer is 9 MMAs (M = 128 pixels, N = 16 channels, K = 16) per 128-pixel
+// block, accumulated in tensor memory.  Pixels whose taps wrap across the
+// region's rows sit in its outer ring, which the next layer's valid outputs
+// never read; cells outside the grid are zeroed after every layer (the
+// layer-wise zero padding of the network).
+constexpr int FO_W = 32, FO_H = 16;
+constexpr int FS_W = FO_W + 6, FS_H = FO_H + 6, FNPIX = FS_W * FS_H;   // 38 x 22 = 836
+constexpr int FNBLK = (FNPIX + 127) / 128, FNPP = FNBLK * 128;          // 7 blocks, 896
+constexpr int FMG = 40;                                                 // zero margin >= 38 + 1
+constexpr int FCHUNK = (FNPP + 2 * FMG) * 16;                           // bytes per 8-channel chunk
+constexpr int FBUF = 2 * FCHUNK;                                        // 16 channels
+constexpr int FWB = 27 * 512;                                           // 3 layers x 9 taps x (16x16 BF16)
+constexpr int FSMEM = FWB + 2 * FBUF;
+constexpr uint32_t FTMEM = 128;
+
+struct InferArgs {
+  const double* z;
+  const double* pm;
+  const uint8_t* act;
+  const double* ewt;
+  double* out;
+  const uint4* wpack;
+  double gamma;
+  int ng, ny, ntx, ntiles;
+  double* partials;
+  unsigned int* counter;
+  double* res;
+  int* err;
+};
+
+union B8 {
+  __nv_bfloat16 h[8];
+  uint4 u;
+};
+
+constexpr int FNT = 512;   // 16 warps: 4 lane quarters x 4 block groups
+
+__global__ void __launch_bounds__(FNT, 2) k_learned_fused(InferArgs a) {
+  extern __shared__ __align__(1024) unsigned char smf[];
+  unsigned char* sW = smf;
+  unsigned char* const buf0 = smf + FWB;
+  unsigned char* const buf1 = smf + FWB + FBUF;
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tslot;
+  __shared__ int s_fail;
+  __shared__ double red[FNT / 32];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, q = warp & 3, hs = warp >> 2;
+  const int n = a.ng * a.ny;
+  for (int i = tid; i < FWB / 16; i += FNT) reinterpret_cast<uint4*>(sW)[i] = a.wpack[i];
+  for (int i = tid; i < 2 * FBUF / 16; i += FNT) reinterpret_cast<uint4*>(buf0)[i] = make_uint4(0, 0, 0, 0);
+  if (warp == 0) tmem_alloc(&tslot, FTMEM);
+  if (tid == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+    s_fail = 0;
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tslot;
+  uint32_t phase = 0;
+  double acc[1] = {0.0};
+  bool good = true;
+  for (int tile = blockIdx.x; tile < a.ntiles && good; tile += gridDim.x) {
+    const int x0 = (tile % a.ntx) * FO_W - 3, y0 = (tile / a.ntx) * FO_H - 3;
+    // features -> buf0
+    for (int p = tid; p < FNPP; p += FNT) {
+      float f[16];
+#pragma unroll
+      for (int k = 0; k < 16; k++) f[k] = 0.f;
+      const int gx = x0 + p % FS_W, gy = y0 + p / FS_W;
+      if (p < FNPIX && gx >= 0 && gx < a.ng && gy >= 0 && gy < a.ny) {
+        const int cell = gy * a.ng + gx;
+        if (!a.act || a.act[cell]) {
+          const float u0 = (float)a.z[cell], u1 = (float)a.z[n + cell], u2 = (float)a.z[2 * n + cell];
+          const float m0 = (float)a.pm[cell], m1 = (float)a.pm[n + cell], m2 = (float)a.pm[2 * n + cell];
+          const float a0 = m1 * u2 - m2 * u1, a1 = m2 * u0 - m0 * u2, a2 = m0 * u1 - m1 * u0;
+          f[0] = u0; f[1] = u1; f[2] = u2; f[3] = a0; f[4] = a1; f[5] = a2;
+          f[6] = m1 * a2 - m2 * a1; f[7] = m2 * a0 - m0 * a2; f[8] = m0 * a1 - m1 * a0;
+        }
+      }
+      B8 c0, c1;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        c0.h[k] = __float2bfloat16_rn(f[k]);
+        c1.h[k] = __float2bfloat16_rn(f[8 + k]);
+      }
+      *reinterpret_cast<uint4*>(buf0 + (FMG + p) * 16) = c0.u;
+      *reinterpret_cast<uint4*>(buf0 + FCHUNK + (FMG + p) * 16) = c1.u;
+    }
+    for (int l = 0; l < 3 && good; l++) {
+      unsigned char* src = (l & 1) ? buf1 : buf0;
+      unsigned char* dst = (l & 1) ? buf0 : buf1;
+      fence_proxy_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t idesc = idesc_bf16_f32(128, 16, 0, 0);
+        for (int b = 0; b < FNBLK; b++)
+          for (int t = 0; t < 9; t++) {
+            const int sh = (t / 3 - 1) * FS_W + (t % 3 - 1);
+            const uint32_t A = smem_u32(src) + (uint32_t)((FMG + 128 * b + sh) * 16);
+            tc_mma_f16(tbase + 16 * b, smem_desc(A, FCHUNK, 128), smem_desc(smem_u32(sW) + (l * 9 + t) * 512, 128, 256),
+                       idesc, t > 0 ? 1u : 0u);
+          }
+        tc_commit(&mbar);
+      }
+      const bool ok = mbar_wait(&mbar, phase, 1u << 22);
+      if (!ok) atomicExch(&s_fail, 1);
+      __syncthreads();
+      if (s_fail) { good = false; break; }
+      phase ^= 1u;
+      tc_fence_after();
+      for (int b = hs; b < FNBLK; b += FNT / 128) {
+        float v[16];
+        tmem_ld16(tbase + ((uint32_t)(32 * q) << 16) + 16 * b, v);
+        const int p = 128 * b + 32 * q + lane;
+        const int ix = p % FS_W, jy = p / FS_W;
+        const int gx = x0 + ix, gy = y0 + jy;
+        const bool inside = p < FNPIX && gx >= 0 && gx < a.ng && gy >= 0 && gy < a.ny;
+        if (l < 2) {
+          B8 c0, c1;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            c0.h[k] = __float2bfloat16_rn(inside ? v[k] : 0.f);
+            c1.h[k] = __float2bfloat16_rn(inside ? v[8 + k] : 0.f);
+          }
+          *reinterpret_cast<uint4*>(dst + (FMG + p) * 16) = c0.u;
+          *reinterpret_cast<uint4*>(dst + FCHUNK + (FMG + p) * 16) = c1.u;
+        } else if (inside && ix >= 3 && ix < FS_W - 3 && jy >= 3 && jy < FS_H - 3) {
+          const int cell = gy * a.ng + gx;
+          const double k = (!a.act || a.act[cell]) ? 1.0 : 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const int i = c * n + cell;
+            const double o = a.ewt[i] * ((a.z[i] + a.gamma * (double)v[c]) * k);
+            a.out[i] = o;
+            acc[0] += o * o;
+          }
+        }
+      }
+    }
+  }
+  if (!good) {
+    if (tid == 0) atomicExch(a.err, 1);
+    mbar_wait(&mbar, phase, 1u << 22);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tbase, FTMEM);
+  }
+  if (a.res && good) {
+    // deterministic sum of out^2: warp trees, warps in order, CTAs in order
+    // by the last CTA to finish (ticket), counter reset for the next use
+    __shared__ bool last;
+    const double v = warp_sum(acc[0]);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < FNT / 32; w++) t += red[w];
+      a.partials[blockIdx.x] = t;
+      __threadfence();
+      last = (atomicAdd(a.counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && tid == 0) {
+      __threadfence();
+      double t = 0.0;
+      for (int k = 0; k < (int)gridDim.x; k++) t += ((volatile double*)a.partials)[k];
+      *a.res = t;
+      *a.counter = 0u;
+    }
+  }
+}
+
+// FP32 weights -> BF16 B operands: layer l, tap t: (n = out channel, k = in
+// channel) K-major, 16 x 16, LBO 128, SBO 256; absent channels zero
+__global__ void k_pack_weights(const float* __restrict__ w, uint16_t* __restrict__ pk) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;   // over 27 * 256 entries
+  if (e >= 27 * 256) return;
+  const int lt = e / 256, l = lt / 9, t = lt % 9, nn = (e % 256) / 16, kk = e % 16;
+  const int cin = (l == 0) ? CIN0 : CH, cout = (l == 2) ? COUT3 : CH;
+  const int base = (l == 0) ? 0 : (l == 1 ? NW1 : NW1 + NW2);
+  float v = 0.f;
+  if (nn < cout && kk < cin) v = w[base + (nn * cin + kk) * 9 + t];
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  pk[(lt * 512 + off_kmajor(nn, kk, 128, 256)) / 2] = *reinterpret_cast<const uint16_t*>(&h);
+}
+
 }  // namespace
 
 // ── host side ──────────────────────────────────────────────────────────
 struct Learned {
   // weights
   float* d_w = nullptr;      // FP32 master (training)
-  float* d_wq = nullptr;     // BF16-rounded copy used by inference
+  float* d_wq = nullptr;     // BF16-rounded copy (FP32 reference inference path)
+  uint16_t* d_wpack = nullptr;  // BF16 tensor-core operands of the fused inference kernel
+  int* d_err = nullptr;
+  bool fused = true;         // fused tensor-core inference (else the FP32 layer-by-layer path)
   float* d_g = nullptr;
   float* d_m1 = nullptr;
   float* d_m2 = nullptr;
   bool have_weights = false;
-  int fell_back = 0;         // block-Jacobi fallback engaged
+  int fell_back = 0;         // block-Jacobi fallback: 1 failed solve, 2 not worth its cost
+  double pol_it_learned = -1.0, pol_it_bj = -1.0, pol_kappa = -1.0;   // last policy judgement
+  int policy = 1;            // 1: cost-aware probing, 0: learned on every solve
   long long napply = 0;
   // inference scratch (whole grid)
   float* d_f = nullptr;      // 9N
@@ -337,6 +544,8 @@ struct Learned {
 static void lfree(Learned* l) {
   float* fs[] = {l->d_w, l->d_wq, l->d_g, l->d_m1, l->d_m2, l->d_f, l->d_a1, l->d_a2, l->d_y3};
   for (float* p : fs) cudaFree(p);
+  cudaFree(l->d_wpack);
+  cudaFree(l->d_err);
   cudaFree(l->d_z);
   for (auto* p : l->hu) cudaFree(p);
   for (auto* p : l->hx) cudaFree(p);
@@ -356,13 +565,22 @@ static int learned_get(llg_ctx* c, Learned** out) {
     const size_t wb = sizeof(float) * NWT;
     if (cudaMalloc(&l->d_w, wb) != cudaSuccess || cudaMalloc(&l->d_wq, wb) != cudaSuccess ||
         cudaMalloc(&l->d_g, wb) != cudaSuccess || cudaMalloc(&l->d_m1, wb) != cudaSuccess ||
-        cudaMalloc(&l->d_m2, wb) != cudaSuccess) {
+        cudaMalloc(&l->d_m2, wb) != cudaSuccess || cudaMalloc(&l->d_wpack, FWB) != cudaSuccess ||
+        cudaMalloc(&l->d_err, sizeof(int)) != cudaSuccess) {
       learned_destroy(l);
       llg_set_error("learned: weight allocation failed");
       return LLG_ERR_NOMEM;
     }
     cudaMemset(l->d_w, 0, wb);
     cudaMemset(l->d_wq, 0, wb);
+    cudaMemset(l->d_wpack, 0, FWB);
+    cudaMemset(l->d_err, 0, sizeof(int));
+    if (cudaFuncSetAttribute((const void*)k_learned_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, FSMEM) !=
+        cudaSuccess) {
+      learned_destroy(l);
+      llg_set_error("learned: shared-memory opt-in failed");
+      return LLG_ERR_CUDA;
+    }
     c->learned = l;
   }
   *out = c->learned;
@@ -405,6 +623,24 @@ int learned_apply(llg_ctx* c, const double* ewt, double* out, int slot) {
   int rc = ensure_infer_scratch(c, l);
   if (rc) return rc;
   const int n = c->ncell;
+  if (l->fused) {
+    InferArgs a{};
+    a.z = l->d_z; a.pm = c->d_pm; a.act = c->d_act; a.ewt = ewt; a.out = out;
+    a.wpack = reinterpret_cast<const uint4*>(l->d_wpack);
+    a.gamma = c->gamma_setup;
+    a.ng = c->p.ng; a.ny = c->p.ny;
+    a.ntx = (c->p.ng + FO_W - 1) / FO_W;
+    a.ntiles = a.ntx * ((c->p.ny + FO_H - 1) / FO_H);
+    a.partials = c->d_red; a.counter = c->d_counter;
+    a.res = slot >= 0 ? c->d_scal + slot : nullptr;
+    a.err = l->d_err;
+    const int grid = std::min(a.ntiles, 2 * c->num_sms);
+    LLG_COUNT(KID_LEARNED);
+    k_learned_fused<<<grid, FNT, FSMEM, c->stream>>>(a);
+    LLG_CUDA_TRY(cudaPeekAtLastError());
+    l->napply++;
+    return 0;
+  }
   LLG_COUNT(KID_LEARNED);
   k_feat_grid<<<c->num_sms * 8, 256, 0, c->stream>>>(l->d_z, c->d_pm, c->d_act, n, l->d_f);
   if ((rc = net_forward(c->stream, l->d_wq, l->d_f, l->d_a1, l->d_a2, l->d_y3, 1, c->p.ny, c->p.ng))) return rc;
@@ -426,8 +662,17 @@ bool learned_active(llg_ctx* c) {
   return c->p.precond_kind == LLG_PREC_LEARNED && c->learned && c->learned->have_weights && !c->learned->fell_back;
 }
 
-void learned_fall_back(llg_ctx* c) {
-  if (c->learned) c->learned->fell_back = 1;
+void learned_fall_back(llg_ctx* c, int reason) {
+  if (c->learned) c->learned->fell_back = reason;
+}
+
+bool learned_policy_on(llg_ctx* c) { return c->learned && c->learned->policy; }
+
+void learned_policy_record(llg_ctx* c, double it_learned, double it_bj, double kappa) {
+  if (!c->learned) return;
+  c->learned->pol_it_learned = it_learned;
+  c->learned->pol_it_bj = it_bj;
+  c->learned->pol_kappa = kappa;
 }
 
 // ── harvesting (called by the integrator after a converged block-Jacobi solve) ──
@@ -562,6 +807,7 @@ int llg_learned_set_weights(llg_ctx* c, const float* h_w, int32_t n) {
   if (rc) return rc;
   LLG_CUDA_TRY(cudaMemcpy(l->d_w, h_w, sizeof(float) * NWT, cudaMemcpyHostToDevice));
   k_round_bf16<<<(NWT + 255) / 256, 256, 0, c->stream>>>(l->d_w, l->d_wq, NWT);
+  k_pack_weights<<<(27 * 256 + 255) / 256, 256, 0, c->stream>>>(l->d_w, l->d_wpack);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
   l->have_weights = true;
@@ -573,6 +819,60 @@ int llg_learned_get_weights(llg_ctx* c, float* h_w, int32_t n) {
   if (!c || !h_w || n != NWT || !c->learned) { llg_set_error("llg_learned_get_weights: no weights"); return LLG_ERR_ARG; }
   LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
   LLG_CUDA_TRY(cudaMemcpy(h_w, c->learned->d_w, sizeof(float) * NWT, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int llg_learned_policy(llg_ctx* c, double* it_learned, double* it_bj, double* kappa) {
+  if (!c) return LLG_ERR_ARG;
+  const Learned* l = c->learned;
+  if (it_learned) *it_learned = l ? l->pol_it_learned : -1.0;
+  if (it_bj) *it_bj = l ? l->pol_it_bj : -1.0;
+  if (kappa) *kappa = l ? l->pol_kappa : -1.0;
+  return 0;
+}
+
+int llg_learned_set_policy(llg_ctx* c, int32_t cost_aware) {
+  if (!c) return LLG_ERR_ARG;
+  Learned* l;
+  int rc = learned_get(c, &l);
+  if (rc) return rc;
+  l->policy = cost_aware != 0;
+  return 0;
+}
+
+int llg_learned_set_fused(llg_ctx* c, int32_t fused) {
+  if (!c) return LLG_ERR_ARG;
+  Learned* l;
+  int rc = learned_get(c, &l);
+  if (rc) return rc;
+  l->fused = fused != 0;
+  return 0;
+}
+
+// out = ewt (z + gamma Net(z; pm)) on active cells for caller-given z, frozen
+// m (pm) and gamma (checker entry point of the inference kernels); writes
+// sum out^2 to *norm2 when it is not null
+int llg_learned_apply(llg_ctx* c, const double* d_z, const double* d_pm, const double* d_ewt, double gamma,
+                      double* d_out, double* norm2) {
+  if (!c || !d_z || !d_pm || !d_ewt || !d_out) return LLG_ERR_ARG;
+  if (!c->learned || !c->learned->have_weights) { llg_set_error("llg_learned_apply: no weights"); return LLG_ERR_STATE; }
+  int rc = ensure_infer_scratch(c, c->learned);
+  if (rc) return rc;
+  const size_t vb = sizeof(double) * 3 * (size_t)c->ncell;
+  LLG_CUDA_TRY(cudaMemcpyAsync(c->learned->d_z, d_z, vb, cudaMemcpyDeviceToDevice, c->stream));
+  LLG_CUDA_TRY(cudaMemcpyAsync(c->d_pm, d_pm, vb, cudaMemcpyDeviceToDevice, c->stream));
+  const double g0 = c->gamma_setup;
+  c->gamma_setup = gamma;
+  rc = learned_apply(c, d_ewt, d_out, 60);
+  c->gamma_setup = g0;
+  if (rc) return rc;
+  double s = 0.0;
+  LLG_CUDA_TRY(cudaMemcpyAsync(&s, c->d_scal + 60, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  int fail = 0;
+  LLG_CUDA_TRY(cudaMemcpy(&fail, c->learned->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (fail) { llg_set_error("learned inference: a tensor-core completion wait ran out"); return LLG_ERR_TIMEOUT; }
+  if (norm2) *norm2 = s;
   return 0;
 }
 
@@ -648,6 +948,7 @@ int llg_learned_train(llg_ctx* c, const llg_train_opts* o, double* loss_first, d
     LLG_CUDA_TRY(cudaPeekAtLastError());
   }
   k_round_bf16<<<(NWT + 255) / 256, 256, 0, s>>>(l->d_w, l->d_wq, NWT);
+  k_pack_weights<<<(27 * 256 + 255) / 256, 256, 0, s>>>(l->d_w, l->d_wpack);
   LLG_CUDA_TRY(cudaStreamSynchronize(s));
   t.release();
   l->have_weights = true;

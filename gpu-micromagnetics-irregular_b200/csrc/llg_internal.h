@@ -140,7 +140,9 @@ int demag_check(llg_ctx* c);
 bool learned_active(llg_ctx* c);                 // LLG_PREC_LEARNED with weights, no fallback
 double* learned_zbuf(llg_ctx* c);                // 3N scratch for the block-Jacobi stage
 int learned_apply(llg_ctx* c, const double* ewt, double* out, int slot /* <0: no norm */);
-void learned_fall_back(llg_ctx* c);
+void learned_fall_back(llg_ctx* c, int reason /* 1 failed solve, 2 cost */);
+void learned_policy_record(llg_ctx* c, double it_learned, double it_bj, double kappa);
+bool learned_policy_on(llg_ctx* c);
 bool learned_harvest_wanted(llg_ctx* c);
 int learned_harvest(llg_ctx* c, const double* u, const double* x, const double* ewt, double gamma);
 

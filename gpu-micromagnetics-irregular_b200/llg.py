@@ -210,6 +210,10 @@ def load(path: str | None = None):
         "llg_learned_set_weights": (I, [VP, P(C.c_float), C.c_int32]),
         "llg_learned_get_weights": (I, [VP, P(C.c_float), C.c_int32]),
         "llg_learned_status": (I, [VP, P(C.c_int32), P(C.c_int32), P(C.c_int64)]),
+        "llg_learned_set_fused": (I, [VP, C.c_int32]),
+        "llg_learned_policy": (I, [VP, P(D), P(D), P(D)]),
+        "llg_learned_set_policy": (I, [VP, C.c_int32]),
+        "llg_learned_apply": (I, [VP, VP, VP, VP, D, VP, P(D)]),
         "llg_learned_loss_grad": (I, [P(C.c_float), C.c_int32, C.c_int32] + [P(C.c_float)] * 6
                                   + [P(D), P(C.c_float), P(C.c_float)]),
     }
@@ -378,10 +382,25 @@ class Context:
                "llg_learned_get_weights")
         return w
 
+    def learned_set_policy(self, cost_aware: bool):
+        _check(self.lib.llg_learned_set_policy(self.h, int(bool(cost_aware))), "llg_learned_set_policy")
+
+    def learned_set_fused(self, fused: bool):
+        _check(self.lib.llg_learned_set_fused(self.h, int(bool(fused))), "llg_learned_set_fused")
+
+    def learned_apply(self, z, m, ewt, gamma, out):
+        n2 = C.c_double()
+        _check(self.lib.llg_learned_apply(self.h, _ptr(z), _ptr(m), _ptr(ewt), float(gamma), _ptr(out),
+                                          C.byref(n2)), "llg_learned_apply")
+        return n2.value
+
     def learned_status(self):
         a, f, n = C.c_int32(), C.c_int32(), C.c_int64()
         _check(self.lib.llg_learned_status(self.h, C.byref(a), C.byref(f), C.byref(n)), "llg_learned_status")
-        return {"active": a.value, "fell_back": f.value, "napply": n.value}
+        il, ib, k = C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib.llg_learned_policy(self.h, C.byref(il), C.byref(ib), C.byref(k)), "llg_learned_policy")
+        return {"active": a.value, "fell_back": f.value, "napply": n.value, "it_learned": il.value,
+                "it_block_jacobi": ib.value, "kappa": k.value}
 
 
 def learned_loss_grad(w, u, m, mask, ewt, x, gamma, want_z=True):

@@ -249,6 +249,23 @@ int  llg_learned_train(llg_ctx* ctx, const llg_train_opts* o, double* loss_first
 int  llg_learned_set_weights(llg_ctx* ctx, const float* h_w, int32_t n);
 int  llg_learned_get_weights(llg_ctx* ctx, float* h_w, int32_t n);
 int  llg_learned_status(llg_ctx* ctx, int32_t* active, int32_t* fell_back, int64_t* napply);
+/* The integrator's cost judgement (every 8th solve of a learned context runs
+ * block-Jacobi as a probe): mean GMRES iterations per solve with the learned
+ * and with the block-Jacobi preconditioner, and kappa = time of one learned
+ * application / one fused Arnoldi operator step; -1 before the first
+ * judgement.  fell_back in llg_learned_status: 0 none, 1 a learned solve
+ * failed, 2 the learned path did not pay for its cost.                     */
+int  llg_learned_policy(llg_ctx* ctx, double* it_learned, double* it_bj, double* kappa);
+/* 1 (default): the cost-aware probing above; 0: learned on every solve.    */
+int  llg_learned_set_policy(llg_ctx* ctx, int32_t cost_aware);
+/* Inference path: 1 (default) one fused tensor-core kernel (tcgen05, BF16
+ * operands and activations, FP32 accumulation); 0 layer-by-layer FP32
+ * kernels with the same BF16-rounded weights (reference path).             */
+int  llg_learned_set_fused(llg_ctx* ctx, int32_t fused);
+/* d_out = ewt (z + gamma Net(z; m)) on active cells for device z, m, ewt;
+ * *norm2 = sum d_out^2 (may be NULL).                                      */
+int  llg_learned_apply(llg_ctx* ctx, const double* d_z, const double* d_m, const double* d_ewt, double gamma,
+                       double* d_out, double* norm2);
 /* Loss, weight gradient and output z of the training kernels on host FP32
  * patches [nb][3][P][P] (mask [nb][P][P], gamma [nb]); h_z may be NULL.     */
 int  llg_learned_loss_grad(const float* h_w, int32_t nb, int32_t P, const float* h_u, const float* h_m,

@@ -81,6 +81,7 @@ def test_trained_network_lowers_gmres_iterations(gpu):
     _, base = _integrate(torch, _ctx(llg.PREC_BLOCK_JACOBI, ng, ny, act), geo, 2.0, opts)
     cl = _ctx(llg.PREC_LEARNED, ng, ny, act)
     cl.learned_set_weights(w)
+    cl.learned_set_policy(False)   # learned on every solve: the network's own effect
     _, lrn = _integrate(torch, cl, geo, 2.0, opts)
     status = cl.learned_status()
     it_b = base["nli"] / base["nni"]
@@ -96,3 +97,69 @@ def _ctx(precond, ng, ny, act):
     c = llg.Context(p)
     c.set_mask(act)
     return c
+
+
+@pytest.mark.parametrize("ng,ny", [(70, 45), (96, 64)])
+def test_inference_paths_match_fp64_oracle(gpu, ng, ny):
+    """Fused tensor-core inference (BF16 activations) and the layer-by-layer
+    FP32 path against the FP64 network with the same BF16-rounded weights,
+    on a grid that is not a multiple of the 32x16 tile, with a hole."""
+    import torch
+    rng = np.random.default_rng(17)
+    theta = (rng.standard_normal(L.nparams()) * 0.15).astype(np.float32)
+    # BF16 rounding (round to nearest even on the upper 16 bits)
+    bits = theta.view(np.uint32).astype(np.uint64)
+    bits = ((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16) << 16
+    theta_bf = bits.astype(np.uint32).view(np.float32).astype(np.float64)
+    n = ng * ny
+    mask = np.ones((ny, ng))
+    mask[ny // 3: ny // 3 + 9, ng // 2: ng // 2 + 13] = 0.0
+    z = rng.standard_normal((3, ny, ng)) * mask[None]
+    m = rng.standard_normal((3, ny, ng))
+    m /= np.linalg.norm(m, axis=0, keepdims=True)
+    ewt = rng.uniform(0.5, 2.0, (3, ny, ng))
+    gamma = 0.03
+    zr, _ = L.forward(theta_bf, z, m, mask, gamma)
+    ref = (ewt * zr).ravel()
+    corr = np.abs(ref - (ewt * z * mask[None]).ravel()).max()
+    p = llg.default_params(ng, ny, precond_kind=llg.PREC_LEARNED)
+    ctx = llg.Context(p)
+    ctx.set_mask(np.tile(mask.ravel(), 3))
+    ctx.learned_set_weights(theta)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a.ravel())).cuda()  # noqa: E731
+    dz, dm, de = d(z), d(m), d(ewt)
+    outs = {}
+    for fused in (1, 0):
+        ctx.learned_set_fused(fused)
+        o = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+        n2 = ctx.learned_apply(dz, dm, de, gamma, o)
+        outs[fused] = (o.cpu().numpy(), n2)
+    ef = np.abs(outs[1][0] - ref).max() / corr
+    er = np.abs(outs[0][0] - ref).max() / corr
+    print(f"{ng}x{ny}: fused (BF16 activations) {ef:.2e}, FP32 layers {er:.2e} of max |correction| {corr:.3e}")
+    assert er <= 1e-5
+    assert ef <= 3e-2
+    assert abs(outs[1][1] - np.sum(outs[1][0] ** 2)) <= 1e-10 * outs[1][1]
+
+
+def test_cost_aware_policy_judges_on_the_same_trajectory(gpu):
+    """Default policy: every 8th solve is a block-Jacobi probe on the same
+    trajectory; the judgement (iterations of both, cost ratio kappa) is
+    recorded and the context keeps the learned path only if it pays."""
+    import torch
+    ng, ny = 192, 128
+    opts = llg.default_solver_opts()
+    p, geo = _film(ng, ny, llg.PREC_BLOCK_JACOBI)
+    act = np.tile(geo["active"].astype(np.float64), 3)
+    ch = _ctx(llg.PREC_BLOCK_JACOBI, ng, ny, act)
+    ch.learned_harvest(32, 1)
+    _integrate(torch, ch, geo, 0.6, opts)
+    ch.learned_train(iters=300, batch=16, patch=32, seed=5, lr=3e-3, init_scale=0.05)
+    cl = _ctx(llg.PREC_LEARNED, ng, ny, act)
+    cl.learned_set_weights(ch.learned_get_weights())
+    _integrate(torch, cl, geo, 2.0, opts)
+    st = cl.learned_status()
+    print("policy", st)
+    assert st["kappa"] > 0.0 and st["it_learned"] > 0.0 and st["it_block_jacobi"] > 0.0
+    pays = st["it_learned"] * 1.6 + (st["it_learned"] + 1.0) * st["kappa"] < st["it_block_jacobi"] * 1.6
+    assert st["fell_back"] == (0 if pays else 2)
