@@ -1,0 +1,121 @@
+// batch.cpp — many independent LLG instances of uneven size on one GPU.
+//
+// The reference runs one geometry per process.  Here a batch owns one
+// context per instance, each on its own CUDA stream, and integrates them
+// concurrently: a pool of host threads takes instances largest-first (cells
+// as the cost estimate, longest-processing-time order) and drives each
+// instance's integrator on its stream, so the kernels of small instances
+// overlap on the GPU instead of serialising behind each other's host syncs.
+// On a context's own stream the demag chain is replayed as a captured CUDA
+// graph, and every demag plan picks its transform launch shapes by timing
+// (k_demag.cu, autotune; cached per transform size, so instances of one size
+// tune once).
+#include <algorithm>
+#include <atomic>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "llg_internal.h"
+
+struct llg_batch {
+  std::vector<llg_ctx*> ctx;
+  std::vector<cudaStream_t> streams;
+  int device = 0;
+};
+
+extern "C" {
+
+int llg_batch_create(int32_t n, const llg_params* params, llg_batch** out) {
+  if (!out || n < 1 || !params) { llg_set_error("llg_batch_create: bad argument"); return LLG_ERR_ARG; }
+  *out = nullptr;
+  llg_batch* b = new llg_batch();
+  cudaGetDevice(&b->device);
+  for (int i = 0; i < n; i++) {
+    llg_ctx* c = nullptr;
+    int rc = llg_create(&params[i], &c);
+    cudaStream_t s = nullptr;
+    if (!rc && cudaStreamCreate(&s) != cudaSuccess) {
+      llg_destroy(c);
+      llg_set_error("llg_batch_create: stream creation failed");
+      rc = LLG_ERR_CUDA;
+    }
+    if (rc) {
+      llg_batch_destroy(b);
+      return rc;
+    }
+    llg_set_stream(c, s);
+    b->ctx.push_back(c);
+    b->streams.push_back(s);
+  }
+  *out = b;
+  return 0;
+}
+
+int llg_batch_size(const llg_batch* b) { return b ? (int)b->ctx.size() : 0; }
+
+llg_ctx* llg_batch_ctx(llg_batch* b, int32_t i) {
+  if (!b || i < 0 || i >= (int)b->ctx.size()) return nullptr;
+  return b->ctx[i];
+}
+
+int llg_batch_integrator_init(llg_batch* b, double t0, const double* const* d_y0, const llg_solver_opts* o) {
+  if (!b || !d_y0 || !o) return LLG_ERR_ARG;
+  // the caller's y0 may still be in flight on the legacy default stream
+  if (cudaDeviceSynchronize() != cudaSuccess) { llg_set_error("llg_batch_integrator_init: device sync"); return LLG_ERR_CUDA; }
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    const int rc = llg_integrator_init(b->ctx[i], t0, d_y0[i], o);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int llg_batch_integrate(llg_batch* b, double tout, double* const* d_yout, int32_t nthreads, int32_t* rcs) {
+  if (!b || !d_yout) return LLG_ERR_ARG;
+  const int n = (int)b->ctx.size();
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->ctx[a]->ncell > b->ctx[c]->ncell; });
+  std::vector<int> rc(n, 0);
+  std::atomic<int> next{0};
+  std::vector<std::string> errs(n);
+  auto worker = [&]() {
+    cudaSetDevice(b->device);
+    for (;;) {
+      const int k = next.fetch_add(1);
+      if (k >= n) break;
+      const int i = order[k];
+      double tret = 0.0;
+      rc[i] = llg_integrate(b->ctx[i], tout, d_yout[i], &tret);
+      if (rc[i]) errs[i] = llg_last_error();
+      if (!rc[i] && cudaStreamSynchronize(b->streams[i]) != cudaSuccess) rc[i] = LLG_ERR_CUDA;
+    }
+  };
+  const int nt = std::max(1, std::min(nthreads > 0 ? nthreads : n, n));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; t++) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
+  int first = 0;
+  for (int i = 0; i < n; i++) {
+    if (rcs) rcs[i] = rc[i];
+    if (rc[i] && !first) {
+      first = rc[i];
+      llg_set_error("instance " + std::to_string(i) + ": " + errs[i]);
+    }
+  }
+  return first;
+}
+
+void llg_batch_destroy(llg_batch* b) {
+  if (!b) return;
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    if (b->streams[i]) cudaStreamSynchronize(b->streams[i]);
+    llg_destroy(b->ctx[i]);
+    if (b->streams[i]) cudaStreamDestroy(b->streams[i]);
+  }
+  delete b;
+}
+
+}  // extern "C"

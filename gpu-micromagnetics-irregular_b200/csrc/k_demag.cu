@@ -31,6 +31,9 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "dev_fft.cuh"
@@ -351,7 +354,7 @@ __global__ void k_tensor_finish(const double2* __restrict__ Sxx, const double2* 
 }  // namespace
 
 // ── host side ───────────────────────────────────────────────────────────
-static constexpr int kRowsNB = 1;  // packed transforms per row-CTA (2 real rows)
+static constexpr int kRowsNB = 1;  // packed transforms per row-CTA at init (tensor spectra)
 
 struct HostFft {
   int n = 0, tx = 32, ept = 8;
@@ -359,6 +362,14 @@ struct HostFft {
   double2* d_tw = nullptr;
   float2* d_twf = nullptr;   // FP32 twiddles (mixed chain)
   int4* d_pass = nullptr;
+  // threads per transform for EPT elements per thread: n/EPT covers the
+  // fixed radices; a generic radix R needs one thread per butterfly (n/R)
+  int tx_for(int e) const {
+    int need = (n + e - 1) / e;
+    for (int r : radix)
+      if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) need = std::max(need, n / r);
+    return ((std::max(need, 32) + 31) / 32) * 32;
+  }
   template <typename R>
   FftPlanT<R> dev() const {
     FftPlanT<R> p{};
@@ -370,6 +381,14 @@ struct HostFft {
     else p.tw = d_twf;
     return p;
   }
+};
+
+// Launch shape of one transform kernel, picked per plan by timing (autotune):
+// nb packed transforms per CTA (rows), ept elements per thread, stage =
+// tensor column prefetched into shared memory (columns).
+struct LaunchCfg {
+  int nb = 1, ept = 8;
+  bool stage = false;
 };
 
 struct DemagPlan {
@@ -384,8 +403,6 @@ struct DemagPlan {
   double* d_tzz = nullptr;
   double2* d_txy = nullptr;
   double* d_T = nullptr;         // 9 real tensor components (kept for host queries)
-  size_t smem_rows = 0, smem_cols = 0, smem_cols_staged = 0;
-  bool stage_tensor = false;     // tensor column prefetched into shared memory
   // mixed-precision chain (LLG_DEMAG_MIXED): FP32 spectrum and tensor spectra
   int mixed = 0;
   float2* d_Sf = nullptr;
@@ -393,9 +410,10 @@ struct DemagPlan {
   float* d_tyyf = nullptr;
   float* d_tzzf = nullptr;
   float2* d_txyf = nullptr;
-  size_t smem_rows_f = 0, smem_cols_f = 0, smem_cols_staged_f = 0;
-  bool stage_tensor_f = false;
+  LaunchCfg rows[2], cols[2];    // [0] FP64 chain, [1] FP32 chain (autotuned)
   DemagTc* tc = nullptr;         // tensor-core column stage (k_demag_tc.cu), when the shape allows
+  cudaGraphExec_t gexec = nullptr;   // captured chain for gkey = (y, w, h) on the context's own stream
+  const void* gkey[3] = {nullptr, nullptr, nullptr};
 };
 
 static int factorize(int n, std::vector<int>& rad) {
@@ -482,6 +500,7 @@ void demag_destroy(DemagPlan* d) {
   cudaFree(d->d_tzzf);
   cudaFree(d->d_txyf);
   demag_tc_destroy(d->tc);
+  if (d->gexec) cudaGraphExecDestroy(d->gexec);
   delete d;
 }
 
@@ -494,45 +513,48 @@ static int set_smem(const void* fn, size_t bytes) {
 
 // ── launch helpers (elements-per-thread dispatch) ─────────────────────────
 template <typename R>
+static constexpr int kp() { return sizeof(R) == 8 ? 0 : 1; }
+
+template <typename R>
 static int launch_rows_fwd(const DemagPlan* d, cudaStream_t s, const double* in, long long cs, int row_len,
-                           int nrows, const double* w, cx_t<R>* S, int ld, int ncomp) {
+                           int nrows, const double* w, cx_t<R>* S, int ld, int ncomp, const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fx.dev<R>();
-  const size_t sm = (sizeof(R) == 8) ? d->smem_rows : d->smem_rows_f;
-  const dim3 g((nrows + 2 * kRowsNB - 1) / (2 * kRowsNB), ncomp), b(d->fx.tx, kRowsNB);
-  if (d->fx.ept == 8)
-    k_rows_fwd<R, kRowsNB, 8><<<g, b, sm, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
-  else
-    k_rows_fwd<R, kRowsNB, 16><<<g, b, sm, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx);
+  const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * d->px;
+  const dim3 g((nrows + 2 * k.nb - 1) / (2 * k.nb), ncomp), b(d->fx.tx_for(k.ept), k.nb);
+#define ROWS_FWD(NB, E) k_rows_fwd<R, NB, E><<<g, b, sm, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx)
+  if (k.nb == 1) { if (k.ept == 8) ROWS_FWD(1, 8); else ROWS_FWD(1, 16); }
+  else { if (k.ept == 8) ROWS_FWD(2, 8); else ROWS_FWD(2, 16); }
+#undef ROWS_FWD
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
 template <typename R>
-static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, const cx_t<R>* S, double* h, long long cs) {
+static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, const cx_t<R>* S, double* h, long long cs,
+                           const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fx.dev<R>();
-  const size_t sm = (sizeof(R) == 8) ? d->smem_rows : d->smem_rows_f;
-  const dim3 g((d->ny + 2 * kRowsNB - 1) / (2 * kRowsNB), 3), b(d->fx.tx, kRowsNB);
-  if (d->fx.ept == 8)
-    k_rows_inv<R, kRowsNB, 8><<<g, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, h, cs, d->ng);
-  else
-    k_rows_inv<R, kRowsNB, 16><<<g, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, h, cs, d->ng);
+  const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * d->px;
+  const dim3 g((d->ny + 2 * k.nb - 1) / (2 * k.nb), 3), b(d->fx.tx_for(k.ept), k.nb);
+#define ROWS_INV(NB, E) k_rows_inv<R, NB, E><<<g, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, h, cs, d->ng)
+  if (k.nb == 1) { if (k.ept == 8) ROWS_INV(1, 8); else ROWS_INV(1, 16); }
+  else { if (k.ept == 8) ROWS_INV(2, 8); else ROWS_INV(2, 16); }
+#undef ROWS_INV
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
 template <typename R>
 static int launch_cols_conv(const DemagPlan* d, cudaStream_t s, cx_t<R>* S, const R* txx, const R* tyy,
-                            const R* tzz, const cx_t<R>* txy) {
+                            const R* tzz, const cx_t<R>* txy, const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fy.dev<R>();
-  const dim3 b(d->fy.tx, 3);
-  const bool stage = (sizeof(R) == 8) ? d->stage_tensor : d->stage_tensor_f;
-  const size_t sm = (sizeof(R) == 8) ? (stage ? d->smem_cols_staged : d->smem_cols)
-                                     : (stage ? d->smem_cols_staged_f : d->smem_cols_f);
+  const dim3 b(d->fy.tx_for(k.ept), 3);
+  const size_t base = sizeof(cx_t<R>) * 3 * (size_t)d->py;
+  const size_t sm = k.stage ? base + (sizeof(R) * 3 + sizeof(cx_t<R>)) * (size_t)d->py : base;
 #define COLS_LAUNCH(E, ST) k_cols_conv<R, E, ST><<<d->hx, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy)
-  if (d->fy.ept == 8) {
-    if (stage) COLS_LAUNCH(8, true); else COLS_LAUNCH(8, false);
+  if (k.ept == 8) {
+    if (k.stage) COLS_LAUNCH(8, true); else COLS_LAUNCH(8, false);
   } else {
-    if (stage) COLS_LAUNCH(16, true); else COLS_LAUNCH(16, false);
+    if (k.stage) COLS_LAUNCH(16, true); else COLS_LAUNCH(16, false);
   }
 #undef COLS_LAUNCH
   LLG_CUDA_TRY(cudaPeekAtLastError());
@@ -551,18 +573,130 @@ static int launch_cols_fwd(const DemagPlan* d, cudaStream_t s, double2* S) {
 }
 
 template <typename R>
-static int set_smem_all(const DemagPlan* d, size_t rows, size_t cols, size_t cols_staged, bool stage) {
+static bool rows_ok(const DemagPlan* d, int nb, int ept) {
+  return d->fx.tx_for(ept) * nb <= 1024 && sizeof(cx_t<R>) * (size_t)nb * d->px <= 227 * 1024;
+}
+template <typename R>
+static size_t cols_smem(const DemagPlan* d, bool stage) {
+  const size_t base = sizeof(cx_t<R>) * 3 * (size_t)d->py;
+  return stage ? base + (sizeof(R) * 3 + sizeof(cx_t<R>)) * (size_t)d->py : base;
+}
+template <typename R>
+static bool cols_ok(const DemagPlan* d, int ept, bool stage) {
+  if (d->fy.tx_for(ept) * 3 > 1024) return false;
+  if (!stage) return cols_smem<R>(d, false) <= 227 * 1024;
+  return d->py % (int)(16 / sizeof(R)) == 0 && cols_smem<R>(d, true) <= 200 * 1024;
+}
+
+// opt in to the dynamic shared memory of every launch shape that fits
+template <typename R>
+static int set_smem_all(DemagPlan* d) {
   int rc;
-  if ((rc = set_smem((const void*)k_rows_fwd<R, kRowsNB, 8>, rows)) ||
-      (rc = set_smem((const void*)k_rows_fwd<R, kRowsNB, 16>, rows)) ||
-      (rc = set_smem((const void*)k_rows_inv<R, kRowsNB, 8>, rows)) ||
-      (rc = set_smem((const void*)k_rows_inv<R, kRowsNB, 16>, rows)) ||
-      (rc = set_smem((const void*)k_cols_conv<R, 8, false>, cols)) ||
-      (rc = set_smem((const void*)k_cols_conv<R, 16, false>, cols)) ||
-      (stage && (rc = set_smem((const void*)k_cols_conv<R, 8, true>, cols_staged))) ||
-      (stage && (rc = set_smem((const void*)k_cols_conv<R, 16, true>, cols_staged))))
+  const size_t r1 = sizeof(cx_t<R>) * (size_t)d->px, r2 = 2 * r1;
+  if ((rc = set_smem((const void*)k_rows_fwd<R, 1, 8>, r1)) || (rc = set_smem((const void*)k_rows_fwd<R, 1, 16>, r1)) ||
+      (rc = set_smem((const void*)k_rows_inv<R, 1, 8>, r1)) || (rc = set_smem((const void*)k_rows_inv<R, 1, 16>, r1)))
     return rc;
-  (void)d;
+  if (r2 <= 227 * 1024 &&
+      ((rc = set_smem((const void*)k_rows_fwd<R, 2, 8>, r2)) || (rc = set_smem((const void*)k_rows_fwd<R, 2, 16>, r2)) ||
+       (rc = set_smem((const void*)k_rows_inv<R, 2, 8>, r2)) || (rc = set_smem((const void*)k_rows_inv<R, 2, 16>, r2))))
+    return rc;
+  const size_t c0 = cols_smem<R>(d, false), c1 = cols_smem<R>(d, true);
+  if ((rc = set_smem((const void*)k_cols_conv<R, 8, false>, c0)) ||
+      (rc = set_smem((const void*)k_cols_conv<R, 16, false>, c0)))
+    return rc;
+  if (c1 <= 200 * 1024 && ((rc = set_smem((const void*)k_cols_conv<R, 8, true>, c1)) ||
+                           (rc = set_smem((const void*)k_cols_conv<R, 16, true>, c1))))
+    return rc;
+  // default shapes (before tuning): one transform per CTA, fewest elements per thread
+  LaunchCfg& rw = d->rows[kp<R>()];
+  LaunchCfg& cl = d->cols[kp<R>()];
+  rw.nb = 1;
+  rw.ept = rows_ok<R>(d, 1, 8) ? 8 : 16;
+  cl.ept = cols_ok<R>(d, 8, false) ? 8 : 16;
+  cl.stage = cols_ok<R>(d, cl.ept, true);
+  if (!rows_ok<R>(d, rw.nb, rw.ept) || !cols_ok<R>(d, cl.ept, false)) {
+    llg_set_error("demag grid too large for the shared-memory transform");
+    return LLG_ERR_NOTSUP;
+  }
+  return 0;
+}
+
+// ── autotuner: time every valid launch shape of the row pair (forward +
+// inverse) and of the column kernel on this plan's buffers, keep the fastest.
+// All shapes compute bitwise-identical results (same butterflies, same
+// operation order per element), so tuning never changes numerics.  Results
+// are cached per (precision, transform size, grid) for later plans.
+struct TuneKey {
+  int prec, px, py, ny, ng;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(prec, px, py, ny, ng) < std::tie(o.prec, o.px, o.py, o.ny, o.ng);
+  }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, std::pair<LaunchCfg, LaunchCfg>> g_tune;
+
+template <typename R>
+static int demag_autotune(llg_ctx* c, DemagPlan* d, cx_t<R>* S, const R* txx, const R* tyy, const R* tzz,
+                          const cx_t<R>* txy, bool tune_cols) {
+  const TuneKey key{kp<R>(), d->px, d->py, d->ny, d->ng};
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      d->rows[kp<R>()] = it->second.first;
+      if (tune_cols) d->cols[kp<R>()] = it->second.second;
+      return 0;
+    }
+  }
+  cudaStream_t s = c->stream;
+  const long long cs = (long long)c->ncell;
+  cudaEvent_t e0, e1;
+  LLG_CUDA_TRY(cudaEventCreate(&e0));
+  LLG_CUDA_TRY(cudaEventCreate(&e1));
+  auto timed = [&](auto&& launch) -> float {
+    if (launch()) return 1e30f;
+    cudaEventRecord(e0, s);
+    for (int k = 0; k < 3; k++)
+      if (launch()) return 1e30f;
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  LaunchCfg best_r = d->rows[kp<R>()], best_c = d->cols[kp<R>()];
+  float tbest = 1e30f;
+  for (int nb = 1; nb <= 2; nb++)
+    for (int ept = 8; ept <= 16; ept *= 2) {
+      if (!rows_ok<R>(d, nb, ept)) continue;
+      LaunchCfg k;
+      k.nb = nb;
+      k.ept = ept;
+      const float t = timed([&]() {
+        int rc = launch_rows_fwd<R>(d, s, c->d_hd, cs, d->ng, d->ny, nullptr, S, d->ny, 3, k);
+        return rc ? rc : launch_rows_inv<R>(d, s, S, c->d_pm, cs, k);
+      });
+      if (t < tbest) { tbest = t; best_r = k; }
+    }
+  if (tune_cols) {
+    tbest = 1e30f;
+    for (int ept = 8; ept <= 16; ept *= 2)
+      for (int st = 0; st <= 1; st++) {
+        if (!cols_ok<R>(d, ept, st != 0)) continue;
+        LaunchCfg k;
+        k.ept = ept;
+        k.stage = st != 0;
+        const float t = timed([&]() { return launch_cols_conv<R>(d, s, S, txx, tyy, tzz, txy, k); });
+        if (t < tbest) { tbest = t; best_c = k; }
+      }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  LLG_CUDA_TRY(cudaGetLastError());
+  d->rows[kp<R>()] = best_r;
+  if (tune_cols) d->cols[kp<R>()] = best_c;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune[key] = {best_r, tune_cols ? best_c : d->cols[kp<R>()]};
   return 0;
 }
 
@@ -592,24 +726,13 @@ int demag_create(llg_ctx* c) {
   int rc = fft_init(d->fx, d->px, kRowsNB);
   if (!rc) rc = fft_init(d->fy, d->py, 3);
   if (rc) { demag_destroy(d); return rc; }
-  d->smem_rows = sizeof(double2) * (size_t)kRowsNB * d->px;
-  d->smem_cols = sizeof(double2) * 3 * (size_t)d->py;
-  d->smem_cols_staged = d->smem_cols + (size_t)40 * d->py;
-  d->stage_tensor = (d->py % 2 == 0) && d->smem_cols_staged <= 200 * 1024;
-  if (d->smem_rows > 227 * 1024 || d->smem_cols > 227 * 1024 || d->fx.tx * kRowsNB > 1024 ||
-      d->fy.tx * 3 > 1024) {
+  d->mixed = (p.demag_precision == LLG_DEMAG_MIXED);
+  if (d->fx.tx * kRowsNB > 1024 || sizeof(double2) * (size_t)d->py > 227 * 1024) {
     llg_set_error("demag grid too large for the shared-memory transform");
     demag_destroy(d);
     return LLG_ERR_NOTSUP;
   }
-  d->mixed = (p.demag_precision == LLG_DEMAG_MIXED);
-  d->smem_rows_f = sizeof(float2) * (size_t)kRowsNB * d->px;
-  d->smem_cols_f = sizeof(float2) * 3 * (size_t)d->py;
-  d->smem_cols_staged_f = d->smem_cols_f + (size_t)20 * d->py;
-  d->stage_tensor_f = (d->py % 4 == 0) && d->smem_cols_staged_f <= 200 * 1024;
-  if ((rc = set_smem_all<double>(d, d->smem_rows, d->smem_cols, d->smem_cols_staged, d->stage_tensor)) ||
-      (d->mixed &&
-       (rc = set_smem_all<float>(d, d->smem_rows_f, d->smem_cols_f, d->smem_cols_staged_f, d->stage_tensor_f))) ||
+  if ((rc = set_smem_all<double>(d)) || (d->mixed && (rc = set_smem_all<float>(d))) ||
       (rc = set_smem((const void*)k_cols_fwd<8>, sizeof(double2) * (size_t)d->py)) ||
       (rc = set_smem((const void*)k_cols_fwd<16>, sizeof(double2) * (size_t)d->py))) {
     demag_destroy(d);
@@ -640,8 +763,11 @@ int demag_create(llg_ctx* c) {
   double2* spec = nullptr;
   LLG_CUDA_TRY(cudaMalloc(&spec, sizeof(double2) * 9 * (size_t)nspec));
   for (int k = 0; k < 9; k++) {
-    if ((rc = launch_rows_fwd<double>(d, s, d->d_T + k * np, 0, d->px, d->py, nullptr, spec + k * nspec, d->py,
-                                      1)) ||
+    LaunchCfg k1;
+    k1.nb = kRowsNB;
+    k1.ept = d->fx.ept;
+    if ((rc = launch_rows_fwd<double>(d, s, d->d_T + k * np, 0, d->px, d->py, nullptr, spec + k * nspec, d->py, 1,
+                                      k1)) ||
         (rc = launch_cols_fwd(d, s, spec + k * nspec))) {
       cudaFree(spec);
       demag_destroy(d);
@@ -689,6 +815,13 @@ int demag_create(llg_ctx* c) {
       c->demag = d;
       return rc;
     }
+    if ((rc = demag_autotune<float>(c, d, d->d_Sf, d->d_txxf, d->d_tyyf, d->d_tzzf, d->d_txyf, d->tc == nullptr))) {
+      c->demag = d;
+      return rc;
+    }
+  } else if ((rc = demag_autotune<double>(c, d, d->d_S, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy, true))) {
+    c->demag = d;
+    return rc;
   }
   c->demag = d;
   return 0;
@@ -699,20 +832,20 @@ static int demag_run_stage(llg_ctx* c, DemagPlan* d, int stage, const double* y,
   const long long cs = (long long)c->ncell;
   if (stage == 0) {
     LLG_COUNT(KID_DEMAG_ROWS_FWD);
-    if (d->mixed) return launch_rows_fwd<float>(d, c->stream, y, cs, d->ng, d->ny, w, d->d_Sf, d->ny, 3);
-    return launch_rows_fwd<double>(d, c->stream, y, cs, d->ng, d->ny, w, d->d_S, d->ny, 3);
+    if (d->mixed) return launch_rows_fwd<float>(d, c->stream, y, cs, d->ng, d->ny, w, d->d_Sf, d->ny, 3, d->rows[1]);
+    return launch_rows_fwd<double>(d, c->stream, y, cs, d->ng, d->ny, w, d->d_S, d->ny, 3, d->rows[0]);
   }
   if (stage == 1) {
     LLG_COUNT(KID_DEMAG_COLS);
     if (d->mixed) {
       if (d->tc) return demag_tc_cols(c, d->tc, d->d_Sf);
-      return launch_cols_conv<float>(d, c->stream, d->d_Sf, d->d_txxf, d->d_tyyf, d->d_tzzf, d->d_txyf);
+      return launch_cols_conv<float>(d, c->stream, d->d_Sf, d->d_txxf, d->d_tyyf, d->d_tzzf, d->d_txyf, d->cols[1]);
     }
-    return launch_cols_conv<double>(d, c->stream, d->d_S, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy);
+    return launch_cols_conv<double>(d, c->stream, d->d_S, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy, d->cols[0]);
   }
   LLG_COUNT(KID_DEMAG_ROWS_INV);
-  if (d->mixed) return launch_rows_inv<float>(d, c->stream, d->d_Sf, h, cs);
-  return launch_rows_inv<double>(d, c->stream, d->d_S, h, cs);
+  if (d->mixed) return launch_rows_inv<float>(d, c->stream, d->d_Sf, h, cs, d->rows[1]);
+  return launch_rows_inv<double>(d, c->stream, d->d_S, h, cs, d->rows[0]);
 }
 
 int demag_apply(llg_ctx* c, const double* y, double* h) {
@@ -726,8 +859,37 @@ int demag_apply_w(llg_ctx* c, const double* y, const double* w, double* h) {
     return 0;
   }
   int rc;
-  for (int stage = 0; stage < 3; stage++)
-    if ((rc = demag_run_stage(c, d, stage, y, w, h))) return rc;
+  if (c->stream == nullptr) {   // legacy default stream: no capture
+    for (int stage = 0; stage < 3; stage++)
+      if ((rc = demag_run_stage(c, d, stage, y, w, h))) return rc;
+    return 0;
+  }
+  // On a context's own stream the three-kernel chain runs as one CUDA graph,
+  // captured on first use for these (y, w, h) buffers and replayed after.
+  if (!(d->gexec && d->gkey[0] == y && d->gkey[1] == w && d->gkey[2] == h)) {
+    if (d->gexec) { cudaGraphExecDestroy(d->gexec); d->gexec = nullptr; }
+    cudaGraph_t graph = nullptr;
+    LLG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    rc = 0;
+    for (int stage = 0; stage < 3 && rc == 0; stage++) rc = demag_run_stage(c, d, stage, y, w, h);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    // the capture launched nothing; the replay below is counted instead
+    g_kcount[KID_DEMAG_ROWS_FWD].fetch_sub(1);
+    g_kcount[KID_DEMAG_COLS].fetch_sub(1);
+    g_kcount[KID_DEMAG_ROWS_INV].fetch_sub(1);
+    if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+    LLG_CUDA_TRY(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&d->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    LLG_CUDA_TRY(ie);
+    d->gkey[0] = y;
+    d->gkey[1] = w;
+    d->gkey[2] = h;
+  }
+  LLG_COUNT(KID_DEMAG_ROWS_FWD);
+  LLG_COUNT(KID_DEMAG_COLS);
+  LLG_COUNT(KID_DEMAG_ROWS_INV);
+  LLG_CUDA_TRY(cudaGraphLaunch(d->gexec, c->stream));
   return 0;
 }
 

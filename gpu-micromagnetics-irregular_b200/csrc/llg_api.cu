@@ -16,7 +16,7 @@
 
 static thread_local std::string g_last_error;
 void llg_set_error(const std::string& msg) { g_last_error = msg; }
-long long g_kcount[KID_COUNT] = {0};
+std::atomic<long long> g_kcount[KID_COUNT];
 int integrator_time_kernel(llg_ctx* c, int kid, int iters, double* avg_ms);
 
 int integrator_create(llg_ctx* c, double t0, const double* y0, const llg_solver_opts* o);
@@ -350,12 +350,12 @@ int llg_get_stats(llg_ctx* c, llg_stats* st) {
 int llg_kernel_counts(int64_t* out, int n) {
   if (!out || n <= 0) return LLG_ERR_ARG;
   const int m = n < KID_COUNT ? n : KID_COUNT;
-  for (int k = 0; k < m; k++) out[k] = g_kcount[k];
+  for (int k = 0; k < m; k++) out[k] = g_kcount[k].load();
   return KID_COUNT;
 }
 
 void llg_reset_kernel_counts(void) {
-  for (int k = 0; k < KID_COUNT; k++) g_kcount[k] = 0;
+  for (int k = 0; k < KID_COUNT; k++) g_kcount[k].store(0);
 }
 
 int llg_time_kernel(llg_ctx* c, int kernel_id, int iters, double* avg_ms) {

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -42,8 +43,8 @@ enum LlgKernel {
   KID_DEMAG_ROWS_FWD, KID_DEMAG_COLS, KID_DEMAG_ROWS_INV, KID_REDUCE, KID_ELEMWISE,
   KID_LEARNED, KID_OTHER, KID_COUNT
 };
-extern long long g_kcount[KID_COUNT];
-#define LLG_COUNT(k) (g_kcount[(k)]++)
+extern std::atomic<long long> g_kcount[KID_COUNT];
+#define LLG_COUNT(k) (g_kcount[(k)].fetch_add(1, std::memory_order_relaxed))
 
 // Physics + geometry view passed by value to every per-cell kernel.
 struct DevProblem {

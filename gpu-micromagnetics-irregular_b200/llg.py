@@ -204,6 +204,12 @@ def load(path: str | None = None):
         "llg_build_geometry": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
         "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
         "llg_selftest_tcgen05": (I, [I, P(D)]),
+        "llg_batch_create": (I, [C.c_int32, P(Params), P(VP)]),
+        "llg_batch_size": (I, [VP]),
+        "llg_batch_ctx": (VP, [VP, C.c_int32]),
+        "llg_batch_integrator_init": (I, [VP, D, P(VP), P(SolverOpts)]),
+        "llg_batch_integrate": (I, [VP, D, P(VP), C.c_int32, P(C.c_int32)]),
+        "llg_batch_destroy": (None, [VP]),
         "llg_learned_harvest": (I, [VP, C.c_int32, C.c_int32]),
         "llg_learned_num_samples": (I, [VP]),
         "llg_learned_train": (I, [VP, P(TrainOpts), P(D), P(D)]),
@@ -258,7 +264,17 @@ class Context:
         if stream is not None:
             _check(self.lib.llg_set_stream(self.h, _ptr(stream) if not hasattr(stream, "cuda_stream") else stream.cuda_stream), "llg_set_stream")
 
+    @classmethod
+    def _borrowed(cls, lib, handle, params):
+        """Non-owning view of a context that a Batch owns."""
+        c = cls.__new__(cls)
+        c.lib, c.params, c.h, c.ncell, c._borrowed_ref = lib, params, C.c_void_p(handle), params.ng * params.ny, True
+        return c
+
     def close(self):
+        if getattr(self, "_borrowed_ref", False):
+            self.h = None
+            return
         if getattr(self, "h", None):
             self.lib.llg_destroy(self.h)
             self.h = None
@@ -401,6 +417,115 @@ class Context:
         _check(self.lib.llg_learned_policy(self.h, C.byref(il), C.byref(ib), C.byref(k)), "llg_learned_policy")
         return {"active": a.value, "fell_back": f.value, "napply": n.value, "it_learned": il.value,
                 "it_block_jacobi": ib.value, "kappa": k.value}
+
+
+class Batch:
+    """Independent instances integrated concurrently (one stream each)."""
+
+    def __init__(self, params_list):
+        self.lib = load()
+        n = len(params_list)
+        arr = (Params * n)(*params_list)
+        h = C.c_void_p()
+        _check(self.lib.llg_batch_create(n, arr, C.byref(h)), "llg_batch_create")
+        self.h = h
+        self.params = list(params_list)
+        self.ctx = [Context._borrowed(self.lib, self.lib.llg_batch_ctx(self.h, i), params_list[i]) for i in range(n)]
+
+    def __len__(self):
+        return len(self.ctx)
+
+    def integrator_init(self, t0, ys, opts):
+        ptrs = (C.c_void_p * len(ys))(*[_ptr(y) for y in ys])
+        _check(self.lib.llg_batch_integrator_init(self.h, float(t0), ptrs, C.byref(opts)), "llg_batch_integrator_init")
+
+    def integrate(self, tout, youts, nthreads=0):
+        ptrs = (C.c_void_p * len(youts))(*[_ptr(y) for y in youts])
+        rcs = (C.c_int32 * len(youts))()
+        _check(self.lib.llg_batch_integrate(self.h, float(tout), ptrs, int(nthreads), rcs), "llg_batch_integrate")
+        return list(rcs)
+
+    def stats(self):
+        return [c.stats() for c in self.ctx]
+
+    def close(self):
+        for c in getattr(self, "ctx", []):
+            c.close()
+        if getattr(self, "h", None):
+            self.lib.llg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _splitmix64(state):
+    state = (state + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return state, z ^ (z >> 31)
+
+
+CONFIG4_SIZES = ((256, 256), (512, 256), (512, 512), (1024, 512))
+CONFIG4_SHAPES = ("square_hole", "annulus", "ellipse", "polycrystal")
+
+
+def config4_instances(n=64, master_seed=12345, demag_precision=DEMAG_MIXED, precond_kind=PREC_BLOCK_JACOBI,
+                      sizes=CONFIG4_SIZES):
+    """The batched mixed workload: n instances with seeded sizes from
+    256x256 .. 1024x512, shapes from {square hole, annulus r 0.15..0.35 N,
+    ellipse rx 0.3 NX ry 0.2 NY (compact index lists), polycrystal 24 grains
+    10 % dead (windowed)}, open demag of strength U[1, 4], jittered uniform or
+    two-domain initial states.  Seeds: master seed -> splitmix64 -> one 64-bit
+    draw per instance (size, shape, strength, IC and srand seed from its bits).
+    Returns a list of dicts with params, geom and a name."""
+    out = []
+    state = master_seed & 0xFFFFFFFFFFFFFFFF
+    for i in range(n):
+        state, z = _splitmix64(state)
+        ng, ny = sizes[z & 3]
+        shape = CONFIG4_SHAPES[(z >> 2) & 3]
+        strength = 1.0 + 3.0 * (((z >> 8) & 0xFFFF) / 65535.0)
+        two_domain = bool((z >> 24) & 1)
+        seed = int((z >> 32) & 0x7FFFFFFF) or 1
+        pkw = dict(demag_mode=DEMAG_OPEN, demag_strength=strength, norm_kind=NORM_REG,
+                   demag_precision=demag_precision, precond_kind=precond_kind)
+        gkw = dict(ic_kind=IC_TWO_DOMAIN_X if two_domain else IC_UNIFORM, ic_jitter_eps=0.01,
+                   init_random_seed=seed)
+        if shape == "square_hole":
+            gkw.update(geometry_kind=GEOM_HOLE_SQUARE, hole_radius_frac_y=0.125)
+        elif shape == "annulus":
+            gkw.update(geometry_kind=GEOM_ANNULUS, annulus_r_in_frac=0.15, annulus_r_out_frac=0.35)
+        elif shape == "ellipse":
+            gkw.update(geometry_kind=GEOM_ELLIPSE, active_rx_frac=0.3, active_ry_frac=0.2)
+            pkw.update(exec_model=EXEC_COMPACT)
+        else:
+            gkw.update(geometry_kind=GEOM_POLYCRYSTAL, num_grains=24, dead_grain_frac=0.10, grain_z_bias=1.0,
+                       hole_seed=seed)
+            pkw.update(windowed=1)
+        out.append(dict(name=f"{i:02d}-{shape}-{ng}x{ny}", params=default_params(ng, ny, **pkw),
+                        geom=default_geom(ng, ny, **gkw), shape=shape))
+    return out
+
+
+def setup_instance(ctx, inst):
+    """Geometry of one config4_instances() entry into a context; returns y0 (host)."""
+    geo = build_geometry(inst["geom"])
+    p = inst["params"]
+    n = p.ng * p.ny
+    if p.windowed:
+        ctx.set_window(geo["w"], geo["msk3"], geo["nsk3"])
+    elif p.exec_model == EXEC_COMPACT:
+        ids = np.arange(n, dtype=np.int32)
+        act = geo["active"]
+        ctx.set_active_ids(ids[act == 1], ids[act == 0])
+    else:
+        ctx.set_mask(np.tile(geo["active"].astype(np.float64), 3))
+    return geo["y0"]
 
 
 def learned_loss_grad(w, u, m, mask, ewt, x, gamma, want_z=True):

@@ -272,6 +272,21 @@ int  llg_learned_loss_grad(const float* h_w, int32_t nb, int32_t P, const float*
                            const float* h_mask, const float* h_ewt, const float* h_x, const float* h_gamma,
                            double* loss, float* h_grad, float* h_z);
 
+/* ── batches of independent instances (no counterpart in the reference) ─ *
+ * One context per instance, each on its own CUDA stream; llg_batch_integrate
+ * advances every instance to tout concurrently from `nthreads` host threads
+ * (<= 0: one per instance), largest instances first.  Instances are set up
+ * through llg_batch_ctx (set_mask / set_active_ids / set_window / learned
+ * weights) before llg_batch_integrator_init.  rcs[i] receives each
+ * instance's llg_integrate code (may be NULL).                            */
+typedef struct llg_batch llg_batch;
+int      llg_batch_create(int32_t n, const llg_params* params, llg_batch** out);
+int      llg_batch_size(const llg_batch* b);
+llg_ctx* llg_batch_ctx(llg_batch* b, int32_t i);
+int      llg_batch_integrator_init(llg_batch* b, double t0, const double* const* d_y0, const llg_solver_opts* o);
+int      llg_batch_integrate(llg_batch* b, double tout, double* const* d_yout, int32_t nthreads, int32_t* rcs);
+void     llg_batch_destroy(llg_batch* b);
+
 /* ── instrumentation ──────────────────────────────────────────────────── */
 /* Kernel families, in this order: RHS, JTV, ARNOLDI (fused Krylov operator),
  * PSETUP, PSOLVE, NORM, DEMAG_ROWS_FWD, DEMAG_COLS, DEMAG_ROWS_INV, REDUCE,
