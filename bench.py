@@ -304,6 +304,43 @@ def roofline_for(lib, run, ng, ny, mixed):
             "kernel_share": {KERNEL_NAMES[k]: v / max(sum(share.values()), 1e-30) for k, v in share.items()}}
 
 
+def short_run(form, rank, t_out, strength_scale=1.0):
+    """Integrate a fresh instance of `form` from t=0 and return y at each t in t_out."""
+    import torch
+    p, g, o = form_params(form, 12345 + rank)
+    p.demag_strength *= strength_scale
+    ctx, geo = make_ctx(p, g)
+    if FORMS[form]["learned"]:
+        ctx.learned_set_weights(train_weights(rank)[0])
+    y0 = torch.from_numpy(geo["y0"]).cuda()
+    ctx.integrator_init(0.0, y0, o)
+    yout = torch.zeros_like(y0)
+    outs = {}
+    for k in range(1, int(round(max(t_out) / 0.1)) + 1):
+        ctx.integrate(0.1 * k, yout)
+        if any(abs(0.1 * k - t) < 1e-9 for t in t_out):
+            outs[round(0.1 * k, 6)] = yout.cpu().numpy().copy()
+    ctx.close()
+    return outs
+
+
+def accuracy_check(form, rank, t_out=(0.5, 1.0, 2.0, 4.0)):
+    """max|dm| of `form` against plain FP64 on the bench workload, from the same
+    initial state, at early times.  Beside it a control: plain FP64 with the
+    demag strength perturbed by 1e-9 relative.  The jittered uniform state
+    under demag at alpha 0.02 is physically unstable, so any perturbation
+    (rounding included) grows exponentially; the control shows that growth."""
+    a = short_run("plain", rank, t_out)
+    b = short_run(form, rank, t_out)
+    c = short_run("plain", rank, t_out, strength_scale=1.0 + 1e-9)
+    return {"t": list(t_out),
+            "max_dm_form_vs_plain_fp64": [float(np.abs(b[round(t, 6)] - a[round(t, 6)]).max()) for t in t_out],
+            "max_dm_control_fp64_strength_1e-9": [float(np.abs(c[round(t, 6)] - a[round(t, 6)]).max())
+                                                  for t in t_out],
+            "note": "plain FP64 vs plain FP64 with demag strength x(1+1e-9): the control measures the "
+                    "workload's own amplification of perturbations"}
+
+
 def e2e_run(args, form, world, rank):
     """Same metric through the public API from host buffers: pinned y0 and
     mask uploaded inside the timed region, one y(t) frame read back per step."""
@@ -374,6 +411,7 @@ def run_ours(args, world, rank, local):
             mixed["ctx"].close()
             compare["mixed_only_value"] = mixed["value"]
             compare["mixed_only_gmres_iters_per_newton"] = mixed["counters"]["nli"] / max(mixed["counters"]["nni"], 1)
+        compare["accuracy_early_t"] = accuracy_check(form, rank)
     e2e = None if args.no_e2e else e2e_run(args, form, world, rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

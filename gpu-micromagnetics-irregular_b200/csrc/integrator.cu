@@ -27,25 +27,9 @@
 
 #include "llg_internal.h"
 
-namespace {
-constexpr int QMAXL = 5;
-constexpr int MAXLL = 16;
-constexpr double UROUND = DBL_EPSILON;
-constexpr double FUZZ_FACTOR = 100.0, HLB_FACTOR = 100.0, HUB_FACTOR = 0.1, H_BIAS = 0.5;
-constexpr int MAX_ITERS = 4;
-constexpr double CORTES = 0.1, THRESH = 1.5, ETAMX1 = 10000.0, ETAMX2 = 10.0, ETAMX3 = 10.0;
-constexpr double ETAMXF = 0.2, ETAMIN = 0.1, ETACF = 0.25, ADDON = 1.0e-6;
-constexpr double BIAS1 = 6.0, BIAS2 = 6.0, BIAS3 = 10.0, ONEPSM = 1.000001;
-constexpr int SMALL_NST = 10, MXNCF = 10, MXNEF = 7, MXNEF1 = 3, SMALL_NEF = 2, LONG_WAIT = 10;
-constexpr int NLS_MAXCOR = 3, MSBP = 20, LS_MSBJ = 51;
-constexpr double CRDOWN = 0.3, DGMAX = 0.3, RDIV = 2.0, LS_EPLIN = 0.05, LS_DGMAX = 0.2, GS_FACTOR = 1000.0;
-constexpr int FIRST_CALL = 0, PREV_CONV_FAIL = 1, PREV_ERR_FAIL = 2, DO_ERROR_TEST = 3, PREDICT_AGAIN = 4,
-              TRY_AGAIN = 5;
-constexpr int NLS_CONTINUE = 901, NLS_CONV_RECVR = 902;
-constexpr int CV_NO_FAILURES = 0, CV_FAIL_BAD_J = 1, CV_FAIL_OTHER = 2;
-constexpr int LS_SUCCESS = 0, LS_RES_REDUCED = 1, LS_CONV_FAIL = 2, LS_QRSOL_FAIL = 3;
-constexpr int SLOT_A = 0, SLOT_DOTS = 8;
+#include "cvode_consts.h"
 
+namespace {
 double powi(double b, int e) {
   double p = 1.0;
   for (int i = 1; i <= (e < 0 ? -e : e); i++) p *= b;
@@ -81,6 +65,60 @@ struct Integrator {
   static constexpr int PROBE_EVERY = 8, MIN_LEARNED = 24, MIN_PROBES = 4;
   long long pol_solves = 0, nsl = 0, nil = 0, nsb = 0, nib = 0;
   double kappa = -1.0;
+  // device-resident form (integrator_dev.cu): graph + device copy of this state
+  int device_resident = 0;
+  DevInteg* dev = nullptr;
+  bool dev_current = false;   // the device copy holds the latest state
+
+  void export_state(DState& s) const {
+    memset(&s, 0, sizeof(s));
+#define LLG_CP_OUT(f) s.f = f;
+    LLG_DS_DOUBLES(LLG_CP_OUT)
+    LLG_DS_INTS(LLG_CP_OUT)
+    LLG_DS_LLS(LLG_CP_OUT)
+#undef LLG_CP_OUT
+    memcpy(s.l, l, sizeof(s.l));
+    memcpy(s.tq, tq, sizeof(s.tq));
+    memcpy(s.tau, tau, sizeof(s.tau));
+    for (int j = 0; j <= QMAXL; j++) s.zn[j] = zn[j];
+    for (int j = 0; j <= MAXLL; j++) s.V[j] = V[j];
+    s.ewt = ewt; s.acor = acor; s.y = y; s.tempv = tempv; s.delta = delta;
+  }
+  void import_state(const DState& s) {
+#define LLG_CP_IN(f) f = s.f;
+    LLG_DS_DOUBLES(LLG_CP_IN)
+    LLG_DS_INTS(LLG_CP_IN)
+    LLG_DS_LLS(LLG_CP_IN)
+#undef LLG_CP_IN
+    memcpy(l, s.l, sizeof(s.l));
+    memcpy(tq, s.tq, sizeof(s.tq));
+    memcpy(tau, s.tau, sizeof(s.tau));
+  }
+  // the device form covers classical Gram-Schmidt with block-Jacobi; the
+  // learned preconditioner and training-pair harvesting stay on the host path
+  bool device_applies() {
+    return device_resident && started && classical_gs && maxl <= MAXLL - 1 && !learned_active(c) &&
+           !learned_harvest_wanted(c);
+  }
+  int integrate_device(double tout, double* yout, double* tret) {
+    if (!dev) {
+      const int rc = devint_create(c, &dev);
+      if (rc) return rc;
+    }
+    if (!dev_current) {
+      DState hs;
+      export_state(hs);
+      const int rc = devint_upload(dev, hs, c);
+      if (rc) return rc;
+      dev_current = true;
+    }
+    DState hs;
+    const int rc = devint_run(dev, c, tout, yout, hs);
+    if (rc) { dev_current = false; return rc; }
+    import_state(hs);
+    *tret = hs.tret;
+    return hs.status;
+  }
 
   // ── helpers ──
   bool ok(int rc) {
@@ -756,6 +794,8 @@ struct Integrator {
   }
 
   int integrate(double tout, double* yout, double* tret) {
+    if (device_applies()) return integrate_device(tout, yout, tret);
+    dev_current = false;   // the host path moves the state on
     const size_t vb = sizeof(double) * (size_t)neq;
     if (!started) {
       if (set_ewt(zn[0]) != 0) return LLG_CV_ILL_INPUT;
@@ -828,6 +868,9 @@ struct Integrator {
   }
 
   void free_all() {
+    devint_destroy(dev);
+    dev = nullptr;
+    dev_current = false;
     for (auto& p : zn) { cudaFree(p); p = nullptr; }
     for (auto& p : V) { cudaFree(p); p = nullptr; }
     double** vs[] = {&ewt, &acor, &y, &tempv, &delta};
@@ -846,6 +889,7 @@ int integrator_create(llg_ctx* c, double t0, const double* y0, const llg_solver_
   b->mxstep = (o->mxstep > 0) ? o->mxstep : 500;
   b->rtol = o->rtol;
   b->atol = o->atol;
+  b->device_resident = o->device_resident ? 1 : 0;
   const size_t vb = sizeof(double) * (size_t)b->neq;
   auto alloc = [&](double** p) -> int {
     LLG_CUDA_TRY(cudaMalloc(p, vb));
@@ -937,4 +981,21 @@ int integrator_stats(llg_ctx* c, llg_stats* st) {
   st->njvevals = b->njv; st->npsolves = b->nps; st->npe = b->npe;
   st->qlast = b->qu; st->qcur = b->next_q; st->hlast = b->hu; st->hcur = b->next_h; st->tcur = b->tn;
   return 0;
+}
+
+int devint_trace(DevInteg* d, llg_ctx* c, unsigned long long* dbuf, int cap);
+int devint_trace_count(DevInteg* d);
+
+int integrator_trace(llg_ctx* c, unsigned long long* buf, int cap) {
+  Integrator* b = c->integ;
+  if (!b || !b->dev || !b->dev_current) {
+    llg_set_error("trace_control needs a device-resident integrator that has run once");
+    return LLG_ERR_STATE;
+  }
+  return devint_trace(b->dev, c, buf, cap);
+}
+
+int integrator_trace_count(llg_ctx* c) {
+  Integrator* b = c->integ;
+  return (b && b->dev) ? devint_trace_count(b->dev) : 0;
 }

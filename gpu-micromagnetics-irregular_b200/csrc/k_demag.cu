@@ -859,7 +859,9 @@ int demag_apply_w(llg_ctx* c, const double* y, const double* w, double* h) {
     return 0;
   }
   int rc;
-  if (c->stream == nullptr) {   // legacy default stream: no capture
+  // legacy default stream, or inside the device-resident step graph's capture:
+  // launch the stages directly
+  if (c->stream == nullptr || c->capturing) {
     for (int stage = 0; stage < 3; stage++)
       if ((rc = demag_run_stage(c, d, stage, y, w, h))) return rc;
     return 0;

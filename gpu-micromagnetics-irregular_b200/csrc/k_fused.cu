@@ -24,6 +24,7 @@
 #include "dev_physics.cuh"
 #include "dev_reduce.cuh"
 #include "llg_internal.h"
+#include "dev_integ.h"
 
 namespace {
 
@@ -39,7 +40,8 @@ int cell_blocks(int ncell) { return red_blocks(ncell); }
 
 __global__ void __launch_bounds__(RT) k_ewt_wrms(double rtol, double atol, const double* __restrict__ y,
                                                  double* __restrict__ ewt, long long n, double* partials,
-                                                 unsigned int* counter, double* out) {
+                                                 unsigned int* counter, double* out, const DevArgs* da) {
+  if (da && !da->run_ewt) return;
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
@@ -60,7 +62,8 @@ __global__ void __launch_bounds__(RT) k_ewt_wrms(double rtol, double atol, const
 __device__ __forceinline__ double ycor_at(const double* ycor, int i) { return ycor ? ycor[i] : 0.0; }
 
 __global__ void k_lin_normalize(const double* __restrict__ zn0, const double* __restrict__ ycor,
-                                double* __restrict__ y, int n, int kind, double eps) {
+                                double* __restrict__ y, int n, int kind, double eps, const DevArgs* da) {
+  if (da && da->ycor_zero) ycor = nullptr;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const double m1 = 1.0 * zn0[k] + 1.0 * ycor_at(ycor, k);
     const double m2 = 1.0 * zn0[n + k] + 1.0 * ycor_at(ycor, n + k);
@@ -86,8 +89,14 @@ __global__ void __launch_bounds__(TX * TY) k_rhs_resid_tile(DevProblem P, const 
                                                             const double* __restrict__ hd,
                                                             const double* __restrict__ zn1,
                                                             const double* __restrict__ ycor, double rl1,
-                                                            double gamma, double* __restrict__ negres) {
+                                                            double gamma, double* __restrict__ negres,
+                                                            const DevArgs* da) {
   __shared__ Tile<1> T;
+  if (da) {
+    rl1 = da->rl1;
+    gamma = da->gamma;
+    if (da->ycor_zero) ycor = nullptr;
+  }
   const double* f[1] = {y};
   load_tile<1>(P, T, f);
   const int gi = blockIdx.x * TX + threadIdx.x, gj = blockIdx.y * TY + threadIdx.y;
@@ -115,8 +124,13 @@ __global__ void k_rhs_resid_compact(DevProblem P, const double* __restrict__ y, 
                                     const int32_t* __restrict__ act_ids, int na,
                                     const int32_t* __restrict__ inact_ids, int ni,
                                     const double* __restrict__ zn1, const double* __restrict__ ycor, double rl1,
-                                    double gamma, double* __restrict__ negres) {
+                                    double gamma, double* __restrict__ negres, const DevArgs* da) {
   const int n = P.ncell;
+  if (da) {
+    rl1 = da->rl1;
+    gamma = da->gamma;
+    if (da->ycor_zero) ycor = nullptr;
+  }
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na + ni; t += gridDim.x * blockDim.x) {
     double o[3] = {0.0, 0.0, 0.0};
     int cell;
@@ -149,10 +163,11 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
                                                          const double* __restrict__ r,
                                                          const double* __restrict__ ewt, double* __restrict__ v0,
                                                          double gamma, double* partials, unsigned int* counter,
-                                                         double* out) {
+                                                         double* out, const DevArgs* da) {
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
   const int n = P.ncell;
+  if (da) gamma = da->gamma_setup;
   for (int k = blockIdx.x * RT + threadIdx.x; k < n; k += gridDim.x * RT) {
     const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
     const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
@@ -204,9 +219,13 @@ __global__ void k_lincomb_div(int nv, CPack c, XPack X, const double* __restrict
 // ycor = 1*ycor + 1*del (ycor_in null: zero); sums (del*w)^2 and (ycor*w)^2
 __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, double* ycor, const double* __restrict__ del,
                                                      const double* __restrict__ w, long long n, double* partials,
-                                                     unsigned int* counter, double* out) {
+                                                     unsigned int* counter, double* out, const DevArgs* da) {
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
+  if (da) {
+    if (!da->run_update) return;
+    ycor_in = da->ycor_zero ? nullptr : ycor;
+  }
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
     const double d = del[i];
     const double yc = 1.0 * (ycor_in ? ycor_in[i] : 0.0) + 1.0 * d;
@@ -248,18 +267,18 @@ int ew_blocks(const llg_ctx* c, long long n) {
 
 }  // namespace
 
-int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot) {
+int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot, const DevArgs* da) {
   LLG_COUNT(KID_REDUCE);
   k_ewt_wrms<<<red_blocks(c->neq), RT, 0, c->stream>>>(rtol, atol, y, ewt, c->neq, c->d_red, c->d_counter,
-                                                       c->d_scal + slot);
+                                                       c->d_scal + slot, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
-int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor, double* y) {
+int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor, double* y, const DevArgs* da) {
   LLG_COUNT(KID_NORM);
   k_lin_normalize<<<ew_blocks(c, c->ncell), 256, 0, c->stream>>>(zn0, ycor, y, c->ncell, c->p.norm_kind,
-                                                                c->p.norm_eps);
+                                                                c->p.norm_eps, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -276,27 +295,27 @@ int fused_field(llg_ctx* c, const double* y) {
 }
 
 int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* ycor, double rl1, double gamma,
-                double* negres) {
+                double* negres, const DevArgs* da) {
   LLG_COUNT(KID_RHS);
   if (c->p.exec_model == LLG_EXEC_COMPACT) {
     const int tot = c->n_active + c->n_inactive;
     k_rhs_resid_compact<<<ew_blocks(c, tot), 256, 0, c->stream>>>(c->dp, y, c->d_hd, c->d_active_ids, c->n_active,
                                                                    c->d_inactive_ids, c->n_inactive, zn1, ycor, rl1,
-                                                                   gamma, negres);
+                                                                   gamma, negres, da);
   } else {
     dim3 g((c->p.ng + TX - 1) / TX, (c->p.ny + TY - 1) / TY);
-    k_rhs_resid_tile<<<g, dim3(TX, TY), 0, c->stream>>>(c->dp, y, c->d_hd, zn1, ycor, rl1, gamma, negres);
+    k_rhs_resid_tile<<<g, dim3(TX, TY), 0, c->stream>>>(c->dp, y, c->d_hd, zn1, ycor, rl1, gamma, negres, da);
   }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
-int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot) {
-  if (!c->have_setup) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
+int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot, const DevArgs* da) {
+  if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
   k_psolve_scale_dot<<<cell_blocks(c->ncell), RT, 0, c->stream>>>(c->dp, c->d_pm, c->d_ph, r, ewt, v0,
                                                                   c->gamma_setup, c->d_red, c->d_counter,
-                                                                  c->d_scal + slot);
+                                                                  c->d_scal + slot, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -324,10 +343,11 @@ int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* cons
   return 0;
 }
 
-int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot) {
+int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot,
+                       const DevArgs* da) {
   LLG_COUNT(KID_REDUCE);
   k_update_wrms2<<<red_blocks(c->neq), RT, 0, c->stream>>>(ycor_zero ? nullptr : ycor, ycor, del, w, c->neq, c->d_red, c->d_counter,
-                                                           c->d_scal + slot);
+                                                           c->d_scal + slot, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

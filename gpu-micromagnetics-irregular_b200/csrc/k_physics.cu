@@ -160,7 +160,8 @@ __global__ void k_jtv_compact(DevProblem P, const double* __restrict__ v, double
 // psetup: freeze (m, h_total) per cell
 __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const double* __restrict__ y,
                                                          const double* __restrict__ hd, double* __restrict__ pm,
-                                                         double* __restrict__ ph) {
+                                                         double* __restrict__ ph, const DevArgs* da) {
+  if (da && !da->run_setup) return;
   __shared__ Tile<1> T;
   const double* f[1] = {y};
   load_tile<1>(P, T, f);
@@ -181,8 +182,9 @@ __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const dou
 }
 
 __global__ void k_psolve(DevProblem P, const double* __restrict__ pm, const double* __restrict__ ph,
-                         const double* __restrict__ r, double* __restrict__ z, double gamma) {
+                         const double* __restrict__ r, double* __restrict__ z, double gamma, const DevArgs* da) {
   const int n = P.ncell;
+  if (da) gamma = da->gamma_setup;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
     const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
@@ -209,8 +211,14 @@ __global__ void __launch_bounds__(TX * TY) k_arnoldi_tile(DevProblem P, const do
                                                           const double* __restrict__ hd,
                                                           const double* __restrict__ pm,
                                                           const double* __restrict__ ph, double gamma,
-                                                          double gamma_p, int scale_out) {
+                                                          double gamma_p, int scale_out, const DevArgs* da) {
   __shared__ Tile<2> T;
+  if (da) {
+    in = da->arn_in;
+    out = da->arn_out;
+    gamma = da->gamma;
+    gamma_p = da->gamma_setup;
+  }
   // stage y and vt = in/s (windowed: w·) with halo
   {
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -332,29 +340,29 @@ int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y) {
   return 0;
 }
 
-int launch_psetup(llg_ctx* c, const double* y, double gamma) {
+int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da) {
   LLG_COUNT(KID_PSETUP);
-  k_psetup_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, y, c->d_hd, c->d_pm, c->d_ph);
+  k_psetup_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, y, c->d_hd, c->d_pm, c->d_ph, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   c->gamma_setup = gamma;
   c->have_setup = 1;
   return 0;
 }
 
-int launch_psolve(llg_ctx* c, const double* r, double* z) {
-  if (!c->have_setup) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
+int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da) {
+  if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
-  k_psolve<<<grid_1d(c, c->ncell, 256), 256, 0, c->stream>>>(c->dp, c->d_pm, c->d_ph, r, z, c->gamma_setup);
+  k_psolve<<<grid_1d(c, c->ncell, 256), 256, 0, c->stream>>>(c->dp, c->d_pm, c->d_ph, r, z, c->gamma_setup, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out, const double* y,
-                      double gamma, int scale_out) {
-  if (!c->have_setup) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
+                      double gamma, int scale_out, const DevArgs* da) {
+  if (!c->have_setup && !da) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_ARNOLDI);
   k_arnoldi_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, in, ewt, out, y, c->d_hd, c->d_pm, c->d_ph,
-                                                               gamma, c->gamma_setup, scale_out);
+                                                               gamma, c->gamma_setup, scale_out, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/llg.h"
+#include "dev_integ.h"
 
 #define LLG_CUDA_TRY(expr)                                                   \
   do {                                                                       \
@@ -44,7 +45,10 @@ enum LlgKernel {
   KID_LEARNED, KID_OTHER, KID_COUNT
 };
 extern std::atomic<long long> g_kcount[KID_COUNT];
-#define LLG_COUNT(k) (g_kcount[(k)].fetch_add(1, std::memory_order_relaxed))
+// nonzero while a CUDA graph is being captured on this thread: the capture
+// launches nothing (the graph's own launches are tallied on the device)
+extern thread_local int g_count_off;
+#define LLG_COUNT(k) (g_count_off ? 0LL : g_kcount[(k)].fetch_add(1, std::memory_order_relaxed))
 
 // Physics + geometry view passed by value to every per-cell kernel.
 struct DevProblem {
@@ -104,18 +108,21 @@ struct llg_ctx {
   Integrator* integ = nullptr;
   Learned* learned = nullptr;
   long long nfe_demag = 0;
+  int capturing = 0;   // 1 while the device-resident step graph is captured
 };
 
 // ── physics kernels (k_physics.cu) ─────────────────────────────────────
 int launch_normalize(llg_ctx* c, double* y);
 int launch_rhs(llg_ctx* c, const double* y, const double* hd, double* ydot);
 int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y);
-int launch_psetup(llg_ctx* c, const double* y, double gamma);
-int launch_psolve(llg_ctx* c, const double* r, double* z);
+int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da = nullptr);
+int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da = nullptr);
 // fused Arnoldi operator:  out = s1 ⊙ P^-1 ( vt − γ J vt ),  vt = in / s2
 // (scale_out 0: out = P^-1 (...) without the s1 factor)
+// (da non-null: in, out, gamma and the setup gamma come from the device-resident
+// integrator's DevArgs at run time; the pointer arguments are ignored)
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out,
-                      const double* y, double gamma, int scale_out = 1);
+                      const double* y, double gamma, int scale_out = 1, const DevArgs* da = nullptr);
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot);
 
 // ── demag (k_demag.cu) ─────────────────────────────────────────────────
@@ -172,14 +179,20 @@ int vhin_bound(llg_ctx* c, double rtol, double atol, const double* y0, const dou
                double* tmp);
 
 // fused integrator passes (k_fused.cu); reductions leave raw sums in d_scal[slot..]
-int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot);
-int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor /* null: zero */, double* y);
+int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot,
+                   const DevArgs* da = nullptr);
+// (da non-null: rl1, gamma, the setup gamma and whether ycor is zero come from
+// the device-resident integrator's DevArgs at run time)
+int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor /* null: zero */, double* y,
+                        const DevArgs* da = nullptr);
 int fused_field(llg_ctx* c, const double* y);
 int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* ycor /* null: zero */, double rl1,
-                double gamma, double* negres);
-int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot);
+                double gamma, double* negres, const DevArgs* da = nullptr);
+int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot,
+                           const DevArgs* da = nullptr);
 int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot);
 int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z);
-int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot);
+int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot,
+                       const DevArgs* da = nullptr);
 int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double b, const double* x3,
                 const double* w, int slot);

@@ -204,6 +204,8 @@ def load(path: str | None = None):
         "llg_build_geometry": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
         "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
         "llg_selftest_tcgen05": (I, [I, P(D)]),
+        "llg_trace_control": (I, [VP, VP, C.c_int32]),
+        "llg_trace_count": (I, [VP]),
         "llg_batch_create": (I, [C.c_int32, P(Params), P(VP)]),
         "llg_batch_size": (I, [VP]),
         "llg_batch_ctx": (VP, [VP, C.c_int32]),

@@ -297,6 +297,13 @@ void llg_reset_kernel_counts(void);
 /* Average device time of one launch of family kernel_id (CUDA events on the
  * context's stream), measured on the live integrator buffers.              */
 int  llg_time_kernel(llg_ctx* ctx, int kernel_id, int iters, double* avg_ms);
+/* Device-resident integrator only (no reference counterpart): record, for
+ * the following llg_integrate calls, one 64-bit word per control step —
+ * (globaltimer ns << 5) | step id — into the device buffer d_buf (cap
+ * words, cleared at each call).  d_buf = NULL stops recording.  Returns the
+ * number of words the last call wrote through llg_trace_count.            */
+int  llg_trace_control(llg_ctx* ctx, uint64_t* d_buf, int32_t cap);
+int  llg_trace_count(llg_ctx* ctx);
 /* Known-answer check of the tensor-core path the mixed demag chain uses
  * (no counterpart in the reference): one 128x64x64 FP16 GEMM into tensor
  * memory against a host FP64 product; *max_rel_err = max |D - ref| /
