@@ -67,6 +67,23 @@ struct Integrator {
   double kappa = -1.0;
   // device-resident form (integrator_dev.cu): graph + device copy of this state
   int device_resident = 0;
+  bool ewt_pending = false;   // weights launched, their checks not yet read
+  static constexpr int SLOT_EWT = 4;
+  // CVODE's pre-step checks: weights well defined, ||y|| finite and above the
+  // accuracy floor
+  int state_check(double bad, double nrm) {
+    if (bad != 0.0) { llg_set_error("a tolerance weight is not positive"); return LLG_CV_ILL_INPUT; }
+    if (!isfinite(nrm)) { llg_set_error("non-finite state (WRMS norm of y is not finite)"); return LLG_CV_BAD_STATE; }
+    if (UROUND * nrm > 1.0) return LLG_CV_TOO_MUCH_ACC;
+    return 0;
+  }
+  bool ewt_fresh = false;     // h_scal holds this step's weight checks
+  int ewt_checked() {
+    // the first read-back of spgmr_spec covers SLOT_EWT; other paths read it here
+    if (!ewt_fresh) ok(fetch_range(c, SLOT_EWT, SLOT_EWT + 2));
+    ewt_fresh = false;
+    return state_check(c->h_scal[SLOT_EWT], wrms_of(c->h_scal[SLOT_EWT + 1]));
+  }
   DevInteg* dev = nullptr;
   bool dev_current = false;   // the device copy holds the latest state
 
@@ -240,14 +257,117 @@ struct Integrator {
     return code;
   }
 
-  int spgmr(double* rhs, double delta_tol, bool learned) {
+  bool fuse_update = false, update_done = false;   // see nls_lsolve / newton
+  double upd_s[2] = {0.0, 0.0};
+
+  // ── read-back-light SPGMR (classical Gram-Schmidt, block-Jacobi) ──
+  // The Arnoldi iterations of one solve are enqueued with every coefficient
+  // formed on the device (V0 / ||V0||, the Gram-Schmidt update from its own
+  // dots, V[k] / ||V[k]||), and the first two are enqueued before any read-
+  // back: the second is dropped, unused, when the first converges or needs a
+  // second Gram-Schmidt pass.  One read-back then returns ||r||, the dots and
+  // the norms of both iterations.  Same kernels, same arithmetic, same
+  // decisions as spgmr() below.
+  static int slot_it(int l) { return 64 + 24 * l; }       // dots of iteration l (l + 2 values)
+  static int slot_ss(int l) { return 64 + 24 * l + 20; }  // sum of squares after its update
+  void enqueue_iter(int l) {
+    const int k = l + 1;
+    ok(launch_arnoldi_op(c, V[l], ewt, V[k], y, gamma));
+    const double* Y[MAXLL + 1];
+    for (int i = 0; i <= k; i++) Y[i] = V[i];
+    ok(vdot_multi_dev(c, k + 1, V[k], Y, slot_it(l)));
+    ok(vgs_update_dev(c, k, V, slot_it(l), slot_ss(l)));
+    ok(vscale_gs(c, slot_it(l) + k, slot_ss(l), V[k]));
+  }
+  int spgmr_spec(double* rhs, double delta_tol, bool harvest, double* zb) {
     const int lmax = maxl;
     int nl = 0, krydim = 0, converged = 0;
     nps++;
-    double ss = 0.0;
+    if (harvest) ok(launch_psolve(c, rhs, zb));   // u = P_BJ^-1 r, kept with the solution
+    if (!ok(fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A))) return LS_CONV_FAIL;
+    ok(vscale_rsqrt(c, SLOT_A, V[0]));
+    int queued = (lmax >= 2) ? 2 : 1;
+    for (int l = 0; l < queued; l++) enqueue_iter(l);
+    ok(fetch_range(c, 0, slot_ss(queued - 1) + 1));
+    if (err) return LS_CONV_FAIL;
+    ewt_fresh = ewt_pending;
+    const double* hsc = c->h_scal;
+    const double beta = sqrt(hsc[SLOT_A]);
+    double rnorm = beta, rho = beta;
+    if (rnorm <= delta_tol) { ok(vconst(c, 0.0, rhs)); return LS_SUCCESS; }
+    for (int i = 0; i <= lmax; i++)
+      for (int j = 0; j < lmax; j++) Hes[i][j] = 0.0;
+    double rot = 1.0;
+    for (int l = 0; l < lmax; l++) {
+      if (l >= queued) {
+        enqueue_iter(l);
+        queued = l + 1;
+        ok(fetch_range(c, slot_it(l), slot_ss(l) + 1));
+        if (err) return LS_CONV_FAIL;
+      }
+      nl++;
+      krydim = l + 1;
+      njv++;
+      nps++;
+      const int k = l + 1;
+      const double* d = hsc + slot_it(l);
+      const double vk_norm = sqrt(d[k]);
+      for (int i = 0; i < k; i++) Hes[i][l] = d[i];
+      double nrm = sqrt(hsc[slot_ss(l)]);
+      bool second = false;
+      if (GS_FACTOR * nrm < vk_norm) {
+        // second pass; the device left V[k] unscaled, so later queued
+        // iterations are void and are enqueued again
+        second = true;
+        queued = k;
+        const double* Y[MAXLL + 1];
+        for (int i = 0; i < k; i++) Y[i] = V[i];
+        double dots[MAXLL + 1], cf[MAXLL + 1], ss = 0.0;
+        const double* X[MAXLL + 1];
+        if (ok(vdot_multi_dev(c, k, V[k], Y, SLOT_DOTS))) ok(fetch_scalars(c, SLOT_DOTS, k, dots));
+        cf[0] = 1.0;
+        X[0] = V[k];
+        for (int i = 0; i < k; i++) { Hes[i][l] += dots[i]; cf[i + 1] = -dots[i]; X[i + 1] = V[i]; }
+        if (ok(fused_lincomb_norm(c, k + 1, cf, X, V[k], SLOT_DOTS))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
+        nrm = sqrt(ss);
+      }
+      Hes[k][l] = nrm;
+      if (qr_fact(krydim) != 0) { nli += nl; return LS_CONV_FAIL; }
+      rot *= givens[2 * l + 1];
+      rho = fabs(rot * rnorm);
+      if (rho <= delta_tol) { converged = 1; break; }
+      if (second) ok(vscale(c, 1.0 / Hes[k][l], V[k], V[k]));
+    }
+    nli += nl;
+    yg[0] = rnorm;
+    for (int i = 1; i <= krydim; i++) yg[i] = 0.0;
+    if (qr_sol(krydim, yg) != 0) return LS_QRSOL_FAIL;
+    if (converged || rho < beta) {
+      const double* X[MAXLL + 1];
+      for (int k = 0; k < krydim; k++) X[k] = V[k];
+      const bool taken = converged || ls_curiter == 0;
+      if (taken && fuse_update) {
+        ok(fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A));
+        ok(fetch_scalars(c, SLOT_A, 2, upd_s));
+        update_done = true;
+      } else {
+        ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs));
+      }
+      if (converged && harvest) ok(learned_harvest(c, zb, rhs, ewt, c->gamma_setup));
+      return converged ? LS_SUCCESS : LS_RES_REDUCED;
+    }
+    return LS_CONV_FAIL;
+  }
+
+  int spgmr(double* rhs, double delta_tol, bool learned) {
+    const int lmax = maxl;
+    int nl = 0, krydim = 0, converged = 0;
     const bool harvest = !learned && learned_harvest_wanted(c);
     double* zb = (learned || harvest) ? learned_zbuf(c) : nullptr;
     if ((learned || harvest) && !zb) return LS_CONV_FAIL;
+    if (!learned && classical_gs) return spgmr_spec(rhs, delta_tol, harvest, zb);
+    nps++;
+    double ss = 0.0;
     if (harvest) ok(launch_psolve(c, rhs, zb));   // u = P_BJ^-1 r, kept with the solution
     if (learned) {
       // V0 = ewt (I + gamma Net) P_BJ^-1 r, and its norm
@@ -305,7 +425,16 @@ struct Integrator {
       // zero initial guess needs no pass of its own
       const double* X[MAXLL + 1];
       for (int k = 0; k < krydim; k++) X[k] = V[k];
-      ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs));
+      // when the Newton iteration will take this correction (nls_lsolve
+      // returns 0), apply it to the correction vector in the same pass
+      const bool taken = converged || ls_curiter == 0;
+      if (taken && fuse_update) {
+        ok(fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A));
+        ok(fetch_scalars(c, SLOT_A, 2, upd_s));
+        update_done = true;
+      } else {
+        ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs));
+      }
       if (converged && harvest) ok(learned_harvest(c, zb, rhs, ewt, c->gamma_setup));
       return converged ? LS_SUCCESS : LS_RES_REDUCED;
     }
@@ -466,7 +595,10 @@ struct Integrator {
       probe = true;
     }
     const long long nli0 = nli;
+    fuse_update = true;
+    update_done = false;
     const int r = spgmr(del, dtol, learned);
+    fuse_update = false;
     if (err) return LLG_CV_LSOLVE_FAIL;
     if (learned) { nsl++; nil += nli - nli0; }
     if (probe) { nsb++; nib += nli - nli0; }
@@ -523,7 +655,13 @@ struct Integrator {
         retval = nls_lsolve(del);
         if (retval != 0) break;
         double s[2] = {0.0, 0.0};
-        if (ok(fused_update_wrms2(c, ycor_zero, ycor, del, ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 2, s));
+        if (update_done) {   // the GMRES solution pass already applied it
+          s[0] = upd_s[0];
+          s[1] = upd_s[1];
+        } else if (ok(fused_update_wrms2(c, ycor_zero, ycor, del, ewt, SLOT_A))) {
+          ok(fetch_scalars(c, SLOT_A, 2, s));
+        }
+        update_done = false;
         ycor_zero = false;
         retval = nls_ctest(s, tq[4], m);
         if (err) return LLG_CV_LSOLVE_FAIL;
@@ -708,6 +846,11 @@ struct Integrator {
       cv_set();
       nflag = cv_nls(nflag);
       if (err) return LLG_CV_RHSFUNC_FAIL;
+      if (ewt_pending) {   // the checks CVODE makes before a step, on this step's weights
+        ewt_pending = false;
+        const int e = ewt_checked();
+        if (e) { restore(saved_t); return e; }
+      }
       const int kflag = handle_nflag(&nflag, saved_t, &ncf);
       if (kflag == PREDICT_AGAIN) continue;
       if (kflag != DO_ERROR_TEST) return kflag;
@@ -819,15 +962,10 @@ struct Integrator {
       next_q = q;
       double nrm = 0.0;
       if (nst > 0) {
-        // new weights and ||zn0|| in one pass
-        double s[2] = {0.0, 0.0};
-        if (ok(fused_ewt_wrms(c, rtol, atol, zn[0], ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 2, s));
-        if (s[0] != 0.0) {
-          cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
-          *tret = tn;
-          return LLG_CV_ILL_INPUT;
-        }
-        nrm = wrms_of(s[1]);
+        // new weights and ||zn0|| in one pass; its checks are read with the
+        // step's first read-back (ewt_checked), not waited for here
+        ok(fused_ewt_wrms(c, rtol, atol, zn[0], ewt, SLOT_EWT));
+        ewt_pending = true;
       }
       if ((mxstep > 0) && (nstloc >= mxstep)) {
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
@@ -835,18 +973,15 @@ struct Integrator {
         llg_set_error("mxstep reached before tout");
         return LLG_CV_TOO_MUCH_WORK;
       }
-      if (nst == 0) nrm = wrms(zn[0]);
-      if (err) return LLG_CV_RHSFUNC_FAIL;
-      if (!isfinite(nrm)) {
-        cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
-        *tret = tn;
-        llg_set_error("non-finite state (WRMS norm of y is not finite)");
-        return LLG_CV_BAD_STATE;
-      }
-      if (UROUND * nrm > 1.0) {
-        cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
-        *tret = tn;
-        return LLG_CV_TOO_MUCH_ACC;
+      if (nst == 0) {
+        nrm = wrms(zn[0]);
+        if (err) return LLG_CV_RHSFUNC_FAIL;
+        const int e = state_check(0.0, nrm);
+        if (e) {
+          cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
+          *tret = tn;
+          return e;
+        }
       }
       const int kflag = cv_step();
       if (kflag != 0) {

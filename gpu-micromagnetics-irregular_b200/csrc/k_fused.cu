@@ -239,6 +239,32 @@ __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, doub
   finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
 }
 
+// GMRES correction and Newton update in one pass: d = (sum_k c_k X_k) / w
+// (the correction, stored only when del is non-null), ycor = 1*ycor + 1*d
+// (ycor_in null: zero), and the sums (d*w)^2, (ycor*w)^2 — per element the
+// arithmetic of k_lincomb_div followed by k_update_wrms2, with the latter's
+// reduction partition
+__global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X, const double* __restrict__ w,
+                                                       double* del, const double* ycor_in, double* ycor, long long n,
+                                                       double* partials, unsigned int* counter, double* out) {
+  __shared__ double sm[2 * (RT / 32)];
+  double acc[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
+    double s = c.c[0] * X.p[0][i];
+    for (int k = 1; k < nv; k++) s = c.c[k] * X.p[k][i] + s;
+    const double wi = w[i];
+    const double d = s / wi;
+    if (del) del[i] = d;
+    const double yc = 1.0 * (ycor_in ? ycor_in[i] : 0.0) + 1.0 * d;
+    ycor[i] = yc;
+    const double p = d * wi, q = yc * wi;
+    acc[0] += p * p;
+    acc[1] += q * q;
+  }
+  block_sum<2>(acc, sm);
+  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
 // sums (x1*w)^2 and ((a x2 + b x3)*w)^2
 __global__ void __launch_bounds__(RT) k_wrms2(const double* __restrict__ x1, double a, const double* __restrict__ x2,
                                               double b, const double* __restrict__ x3, const double* __restrict__ w,
@@ -357,6 +383,19 @@ int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double
   LLG_COUNT(KID_REDUCE);
   k_wrms2<<<red_blocks(c->neq), RT, 0, c->stream>>>(x1, a, x2, b, x3, w, c->neq, c->d_red, c->d_counter,
                                                     c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
+                         double* del, bool ycor_zero, double* ycor, int slot) {
+  if (nv < 1 || nv > FV) { llg_set_error("lincomb_update: bad nvec"); return LLG_ERR_ARG; }
+  CPack cp{};
+  XPack xp{};
+  for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
+  LLG_COUNT(KID_REDUCE);
+  k_lincomb_update<<<red_blocks(c->neq), RT, 0, c->stream>>>(nv, cp, xp, w, del, ycor_zero ? nullptr : ycor, ycor,
+                                                             c->neq, c->d_red, c->d_counter, c->d_scal + slot);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

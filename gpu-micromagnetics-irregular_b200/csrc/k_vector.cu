@@ -17,6 +17,7 @@
 // operation sequence in registers, so they give the same bits as the chains
 // while moving each vector once.
 #include <math.h>
+#include <string.h>
 
 #include "llg_internal.h"
 #include "dev_reduce.cuh"
@@ -187,6 +188,47 @@ __global__ void k_scale_cols(int q, CoefPack f, MPtrPack zn, long long n) {
   }
 }
 
+// z = x / sqrt(*ss): the first Krylov vector scaled by its norm without a
+// read-back (the host's vscale(1.0 / rnorm) with rnorm = sqrt(ss))
+__global__ void k_scale_rsqrt(const double* __restrict__ ss, const double* __restrict__ x, double* __restrict__ z,
+                              long long n) {
+  const double a = 1.0 / sqrt(*ss);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] = a * x[i];
+}
+// z = x / sqrt(*ss) unless classical Gram-Schmidt's norm test asks for a
+// second pass (1000 ||x|| < ||x before the update||), in which case x is left
+// as it is for the host to finish
+__global__ void k_scale_gs(const double* __restrict__ vk_dot, const double* __restrict__ ss,
+                           const double* __restrict__ x, double* __restrict__ z, long long n) {
+  if (1000.0 * sqrt(*ss) < sqrt(*vk_dot)) return;
+  const double a = 1.0 / sqrt(*ss);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] = a * x[i];
+}
+// classical Gram-Schmidt update with the dots read on the device:
+// z = 1 z + sum_{i<k} (-dots_i) X_i, and sum z^2 (the arithmetic of
+// k_lincomb_norm with coefficients {1, -dots_0, ..., -dots_{k-1}})
+__global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double* __restrict__ dots, double* z,
+                                                  long long n, double* partials, unsigned int* counter,
+                                                  double* out) {
+  __shared__ double sm[RT / 32];
+  double cf[MAXV - 1];
+#pragma unroll
+  for (int j = 0; j < MAXV - 1; j++) cf[j] = (j < k) ? -dots[j] : 0.0;
+  double acc[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
+    double s = 1.0 * z[i];
+#pragma unroll
+    for (int j = 0; j < MAXV - 1; j++)
+      if (j < k) s = cf[j] * X.p[j][i] + s;
+    z[i] = s;
+    acc[0] += s * s;
+  }
+  block_sum<1>(acc, sm);
+  finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
 int ew_grid(const llg_ctx* c, long long n) {
   long long g = (n + 255) / 256;
   const long long cap = (long long)c->num_sms * 8;
@@ -200,11 +242,12 @@ int ew_grid(const llg_ctx* c, long long n) {
 int reductions_init(llg_ctx* c) {
   c->red_blocks_max = RMAXB;
   LLG_CUDA_TRY(cudaMalloc(&c->d_red, sizeof(double) * MAXV * RMAXB));
-  LLG_CUDA_TRY(cudaMalloc(&c->d_scal, sizeof(double) * 64));
+  LLG_CUDA_TRY(cudaMalloc(&c->d_scal, sizeof(double) * NSCAL));
   LLG_CUDA_TRY(cudaMalloc(&c->d_counter, sizeof(unsigned int) * 4));
   LLG_CUDA_TRY(cudaMemset(c->d_counter, 0, sizeof(unsigned int) * 4));
-  LLG_CUDA_TRY(cudaMemset(c->d_scal, 0, sizeof(double) * 64));
-  LLG_CUDA_TRY(cudaMallocHost(&c->h_scal, sizeof(double) * 64));
+  LLG_CUDA_TRY(cudaMemset(c->d_scal, 0, sizeof(double) * NSCAL));
+  LLG_CUDA_TRY(cudaMallocHost(&c->h_scal, sizeof(double) * NSCAL));
+  memset(c->h_scal, 0, sizeof(double) * NSCAL);
   return 0;
 }
 
@@ -249,6 +292,39 @@ int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double
   const long long n = c->neq;
   LLG_COUNT(KID_REDUCE);
   k_wrms_lin<<<red_blocks(n), RT, 0, c->stream>>>(a, x, b, y, w, n, c->d_red, c->d_counter, c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fetch_range(llg_ctx* c, int lo, int hi) {
+  if (lo < 0 || hi > NSCAL || hi <= lo) { llg_set_error("fetch_range: bad slots"); return LLG_ERR_ARG; }
+  LLG_CUDA_TRY(cudaMemcpyAsync(c->h_scal + lo, c->d_scal + lo, sizeof(double) * (hi - lo), cudaMemcpyDeviceToHost,
+                               c->stream));
+  LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int vscale_rsqrt(llg_ctx* c, int slot_ss, double* x) {
+  LLG_COUNT(KID_ELEMWISE);
+  k_scale_rsqrt<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(c->d_scal + slot_ss, x, x, c->neq);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int vscale_gs(llg_ctx* c, int slot_vk_dot, int slot_ss, double* x) {
+  LLG_COUNT(KID_ELEMWISE);
+  k_scale_gs<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(c->d_scal + slot_vk_dot, c->d_scal + slot_ss, x, x, c->neq);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss) {
+  if (k < 1 || k > MAXV - 1) { llg_set_error("gs_update: bad k"); return LLG_ERR_ARG; }
+  PtrPack pk{};
+  for (int j = 0; j < k; j++) pk.p[j] = V[j];
+  LLG_COUNT(KID_REDUCE);
+  k_gs_update<<<red_blocks(c->neq), RT, 0, c->stream>>>(k, pk, c->d_scal + slot_dots, V[k], c->neq, c->d_red,
+                                                       c->d_counter, c->d_scal + slot_ss);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

@@ -51,6 +51,9 @@ extern thread_local int g_count_off;
 #define LLG_COUNT(k) (g_count_off ? 0LL : g_kcount[(k)].fetch_add(1, std::memory_order_relaxed))
 
 // Physics + geometry view passed by value to every per-cell kernel.
+// scalar result slots (doubles) in d_scal / h_scal
+constexpr int NSCAL = 512;
+
 struct DevProblem {
   int ng, ny;
   int ncell;
@@ -98,7 +101,7 @@ struct llg_ctx {
   int have_setup = 0;
 
   // reductions
-  double* d_red = nullptr;      // partial sums scratch
+  double* d_red = nullptr;      // partial sums scratch (17 x 1024 doubles)
   double* d_scal = nullptr;     // scalar results (device)
   unsigned int* d_counter = nullptr;
   double* h_scal = nullptr;     // pinned host mirror
@@ -163,6 +166,12 @@ int vwrms_dev(llg_ctx* c, const double* x, const double* w, int slot);
 int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double* y,
                    const double* w, int slot);
 int fetch_scalars(llg_ctx* c, int slot, int n, double* out);
+// copy d_scal[lo, hi) to c->h_scal[lo, hi) and wait (one read-back)
+int fetch_range(llg_ctx* c, int lo, int hi);
+// device-coefficient forms used by the read-back-light SPGMR
+int vscale_rsqrt(llg_ctx* c, int slot_ss, double* x);                  // x /= sqrt(d_scal[slot_ss])
+int vscale_gs(llg_ctx* c, int slot_vk_dot, int slot_ss, double* x);    // same, unless a 2nd GS pass is due
+int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss);
 double vmaxnorm_host(llg_ctx* c, const double* x);
 int vlin(llg_ctx* c, double a, const double* x, double b, const double* y, double* z);
 int vscale(llg_ctx* c, double a, const double* x, double* z);
@@ -196,3 +205,8 @@ int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* d
                        const DevArgs* da = nullptr);
 int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double b, const double* x3,
                 const double* w, int slot);
+
+// GMRES correction (stored only when del is non-null) + Newton update + both norms
+int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
+                         double* del, bool ycor_zero, double* ycor, int slot);
+
