@@ -1363,6 +1363,8 @@ int devint_run(DevInteg* d, llg_ctx* c, double tout, double* yout, DState& hs) {
   LLG_CUDA_TRY(cudaPeekAtLastError());
   LLG_CUDA_TRY(cudaGraphLaunch(d->exec, c->stream));
   LLG_CUDA_TRY(cudaMemcpyAsync(d->h_s, d->d_s, sizeof(DState), cudaMemcpyDeviceToHost, c->stream));
+  LLG_CUDA_TRY(cudaMemcpyAsync(c->h_scal + SLOT_TCERR, c->d_scal + SLOT_TCERR, sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream));
   LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
   hs = *d->h_s;
   g_kcount[KID_OTHER].fetch_add(1, std::memory_order_relaxed);   // k_call_args

@@ -28,6 +28,7 @@
 // (field point in the mid-plane) the xz, yz, zx, zy integrals cancel; init
 // verifies this numerically and refuses the plan otherwise.
 #include <math.h>
+#include <string.h>
 #include <stdio.h>
 
 #include <algorithm>
@@ -904,6 +905,17 @@ int demag_stage(llg_ctx* c, int stage, const double* y, double* h) {
 
 int demag_check(llg_ctx* c) {
   if (c->demag && c->demag->tc && demag_tc_failed(c, c->demag->tc)) {
+    llg_set_error("demag: a tensor-core completion wait ran out (results invalid)");
+    return LLG_ERR_TIMEOUT;
+  }
+  return 0;
+}
+
+int demag_check_last(llg_ctx* c) {
+  if (!(c->demag && c->demag->tc)) return 0;
+  int f = 0;
+  memcpy(&f, c->h_scal + SLOT_TCERR, sizeof(int));
+  if (f) {
     llg_set_error("demag: a tensor-core completion wait ran out (results invalid)");
     return LLG_ERR_TIMEOUT;
   }

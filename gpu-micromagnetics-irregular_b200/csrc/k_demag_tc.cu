@@ -450,8 +450,10 @@ int demag_tc_create(llg_ctx* c, int px, int py, int hx, int ny, const float* txx
     tw[j] = make_float2((float)cosl(ang), (float)sinl(ang));
   }
   auto fail = [&](int rc) { demag_tc_destroy(t); return rc; };
-  if (cudaMalloc(&t->d_bmat, BB) != cudaSuccess || cudaMalloc(&t->d_tw, sizeof(float2) * P) != cudaSuccess ||
-      cudaMalloc(&t->d_err, sizeof(int) * 2) != cudaSuccess) {
+  // the timeout flag (and, during this set-up, the tensor scan's maximum) lives
+  // in the context's scalar slots, so the integrator's read-backs carry it home
+  t->d_err = reinterpret_cast<int*>(c->d_scal + SLOT_TCERR);
+  if (cudaMalloc(&t->d_bmat, BB) != cudaSuccess || cudaMalloc(&t->d_tw, sizeof(float2) * P) != cudaSuccess) {
     llg_set_error("demag_tc_create: device allocation failed");
     return fail(LLG_ERR_NOMEM);
   }
@@ -489,7 +491,6 @@ void demag_tc_destroy(DemagTc* t) {
   if (!t) return;
   cudaFree(t->d_bmat);
   cudaFree(t->d_tw);
-  cudaFree(t->d_err);
   delete t;
 }
 

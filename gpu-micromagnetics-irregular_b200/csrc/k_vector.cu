@@ -19,6 +19,9 @@
 #include <math.h>
 #include <string.h>
 
+#include <atomic>
+#include <chrono>
+
 #include "llg_internal.h"
 #include "dev_reduce.cuh"
 
@@ -229,6 +232,19 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
   finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
 }
 
+// one warp copies d_scal[lo, hi) into the mapped host mailbox, makes the
+// copies visible to the host, then writes the sequence word last
+__global__ void k_publish(const double* __restrict__ src, int lo, int hi, double* mail,
+                          unsigned long long seq) {
+  for (int i = lo + (int)threadIdx.x; i < hi; i += 32) mail[i] = src[i];
+  __threadfence_system();
+  __syncwarp();
+  if (threadIdx.x == 0) {
+    volatile unsigned long long* flag = reinterpret_cast<volatile unsigned long long*>(mail + NSCAL);
+    *flag = seq;
+  }
+}
+
 int ew_grid(const llg_ctx* c, long long n) {
   long long g = (n + 255) / 256;
   const long long cap = (long long)c->num_sms * 8;
@@ -248,6 +264,10 @@ int reductions_init(llg_ctx* c) {
   LLG_CUDA_TRY(cudaMemset(c->d_scal, 0, sizeof(double) * NSCAL));
   LLG_CUDA_TRY(cudaMallocHost(&c->h_scal, sizeof(double) * NSCAL));
   memset(c->h_scal, 0, sizeof(double) * NSCAL);
+  LLG_CUDA_TRY(cudaHostAlloc(&c->h_mail, sizeof(double) * (NSCAL + 1), cudaHostAllocMapped));
+  memset(c->h_mail, 0, sizeof(double) * (NSCAL + 1));
+  LLG_CUDA_TRY(cudaHostGetDevicePointer((void**)&c->d_mail, c->h_mail, 0));
+  c->mail_seq = 0;
   return 0;
 }
 
@@ -256,9 +276,11 @@ void reductions_free(llg_ctx* c) {
   cudaFree(c->d_scal);
   cudaFree(c->d_counter);
   if (c->h_scal) cudaFreeHost(c->h_scal);
+  if (c->h_mail) cudaFreeHost(c->h_mail);
   c->d_red = c->d_scal = nullptr;
   c->d_counter = nullptr;
   c->h_scal = nullptr;
+  c->h_mail = c->d_mail = nullptr;
 }
 
 int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot) {
@@ -296,11 +318,34 @@ int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double
   return 0;
 }
 
+// Read-back of d_scal[lo, hi) into h_scal: the publish kernel runs after the
+// producing kernels (stream order) and the host polls the mailbox's sequence
+// word, instead of a device-to-host copy plus a stream synchronisation (the
+// copy engine's start-up and the wake-up were most of a read-back's cost).
+// The poll is bounded by wall time; past it (or after a launch error) the
+// stream is synchronised, which reports any device-side failure.
 int fetch_range(llg_ctx* c, int lo, int hi) {
   if (lo < 0 || hi > NSCAL || hi <= lo) { llg_set_error("fetch_range: bad slots"); return LLG_ERR_ARG; }
-  LLG_CUDA_TRY(cudaMemcpyAsync(c->h_scal + lo, c->d_scal + lo, sizeof(double) * (hi - lo), cudaMemcpyDeviceToHost,
-                               c->stream));
-  LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const unsigned long long seq = ++c->mail_seq;
+  k_publish<<<1, 32, 0, c->stream>>>(c->d_scal, lo, hi, c->d_mail, seq);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  volatile unsigned long long* flag = reinterpret_cast<volatile unsigned long long*>(c->h_mail + NSCAL);
+  bool seen = false;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (unsigned long it = 0;; it++) {
+    if (*flag >= seq) { seen = true; break; }
+    if ((it & 1023) == 1023) {
+      if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(200)) break;
+      if (cudaStreamQuery(c->stream) == cudaSuccess && *flag >= seq) { seen = true; break; }
+    }
+  }
+  if (!seen) {
+    LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (*flag < seq) { llg_set_error("fetch_range: read-back did not arrive"); return LLG_ERR_CUDA; }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  const volatile double* mail = c->h_mail;
+  for (int i = lo; i < hi; i++) c->h_scal[i] = mail[i];
   return 0;
 }
 
@@ -330,9 +375,8 @@ int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_
 }
 
 int fetch_scalars(llg_ctx* c, int slot, int n, double* out) {
-  LLG_CUDA_TRY(cudaMemcpyAsync(c->h_scal + slot, c->d_scal + slot, sizeof(double) * n, cudaMemcpyDeviceToHost,
-                               c->stream));
-  LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const int rc = fetch_range(c, slot, slot + n);
+  if (rc) return rc;
   for (int k = 0; k < n; k++) out[k] = c->h_scal[slot + k];
   return 0;
 }

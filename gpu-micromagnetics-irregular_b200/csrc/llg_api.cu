@@ -341,13 +341,17 @@ int llg_integrator_init(llg_ctx* c, double t0, const double* d_y0, const llg_sol
 int llg_integrate(llg_ctx* c, double tout, double* d_yout, double* tret) {
   if (!c || !d_yout || !tret) return LLG_ERR_ARG;
   const int rc = integrator_run(c, tout, d_yout, tret);
-  const int dc = demag_check(c);
+  // the flag as of the call's last read-back (the BDF step's first linear
+  // solve reads it home with its other scalars); llg_get_stats checks it again
+  const int dc = demag_check_last(c);
   return dc ? dc : rc;
 }
 
 int llg_get_stats(llg_ctx* c, llg_stats* st) {
   if (!c || !st) return LLG_ERR_ARG;
-  return integrator_stats(c, st);
+  const int rc = integrator_stats(c, st);
+  if (rc) return rc;
+  return demag_check(c);
 }
 
 int llg_kernel_counts(int64_t* out, int n) {

@@ -53,6 +53,7 @@ extern thread_local int g_count_off;
 // Physics + geometry view passed by value to every per-cell kernel.
 // scalar result slots (doubles) in d_scal / h_scal
 constexpr int NSCAL = 512;
+constexpr int SLOT_TCERR = 6;   // the tensor-core demag stage's timeout flag (int in the slot's low word)
 
 struct DevProblem {
   int ng, ny;
@@ -105,6 +106,11 @@ struct llg_ctx {
   double* d_scal = nullptr;     // scalar results (device)
   unsigned int* d_counter = nullptr;
   double* h_scal = nullptr;     // pinned host mirror
+  // read-back mailbox: mapped pinned host memory that a one-warp kernel fills
+  // with d_scal[lo, hi) and then a sequence number (the host spins on it)
+  double* h_mail = nullptr;     // NSCAL values + the sequence word (host view)
+  double* d_mail = nullptr;     // the same memory, device view
+  unsigned long long mail_seq = 0;
   int red_blocks_max = 0;
 
   DemagPlan* demag = nullptr;
@@ -145,7 +151,11 @@ void demag_tc_destroy(DemagTc* t);
 int demag_tc_cols(llg_ctx* c, DemagTc* t, float2* Sf);
 int demag_tc_failed(llg_ctx* c, DemagTc* t);
 // LLG_ERR_TIMEOUT if a bounded tensor-core wait of the demag chain ran out
+// (reads the flag back and waits)
 int demag_check(llg_ctx* c);
+// the same, from the copy of the flag that the integrator's last read-back
+// brought home (no wait; integrate calls use it)
+int demag_check_last(llg_ctx* c);
 
 // ── learned preconditioner (k_learned.cu) ──────────────────────────────
 bool learned_active(llg_ctx* c);                 // LLG_PREC_LEARNED with weights, no fallback

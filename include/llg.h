@@ -218,7 +218,9 @@ int  llg_dot_multi_noalloc(int nvec, const double* d_x, const double* const* d_Y
 int  llg_integrator_init(llg_ctx* ctx, double t0, const double* d_y0,
                          const llg_solver_opts* opts);
 /* Advance to tout (CV_NORMAL: may step past tout, returns y(tout) by
- * interpolation).  d_yout: device, 3*ncell.                                */
+ * interpolation).  d_yout: device, 3*ncell.  LLG_ERR_TIMEOUT when a bounded
+ * tensor-core wait of the mixed demag chain ran out, as of the call's last
+ * scalar read-back; llg_get_stats reads that flag again and waits for it.  */
 int  llg_integrate(llg_ctx* ctx, double tout, double* d_yout, double* tret);
 int  llg_get_stats(llg_ctx* ctx, llg_stats* st);
 
