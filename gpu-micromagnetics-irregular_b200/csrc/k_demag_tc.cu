@@ -171,8 +171,28 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
     return true;
   };
 
+  // L2 prefetch of one group's tensor columns (and, for a later group, its
+  // spectrum columns): the tensor multiply and the next group's F1 loads then
+  // read L2 instead of waiting on HBM
+  auto prefetch_group = [&](int gg, bool spectrum) {
+    if (tid != 0 || gg >= a.ngroups) return;
+    for (int qq = 0; qq < NCOL; qq++) {
+      const int k2 = gg * NCOL + qq;
+      if (k2 >= a.hx) break;
+      const long long tb = (long long)k2 * P;
+      prefetch_l2_bulk(a.txx + tb, P * sizeof(float));
+      prefetch_l2_bulk(a.tyy + tb, P * sizeof(float));
+      prefetch_l2_bulk(a.tzz + tb, P * sizeof(float));
+      prefetch_l2_bulk(a.txy + tb, P * sizeof(float2));
+      if (spectrum)
+        for (int cc = 0; cc < 3; cc++)
+          prefetch_l2_bulk(a.S + ((long long)cc * a.hx + k2) * a.ld, (uint32_t)(a.ld * sizeof(float2)));
+    }
+  };
+  prefetch_group(blockIdx.x, false);
   bool good = true;
   for (int g = blockIdx.x; g < a.ngroups && good; g += gridDim.x) {
+    prefetch_group(g + gridDim.x, true);
     const int kx = g * NCOL + q;
     const bool colok = kx < a.hx;
     // ── F1 operand: rows 32q + n2, K = (n1, re/im), this warp's own row ──

@@ -205,7 +205,7 @@ __global__ void k_psolve(DevProblem P, const double* __restrict__ pm, const doub
 // Fused Arnoldi operator of left-preconditioned, ewt-scaled GMRES:
 //   vt = in / s ;  u = vt − γ J(y) vt ;  out = s ⊙ P^-1 u
 // One pass: reads in (stencil), s (stencil), y (stencil), pm/ph, writes out.
-__global__ void __launch_bounds__(TX * TY) k_arnoldi_tile(DevProblem P, const double* __restrict__ in,
+__global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const double* __restrict__ in,
                                                           const double* __restrict__ s,
                                                           double* __restrict__ out, const double* __restrict__ y,
                                                           const double* __restrict__ hd,
@@ -246,9 +246,21 @@ __global__ void __launch_bounds__(TX * TY) k_arnoldi_tile(DevProblem P, const do
   if (gi >= P.ng || gj >= P.ny) return;
   const int n = P.ncell, cell = gj * P.ng + gi;
   const int sx = threadIdx.x + 1, sy = threadIdx.y + 1;
-  const double m[3] = {y[cell], y[n + cell], y[2 * n + cell]};
   const double ss[3] = {s[cell], s[n + cell], s[2 * n + cell]};
-  const double vv[3] = {in[cell] / ss[0], in[n + cell] / ss[1], in[2 * n + cell] / ss[2]};
+  double m[3], vv[3];
+  if (!P.windowed) {   // the staged centre holds y and in/s themselves (window 1)
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      m[a] = T.v[0][a][sy][sx];
+      vv[a] = T.v[1][a][sy][sx];
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      m[a] = y[a * n + cell];
+      vv[a] = in[a * n + cell] / ss[a];
+    }
+  }
   double msk[3], nsk[3];
   cell_axes(P, cell, msk, nsk);
   double h[3];
