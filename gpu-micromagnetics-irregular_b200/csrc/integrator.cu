@@ -130,6 +130,7 @@ struct Integrator {
       dev_current = true;
     }
     DState hs;
+    y_ready = false;
     const int rc = devint_run(dev, c, tout, yout, hs);
     if (rc) { dev_current = false; return rc; }
     import_state(hs);
@@ -494,16 +495,31 @@ struct Integrator {
     gamrat = (nst > 0) ? gamma / gammap : 1.0;
   }
 
+  // The weights of a new step and a rescale of zn are not separate passes:
+  // predict() applies them (fused_predict), together with the first Newton
+  // iterate y = normalise(zn0) that nls_residual then reuses.
+  bool ewt_due = false;       // this step's weights still to be formed
+  bool resc_pending = false;  // zn[j] *= resc_f[j] still to be applied
+  double resc_f[QMAXL + 1] = {};
+  bool y_ready = false;       // y = normalise(zn0) for the current zn0
   void predict() {
     tn += h;
-    ok(vnordsieck_shift(c, q, zn, +1));
+    ok(fused_predict(c, q, zn, resc_f, resc_pending, ewt_due, rtol, atol, ewt, y, SLOT_EWT));
+    if (ewt_due) ewt_pending = true;
+    ewt_due = false;
+    resc_pending = false;
+    y_ready = true;
   }
   void restore(double saved_t) {
     tn = saved_t;
     ok(vnordsieck_shift(c, q, zn, -1));
+    y_ready = false;
   }
   void rescale() {
-    ok(vscale_columns(c, q, eta, zn));
+    if (resc_pending) ok(vscale_columns_f(c, q, resc_f, zn));   // (not reached: a predict follows every rescale)
+    double factor = eta;
+    for (int j = 1; j <= q; j++) { resc_f[j] = factor; factor *= eta; }
+    resc_pending = true;
     h = hscale * eta;
     next_h = h;
     hscale = h;
@@ -562,7 +578,8 @@ struct Integrator {
   int nls_residual(const double* ycor, double* negres) {
     nfe++;
     const double* yc = ycor_zero ? nullptr : ycor;
-    int r = fused_lin_normalize(c, zn[0], yc, y);
+    int r = (ycor_zero && y_ready) ? 0 : fused_lin_normalize(c, zn[0], yc, y);
+    y_ready = false;
     if (!r) r = fused_field(c, y);
     if (!r) r = fused_resid(c, y, zn[1], yc, rl1, gamma, negres);
     if (r) { err = r; return LLG_CV_RHSFUNC_FAIL; }
@@ -746,6 +763,9 @@ struct Integrator {
     ok(vscale(c, h, tempv, zn[1]));
     return TRY_AGAIN;
   }
+  // complete_step; when prepare_next will select the order, the norms it needs
+  // are summed in the same pass (one read-back there)
+  bool norms_ready = false;
   void complete_step() {
     nst++;
     nscon++;
@@ -754,13 +774,17 @@ struct Integrator {
     for (int i = q; i >= 2; i--) tau[i] = tau[i - 1];
     if ((q == 1) && (nst > 1)) tau[2] = tau[1];
     tau[1] = h;
-    ok(vscale_add_multi(c, q + 1, l, acor, zn, zn));
     qwait--;
-    if ((qwait == 1) && (q != qmax)) {
-      ok(vscale(c, 1.0, acor, zn[qmax]));
+    const bool save = (qwait == 1) && (q != qmax);
+    if (save) {
       saved_tq5 = tq[5];
       indx_acor = qmax;
     }
+    norms_ready = (etamax != 1.0) && (qwait == 0);
+    const double cquot =
+        (norms_ready && q != qmax && saved_tq5 != 0.0) ? (tq[5] / saved_tq5) * powi(h / tau[2], L) : 0.0;
+    ok(fused_complete(c, q, qmax, l, acor, zn, save, norms_ready, cquot, ewt, SLOT_A));
+    y_ready = false;
   }
   void set_eta() {
     if (eta < THRESH) {
@@ -773,24 +797,6 @@ struct Integrator {
       hprime = h * eta;
       if (qprime < q) nscon = 0;
     }
-  }
-  double eta_qm1() {
-    if (q > 1) {
-      const double ddn = wrms(zn[q]) * tq[1];
-      return 1.0 / (powr(BIAS1 * ddn, 1.0 / q) + ADDON);
-    }
-    return 0.0;
-  }
-  double eta_qp1() {
-    if (q != qmax) {
-      if (saved_tq5 == 0.0) return 0.0;
-      const double cquot = (tq[5] / saved_tq5) * powi(h / tau[2], L);
-      double dup = 0.0;
-      if (ok(vwrms_diff_dev(c, -cquot, zn[qmax], 1.0, acor, ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 1, &dup));
-      dup *= tq[3];
-      return 1.0 / (powr(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
-    }
-    return 0.0;
   }
   void choose_eta() {
     double etam = etaqm1 > etaq ? etaqm1 : etaq;
@@ -820,18 +826,23 @@ struct Integrator {
       return;
     }
     qwait = 2;
-    if (q > 1 && q != qmax && saved_tq5 != 0.0) {
-      // both order-change norms in one pass
-      const double cquot = (tq[5] / saved_tq5) * powi(h / tau[2], L);
-      double s[2] = {0.0, 0.0};
-      if (ok(fused_wrms2(c, zn[q], -cquot, zn[qmax], 1.0, acor, ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 2, s));
+    // ||zn[q]|| and ||acor - cquot zn[qmax]||, summed by complete_step's pass
+    double s[2] = {0.0, 0.0};
+    if (norms_ready) ok(fetch_scalars(c, SLOT_A, 2, s));
+    else if (ok(fused_wrms2(c, zn[q], -((q != qmax && saved_tq5 != 0.0) ? (tq[5] / saved_tq5) * powi(h / tau[2], L)
+                                                                          : 0.0),
+                            zn[qmax], 1.0, acor, ewt, SLOT_A)))
+      ok(fetch_scalars(c, SLOT_A, 2, s));
+    norms_ready = false;
+    etaqm1 = 0.0;
+    if (q > 1) {
       const double ddn = wrms_of(s[0]) * tq[1];
       etaqm1 = 1.0 / (powr(BIAS1 * ddn, 1.0 / q) + ADDON);
+    }
+    etaqp1 = 0.0;
+    if (q != qmax && saved_tq5 != 0.0) {
       const double dup = wrms_of(s[1]) * tq[3];
       etaqp1 = 1.0 / (powr(BIAS3 * dup, 1.0 / (L + 1)) + ADDON);
-    } else {
-      etaqm1 = eta_qm1();
-      etaqp1 = eta_qp1();
     }
     choose_eta();
     set_eta();
@@ -962,10 +973,9 @@ struct Integrator {
       next_q = q;
       double nrm = 0.0;
       if (nst > 0) {
-        // new weights and ||zn0|| in one pass; its checks are read with the
-        // step's first read-back (ewt_checked), not waited for here
-        ok(fused_ewt_wrms(c, rtol, atol, zn[0], ewt, SLOT_EWT));
-        ewt_pending = true;
+        // new weights and ||zn0||: formed by the step's first predict pass;
+        // their checks are read with the step's first read-back (ewt_checked)
+        ewt_due = true;
       }
       if ((mxstep > 0) && (nstloc >= mxstep)) {
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);

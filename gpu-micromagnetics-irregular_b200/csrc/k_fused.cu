@@ -35,6 +35,9 @@ struct CPack {
 struct XPack {
   const double* p[FV];
 };
+struct ZPack {
+  double* p[8];
+};
 
 int cell_blocks(int ncell) { return red_blocks(ncell); }
 
@@ -283,6 +286,115 @@ __global__ void __launch_bounds__(RT) k_wrms2(const double* __restrict__ x1, dou
   finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
 }
 
+// Start of a BDF attempt, one pass per cell: (new step only) the tolerance
+// weights of zn0 with their bad-weight count and ||zn0||^2; (when pending)
+// zn[j] *= f_j, j = 1..Q; the Nordsieck predictor (Pascal triangle); and y =
+// normalise(zn0 + 0), the first Newton iterate's state.  Per element the
+// arithmetic of k_ewt_wrms, k_scale_cols, k_nordsieck and k_lin_normalize.
+// Every load of a cell is issued before its first store.
+template <int Q>
+__global__ void __launch_bounds__(RT) k_predict_fused(ZPack zn, CPack f, int pend, int do_ewt, double rtol,
+                                                      double atol, double* __restrict__ ewt, double* __restrict__ y,
+                                                      int n, int kind, double eps, double* partials,
+                                                      unsigned int* counter, double* out) {
+  __shared__ double sm[2 * (RT / 32)];
+  double acc[2] = {0.0, 0.0};
+  for (int cell = blockIdx.x * RT + threadIdx.x; cell < n; cell += gridDim.x * RT) {
+    double v[3][Q + 1];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int j = 0; j <= Q; j++) v[a][j] = zn.p[j][(long long)a * n + cell];
+    double m[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const long long i = (long long)a * n + cell;
+      if (do_ewt) {
+        const double t = rtol * fabs(v[a][0]) + atol;
+        if (!(t > 0.0)) acc[0] += 1.0;
+        const double w = 1.0 / t;
+        ewt[i] = w;
+        const double p = v[a][0] * w;
+        acc[1] += p * p;
+      }
+      if (pend) {
+#pragma unroll
+        for (int j = 1; j <= Q; j++) v[a][j] = f.c[j] * v[a][j];
+      }
+#pragma unroll
+      for (int k = 1; k <= Q; k++)
+#pragma unroll
+        for (int j = Q; j >= k; j--) v[a][j - 1] = v[a][j - 1] + v[a][j];
+#pragma unroll
+      for (int j = 0; j < Q; j++) zn.p[j][i] = v[a][j];
+      if (pend) zn.p[Q][i] = v[a][Q];
+      m[a] = 1.0 * v[a][0] + 1.0 * 0.0;
+    }
+    double o[3] = {m[0], m[1], m[2]};
+    if (kind != LLG_NORM_NONE) {
+      const double ymp = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+      if (kind == LLG_NORM_REG) {
+        const double inv = 1.0 / (ymp + eps);
+        o[0] = m[0] * inv; o[1] = m[1] * inv; o[2] = m[2] * inv;
+      } else if (ymp > 1.0e-30) {
+        const double inv = 1.0 / ymp;
+        o[0] = m[0] * inv; o[1] = m[1] * inv; o[2] = m[2] * inv;
+      }
+    }
+    y[cell] = o[0]; y[n + cell] = o[1]; y[2 * n + cell] = o[2];
+  }
+  if (do_ewt) {
+    block_sum<2>(acc, sm);
+    finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  }
+}
+
+// complete_step and the order-selection norms in one pass: zn[j] = l_j acor +
+// zn[j] (j = 0..Q); zn[qmax] = 1 * acor when save; when norms, the sums
+// (zn[Q] w)^2 and ((-cquot zn[qmax] + 1 acor) w)^2 of the updated vectors —
+// the arithmetic of k_scale_add_multi, k_scale and k_wrms2, with k_wrms2's
+// reduction partition.  Every load of an element is issued before its stores.
+template <int Q>
+__global__ void __launch_bounds__(RT) k_complete_norms(int qmax, CPack l, const double* __restrict__ acor, ZPack zn,
+                                                       double* zmaxp, int save, int norms, double a2,
+                                                       const double* __restrict__ w,
+                                                       long long n, double* partials, unsigned int* counter,
+                                                       double* out) {
+  __shared__ double sm[2 * (RT / 32)];
+  double acc[2] = {0.0, 0.0};
+  const bool far = norms && !save && qmax > Q;   // zn[qmax] is read, not updated
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
+    const double xi = acor[i];
+    double v[Q + 1];
+#pragma unroll
+    for (int j = 0; j <= Q; j++) v[j] = zn.p[j][i];
+    const double zfar = far ? zmaxp[i] : 0.0;
+    const double wi = norms ? w[i] : 0.0;
+#pragma unroll
+    for (int j = 0; j <= Q; j++) {
+      v[j] = l.c[j] * xi + v[j];
+      zn.p[j][i] = v[j];
+    }
+    double zmax = (qmax == Q) ? v[Q] : zfar;
+    if (save) {
+      const double z = 1.0 * xi;
+      zmaxp[i] = z;
+      zmax = z;
+    }
+    if (norms) {
+      const double p = v[Q] * wi;
+      const double u = a2 * zmax + 1.0 * xi;
+      const double qq = u * wi;
+      acc[0] += p * p;
+      acc[1] += qq * qq;
+    }
+  }
+  if (norms) {
+    block_sum<2>(acc, sm);
+    finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  }
+}
+
 int ew_blocks(const llg_ctx* c, long long n) {
   long long g = (n + 255) / 256;
   const long long cap = (long long)c->num_sms * 8;
@@ -396,6 +508,60 @@ int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* c
   LLG_COUNT(KID_REDUCE);
   k_lincomb_update<<<red_blocks(c->neq), RT, 0, c->stream>>>(nv, cp, xp, w, del, ycor_zero ? nullptr : ycor, ycor,
                                                              c->neq, c->d_red, c->d_counter, c->d_scal + slot);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pend, bool do_ewt, double rtol,
+                  double atol, double* ewt, double* y, int slot) {
+  if (q < 1 || q > 5) { llg_set_error("predict: bad order"); return LLG_ERR_ARG; }
+  ZPack zp{};
+  CPack fp{};
+  for (int j = 0; j <= q; j++) { zp.p[j] = zn[j]; fp.c[j] = f ? f[j] : 1.0; }
+  LLG_COUNT(KID_ELEMWISE);
+  long long nbl = (c->ncell + RT - 1) / RT;   // ~one cell per thread, up to the partials' capacity
+  if (nbl > RMAXB) nbl = RMAXB;
+  if (nbl < 1) nbl = 1;
+  const int nb = (int)nbl;
+  const int pe = pend ? 1 : 0, de = do_ewt ? 1 : 0;
+  double* out = c->d_scal + slot;
+#define PRED(Q)                                                                                                \
+  k_predict_fused<Q><<<nb, RT, 0, c->stream>>>(zp, fp, pe, de, rtol, atol, ewt, y, c->ncell, c->p.norm_kind,   \
+                                               c->p.norm_eps, c->d_red, c->d_counter, out)
+  switch (q) {
+    case 1: PRED(1); break;
+    case 2: PRED(2); break;
+    case 3: PRED(3); break;
+    case 4: PRED(4); break;
+    default: PRED(5); break;
+  }
+#undef PRED
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int fused_complete(llg_ctx* c, int q, int qmax, const double* l, const double* acor, double* const* zn, bool save,
+                   bool norms, double cquot, const double* w, int slot) {
+  if (q < 0 || q > 5 || qmax < q || qmax > 5) { llg_set_error("complete: bad order"); return LLG_ERR_ARG; }
+  ZPack zp{};
+  CPack lp{};
+  for (int j = 0; j <= qmax; j++) zp.p[j] = zn[j];
+  for (int j = 0; j <= q; j++) lp.c[j] = l[j];
+  LLG_COUNT(KID_ELEMWISE);
+  const int sv = save ? 1 : 0, nm = norms ? 1 : 0;
+#define COMP(Q)                                                                                    \
+  k_complete_norms<Q><<<red_blocks(c->neq), RT, 0, c->stream>>>(qmax, lp, acor, zp, zn[qmax], sv, nm, -cquot, \
+                                                                w, c->neq, c->d_red, c->d_counter,             \
+                                                                c->d_scal + slot)
+  switch (q) {
+    case 0: COMP(0); break;
+    case 1: COMP(1); break;
+    case 2: COMP(2); break;
+    case 3: COMP(3); break;
+    case 4: COMP(4); break;
+    default: COMP(5); break;
+  }
+#undef COMP
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

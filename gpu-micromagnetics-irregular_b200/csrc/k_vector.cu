@@ -460,6 +460,16 @@ int vscale_columns(llg_ctx* c, int q, double eta, double* const* zn) {
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
+int vscale_columns_f(llg_ctx* c, int q, const double* f, double* const* zn) {
+  if (q < 1) return 0;
+  CoefPack fp{};
+  MPtrPack zp{};
+  for (int j = 1; j <= q; j++) { fp.c[j] = f[j]; zp.p[j] = zn[j]; }
+  LLG_COUNT(KID_ELEMWISE);
+  k_scale_cols<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(q, fp, zp, c->neq);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
 int vset_ewt(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot) {
   const long long n = c->neq;
   LLG_COUNT(KID_REDUCE);

@@ -193,6 +193,7 @@ int vscale_add_multi(llg_ctx* c, int nvec, const double* a, const double* x,
                      double* const* Y, double* const* Z);
 int vnordsieck_shift(llg_ctx* c, int q, double* const* zn, int sign);
 int vscale_columns(llg_ctx* c, int q, double eta, double* const* zn);
+int vscale_columns_f(llg_ctx* c, int q, const double* f, double* const* zn);   // zn[j] *= f[j], j = 1..q
 int vset_ewt(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot);
 int vhin_bound(llg_ctx* c, double rtol, double atol, const double* y0, const double* f0,
                double* tmp);
@@ -216,6 +217,14 @@ int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* d
 int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double b, const double* x3,
                 const double* w, int slot);
 
+// start of a BDF attempt: (do_ewt) weights + checks, (pend) zn[j] *= f[j], the
+// Nordsieck predictor and y = normalise(zn0)  [k_fused.cu]
+int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pend, bool do_ewt, double rtol,
+                  double atol, double* ewt, double* y, int slot);
+// complete_step (+ zn[qmax] = acor when save) and, when norms, the order-
+// selection sums of the updated vectors
+int fused_complete(llg_ctx* c, int q, int qmax, const double* l, const double* acor, double* const* zn, bool save,
+                   bool norms, double cquot, const double* w, int slot);
 // GMRES correction (stored only when del is non-null) + Newton update + both norms
 int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
                          double* del, bool ycor_zero, double* ycor, int slot);
