@@ -829,7 +829,7 @@ int demag_create(llg_ctx* c) {
 }
 
 // stage 0 rows_fwd, 1 column convolution, 2 rows_inv; FP64 or mixed chain
-static int demag_run_stage(llg_ctx* c, DemagPlan* d, int stage, const double* y, const double* w, double* h) {
+static int demag_run_stage_raw(llg_ctx* c, DemagPlan* d, int stage, const double* y, const double* w, double* h) {
   const long long cs = (long long)c->ncell;
   if (stage == 0) {
     LLG_COUNT(KID_DEMAG_ROWS_FWD);
@@ -847,6 +847,15 @@ static int demag_run_stage(llg_ctx* c, DemagPlan* d, int stage, const double* y,
   LLG_COUNT(KID_DEMAG_ROWS_INV);
   if (d->mixed) return launch_rows_inv<float>(d, c->stream, d->d_Sf, h, cs, d->rows[1]);
   return launch_rows_inv<double>(d, c->stream, d->d_S, h, cs, d->rows[0]);
+}
+
+// (timed when the family's live kernel timer is on)
+static int demag_run_stage(llg_ctx* c, DemagPlan* d, int stage, const double* y, const double* w, double* h) {
+  const int kid = (stage == 0) ? KID_DEMAG_ROWS_FWD : (stage == 1) ? KID_DEMAG_COLS : KID_DEMAG_ROWS_INV;
+  ktimer_mark(c, kid, true);
+  const int rc = demag_run_stage_raw(c, d, stage, y, w, h);
+  ktimer_mark(c, kid, false);
+  return rc;
 }
 
 int demag_apply(llg_ctx* c, const double* y, double* h) {

@@ -373,8 +373,10 @@ int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* o
                       double gamma, int scale_out, const DevArgs* da) {
   if (!c->have_setup && !da) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_ARNOLDI);
+  ktimer_mark(c, KID_ARNOLDI, true);
   k_arnoldi_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, in, ewt, out, y, c->d_hd, c->d_pm, c->d_ph,
                                                                gamma, c->gamma_setup, scale_out, da);
+  ktimer_mark(c, KID_ARNOLDI, false);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

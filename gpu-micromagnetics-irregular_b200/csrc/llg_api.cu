@@ -69,6 +69,24 @@ static int validate(const llg_params* p) {
   return 0;
 }
 
+void ktimer_mark(llg_ctx* c, int kid, bool pre) {
+  if (!(c->timer_mask & (1u << kid)) || !c->timer_ev || c->capturing) return;
+  int& k = c->timer_n[kid];
+  // a pair per launch; a launch without room for both events is not timed
+  if (pre ? (k + 2 > c->timer_cap) : ((k & 1) == 0)) return;
+  cudaEventRecord(c->timer_ev[kid][k], c->stream);
+  k++;
+}
+
+static void timer_free(llg_ctx* c) {
+  if (!c->timer_ev) return;
+  for (int f = 0; f < KID_COUNT; f++)
+    for (auto e : c->timer_ev[f]) cudaEventDestroy(e);
+  delete[] c->timer_ev;
+  c->timer_ev = nullptr;
+  c->timer_mask = 0;
+}
+
 extern "C" {
 
 const char* llg_last_error(void) { return g_last_error.c_str(); }
@@ -141,6 +159,7 @@ int llg_create(const llg_params* p, llg_ctx** out) {
 void llg_destroy(llg_ctx* c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  timer_free(c);
   integrator_destroy(c->integ);
   learned_destroy(c->learned);
   demag_destroy(c->demag);
@@ -352,6 +371,40 @@ int llg_get_stats(llg_ctx* c, llg_stats* st) {
   const int rc = integrator_stats(c, st);
   if (rc) return rc;
   return demag_check(c);
+}
+
+int llg_kernel_timer_start(llg_ctx* c, uint32_t family_mask, int32_t max_launches) {
+  if (!c || max_launches <= 0) return LLG_ERR_ARG;
+  timer_free(c);
+  c->timer_ev = new std::vector<cudaEvent_t>[KID_COUNT];
+  c->timer_cap = 2 * max_launches;
+  for (int f = 0; f < KID_COUNT; f++) {
+    c->timer_n[f] = 0;
+    if (!(family_mask & (1u << f))) continue;
+    c->timer_ev[f].resize(c->timer_cap);
+    for (auto& e : c->timer_ev[f])
+      if (cudaEventCreate(&e) != cudaSuccess) { timer_free(c); llg_set_error("kernel timer: event creation"); return LLG_ERR_CUDA; }
+  }
+  c->timer_mask = family_mask;
+  return 0;
+}
+
+int llg_kernel_timer_stop(llg_ctx* c, double* total_ms, int64_t* launches, int32_t n) {
+  if (!c || !total_ms || !launches || n <= 0) return LLG_ERR_ARG;
+  if (!c->timer_ev) { llg_set_error("kernel timer not started"); return LLG_ERR_STATE; }
+  LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int f = 0; f < n; f++) { total_ms[f] = 0.0; launches[f] = 0; }
+  for (int f = 0; f < KID_COUNT && f < n; f++) {
+    for (int k = 0; k + 1 < c->timer_n[f]; k += 2) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, c->timer_ev[f][k], c->timer_ev[f][k + 1]) == cudaSuccess) {
+        total_ms[f] += ms;
+        launches[f]++;
+      }
+    }
+  }
+  timer_free(c);
+  return 0;
 }
 
 int llg_kernel_counts(int64_t* out, int n) {

@@ -49,6 +49,9 @@ extern std::atomic<long long> g_kcount[KID_COUNT];
 // launches nothing (the graph's own launches are tallied on the device)
 extern thread_local int g_count_off;
 #define LLG_COUNT(k) (g_count_off ? 0LL : g_kcount[(k)].fetch_add(1, std::memory_order_relaxed))
+struct llg_ctx;
+// event before (pre = true) / after a launch of family kid, when it is timed
+void ktimer_mark(llg_ctx* c, int kid, bool pre);
 
 // Physics + geometry view passed by value to every per-cell kernel.
 // scalar result slots (doubles) in d_scal / h_scal
@@ -118,6 +121,12 @@ struct llg_ctx {
   Learned* learned = nullptr;
   long long nfe_demag = 0;
   int capturing = 0;   // 1 while the device-resident step graph is captured
+  // live timing of selected kernel families (llg_kernel_timer_*): one event
+  // pair around each launch of a family whose bit is set in timer_mask
+  unsigned timer_mask = 0;
+  std::vector<cudaEvent_t>* timer_ev = nullptr;   // [KID_COUNT] lists, pre-created
+  int timer_cap = 0;
+  int timer_n[16] = {};
 };
 
 // ── physics kernels (k_physics.cu) ─────────────────────────────────────

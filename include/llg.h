@@ -299,6 +299,14 @@ void llg_reset_kernel_counts(void);
 /* Average device time of one launch of family kernel_id (CUDA events on the
  * context's stream), measured on the live integrator buffers.              */
 int  llg_time_kernel(llg_ctx* ctx, int kernel_id, int iters, double* avg_ms);
+/* Live kernel timing (no reference counterpart): an event pair on the
+ * context's stream around each of the next max_launches launches of every
+ * family whose bit (1 << family) is set in family_mask — the fused Arnoldi
+ * operator and the three demag stages are instrumented.  _stop waits, then
+ * writes per family (arrays of n) the summed device time and the launches
+ * timed.                                                                  */
+int  llg_kernel_timer_start(llg_ctx* ctx, uint32_t family_mask, int32_t max_launches);
+int  llg_kernel_timer_stop(llg_ctx* ctx, double* total_ms, int64_t* launches, int32_t n);
 /* Device-resident integrator only (no reference counterpart): record, for
  * the following llg_integrate calls, one 64-bit word per control step —
  * (globaltimer ns << 5) | step id — into the device buffer d_buf (cap
