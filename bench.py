@@ -252,11 +252,15 @@ def timed_run(args, form, world, rank, local, lib, clocks=True):
     clk = Clocks(local) if clocks else None
     if clk:
         clk.__enter__()
+    if args.profile_window:
+        torch.cuda.profiler.start()
     e0.record()
     for _ in range(args.steps):
         step()
     e1.record()
     torch.cuda.synchronize()
+    if args.profile_window:
+        torch.cuda.profiler.stop()
     if clk:
         clk.__exit__(None, None, None)
     ms = dist_max(e0.elapsed_time(e1), world)
@@ -603,6 +607,8 @@ def main():
     ap.add_argument("--form", choices=sorted(FORMS), default=None,
                     help="form to time (default: the best one built, compared against plain FP64)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--profile-window", action="store_true",
+                    help="cudaProfilerStart/Stop around the timed steps (ncu --profile-from-start off)")
     ap.add_argument("--workload", choices=["1536x512", "config4"], default="1536x512",
                     help="config4: the 64-instance batched workload (its own JSON line)")
     args = ap.parse_args()
