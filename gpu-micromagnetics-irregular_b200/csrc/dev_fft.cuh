@@ -35,6 +35,17 @@ struct FftPlanT {
   const cx_t<R>* tw;    // tw[k] = exp(-2 pi i k / n)
 };
 
+// Padded transform buffers (PAD = true): one unused element after every 128
+// bytes, so the small-span Stockham scatters (stride R or R*Ns elements
+// across a warp) spread over all banks instead of a few.
+template <typename R, bool PAD>
+__device__ __forceinline__ int fpad(int i) {
+  if constexpr (PAD) return i + (i >> (sizeof(R) == 8 ? 3 : 4));
+  else return i;
+}
+template <typename R>
+__host__ __device__ constexpr int padded_len(int n) { return n + (n >> (sizeof(R) == 8 ? 3 : 4)) + 1; }
+
 template <typename R>
 __device__ __forceinline__ cx_t<R> cmul(cx_t<R> a, cx_t<R> b) {
   return mk<R>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -131,7 +142,7 @@ __device__ __forceinline__ void dft_fixed(cx_t<R>* v) {
 // twiddle + DFT_R + scatter to (j / Ns)·Ns·R + j % Ns + r·Ns.
 // A row of tx threads covers n/R butterflies with at most MB each
 // (tx >= n/EPT is guaranteed by the plan).
-template <typename R, int RAD, int SIGN, int EPT>
+template <typename R, int RAD, int SIGN, int EPT, bool PAD>
 __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& pl, int4 ps) {
   constexpr int MB = (EPT + RAD - 1) / RAD;
   const int n = pl.n, nb = n / RAD, Ns = ps.y, lg = ps.z;
@@ -142,7 +153,7 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
     const int j = threadIdx.x + u * blockDim.x;
     if (j < nb) {
 #pragma unroll
-      for (int r = 0; r < RAD; r++) v[u][r] = buf[j + r * nb];
+      for (int r = 0; r < RAD; r++) v[u][r] = buf[fpad<R, PAD>(j + r * nb)];
     }
   }
   __syncthreads();
@@ -166,7 +177,7 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
       dft_fixed<R, RAD, SIGN>(v[u]);
       const int ob = q * Ns * RAD + jm;
 #pragma unroll
-      for (int r = 0; r < RAD; r++) buf[ob + r * Ns] = v[u][r];
+      for (int r = 0; r < RAD; r++) buf[fpad<R, PAD>(ob + r * Ns)] = v[u][r];
     }
   }
   __syncthreads();
@@ -174,7 +185,7 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
 
 // Any other radix (small primes, test sizes only): one butterfly per thread
 // (the plan sizes tx >= n/R), R <= 64, O(R^2).
-template <typename R, int SIGN>
+template <typename R, int SIGN, bool PAD>
 __device__ void stockham_pass_generic(cx_t<R>* buf, const FftPlanT<R>& pl, int4 ps) {
   const int RAD = ps.x;
   const int n = pl.n, nb = n / RAD, Ns = ps.y;
@@ -182,7 +193,7 @@ __device__ void stockham_pass_generic(cx_t<R>* buf, const FftPlanT<R>& pl, int4 
   const int j = threadIdx.x;
   cx_t<R> v[64];
   if (j < nb) {
-    for (int r = 0; r < RAD; r++) v[r] = buf[j + r * nb];
+    for (int r = 0; r < RAD; r++) v[r] = buf[fpad<R, PAD>(j + r * nb)];
   }
   __syncthreads();
   if (j < nb) {
@@ -192,7 +203,7 @@ __device__ void stockham_pass_generic(cx_t<R>* buf, const FftPlanT<R>& pl, int4 
     for (int k = 0; k < RAD; k++) {
       cx_t<R> acc = v[0];
       for (int r = 1; r < RAD; r++) acc = cadd<R>(acc, cmul<R>(v[r], twid<R, SIGN>(pl, ((r * k) % RAD) * rstride)));
-      buf[ob + k * Ns] = acc;
+      buf[fpad<R, PAD>(ob + k * Ns)] = acc;
     }
   }
   __syncthreads();
@@ -203,15 +214,15 @@ __device__ void stockham_pass_generic(cx_t<R>* buf, const FftPlanT<R>& pl, int4 
 // as straight-line regions in factorisation order (8s, one 4, one 2, 3s, 5s,
 // other primes): a runtime switch over radices inside one loop makes the
 // register allocator keep every variant's state live at once.
-template <typename R, int SIGN, int EPT>
+template <typename R, int SIGN, int EPT, bool PAD = false>
 __device__ void fft_stockham(cx_t<R>* buf, const FftPlanT<R>& pl) {
   int p = 0;
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<R, 8, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
-  if (p < pl.nr && __ldg(&pl.pass[p].x) == 4) { stockham_pass<R, 4, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  if (p < pl.nr && __ldg(&pl.pass[p].x) == 2) { stockham_pass<R, 2, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<R, 3, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<R, 5, SIGN, EPT>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pl.nr; p++) stockham_pass_generic<R, SIGN>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<R, 8, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  if (p < pl.nr && __ldg(&pl.pass[p].x) == 4) { stockham_pass<R, 4, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  if (p < pl.nr && __ldg(&pl.pass[p].x) == 2) { stockham_pass<R, 2, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<R, 3, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<R, 5, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pl.nr; p++) stockham_pass_generic<R, SIGN, PAD>(buf, pl, __ldg(&pl.pass[p]));
 }
 
 }  // namespace

@@ -67,7 +67,8 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
   const int y0 = blockIdx.x * (2 * NB);
   const int n = pl.n;
   const int b = threadIdx.y;
-  cx_t<R>* buf = sm + b * n;
+  const int np = padded_len<R>(n);
+  cx_t<R>* buf = sm + b * np;
   const double* src = in + (long long)c * comp_stride;
   const int ya = y0 + 2 * b, yb = ya + 1;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -82,18 +83,18 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
         vb = src[q] * (w ? w[q] : 1.0);
       }
     }
-    buf[i] = mk<R>((R)va, (R)vb);
+    buf[fpad<R, true>(i)] = mk<R>((R)va, (R)vb);
   }
   __syncthreads();
-  fft_stockham<R, -1, EPT>(buf, pl);
+  fft_stockham<R, -1, EPT, true>(buf, pl);
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int e = tid; e < Hx * 2 * NB; e += T) {
     const int kx = e / (2 * NB), r = e - kx * (2 * NB);
     const int bb = r >> 1, which = r & 1;
     const int y = y0 + r;
     if (y >= nrows) continue;
-    const cx_t<R> zk = sm[bb * n + kx];
-    const cx_t<R> zm = sm[bb * n + ((n - kx) % n)];
+    const cx_t<R> zk = sm[bb * np + fpad<R, true>(kx)];
+    const cx_t<R> zm = sm[bb * np + fpad<R, true>((n - kx) % n)];
     cx_t<R> out;
     if (!which) out = mk<R>(R(0.5) * (zk.x + zm.x), R(0.5) * (zk.y - zm.y));
     else out = mk<R>(R(0.5) * (zk.y + zm.y), R(-0.5) * (zk.x - zm.x));
@@ -188,7 +189,8 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
   const int b = threadIdx.y;
   const bool even = (n % 2) == 0;
   const int ya = y0 + 2 * b, yb = ya + 1;
-  C* buf = sm + b * n;
+  const int np = padded_len<R>(n);
+  C* buf = sm + b * np;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
     const int kk = (k < Hx) ? k : n - k;
     C A = mk<R>(R(0), R(0)), B = mk<R>(R(0), R(0));
@@ -197,17 +199,17 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
     if (yb < nrows) B = col[yb];
     if (kk == 0 || (even && kk == n / 2)) { A.y = R(0); B.y = R(0); }
     if (k >= Hx) { A.y = -A.y; B.y = -B.y; }
-    buf[k] = mk<R>(A.x - B.y, A.y + B.x);
+    buf[fpad<R, true>(k)] = mk<R>(A.x - B.y, A.y + B.x);
   }
   __syncthreads();
-  fft_stockham<R, +1, EPT>(buf, pl);
+  fft_stockham<R, +1, EPT, true>(buf, pl);
   double* dst = h + (long long)c * comp_stride;
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int e = tid; e < NB * 2 * ng; e += T) {
     const int r = e / ng, i = e - r * ng;
     const int y = y0 + r;
     if (y >= nrows) continue;
-    const C z = sm[(r >> 1) * n + i];
+    const C z = sm[(r >> 1) * np + fpad<R, true>(i)];
     dst[(long long)y * ng + i] = (double)((r & 1) ? z.y : z.x);
   }
 }
@@ -520,7 +522,7 @@ template <typename R>
 static int launch_rows_fwd(const DemagPlan* d, cudaStream_t s, const double* in, long long cs, int row_len,
                            int nrows, const double* w, cx_t<R>* S, int ld, int ncomp, const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fx.dev<R>();
-  const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * d->px;
+  const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((nrows + 2 * k.nb - 1) / (2 * k.nb), ncomp), b(d->fx.tx_for(k.ept), k.nb);
 #define ROWS_FWD(NB, E) k_rows_fwd<R, NB, E><<<g, b, sm, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx)
   if (k.nb == 1) { if (k.ept == 8) ROWS_FWD(1, 8); else ROWS_FWD(1, 16); }
@@ -534,7 +536,7 @@ template <typename R>
 static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, const cx_t<R>* S, double* h, long long cs,
                            const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fx.dev<R>();
-  const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * d->px;
+  const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((d->ny + 2 * k.nb - 1) / (2 * k.nb), 3), b(d->fx.tx_for(k.ept), k.nb);
 #define ROWS_INV(NB, E) k_rows_inv<R, NB, E><<<g, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, h, cs, d->ng)
   if (k.nb == 1) { if (k.ept == 8) ROWS_INV(1, 8); else ROWS_INV(1, 16); }
@@ -575,7 +577,7 @@ static int launch_cols_fwd(const DemagPlan* d, cudaStream_t s, double2* S) {
 
 template <typename R>
 static bool rows_ok(const DemagPlan* d, int nb, int ept) {
-  return d->fx.tx_for(ept) * nb <= 1024 && sizeof(cx_t<R>) * (size_t)nb * d->px <= 227 * 1024;
+  return d->fx.tx_for(ept) * nb <= 1024 && sizeof(cx_t<R>) * (size_t)nb * padded_len<R>(d->px) <= 227 * 1024;
 }
 template <typename R>
 static size_t cols_smem(const DemagPlan* d, bool stage) {
@@ -593,7 +595,7 @@ static bool cols_ok(const DemagPlan* d, int ept, bool stage) {
 template <typename R>
 static int set_smem_all(DemagPlan* d) {
   int rc;
-  const size_t r1 = sizeof(cx_t<R>) * (size_t)d->px, r2 = 2 * r1;
+  const size_t r1 = sizeof(cx_t<R>) * (size_t)padded_len<R>(d->px), r2 = 2 * r1;
   if ((rc = set_smem((const void*)k_rows_fwd<R, 1, 8>, r1)) || (rc = set_smem((const void*)k_rows_fwd<R, 1, 16>, r1)) ||
       (rc = set_smem((const void*)k_rows_inv<R, 1, 8>, r1)) || (rc = set_smem((const void*)k_rows_inv<R, 1, 16>, r1)))
     return rc;
