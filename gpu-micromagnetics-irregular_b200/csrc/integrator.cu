@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "llg_internal.h"
+#include "launch.h"
 
 #include "cvode_consts.h"
 
@@ -949,6 +950,9 @@ struct Integrator {
 
   int integrate(double tout, double* yout, double* tret) {
     if (device_applies()) return integrate_device(tout, yout, tret);
+    // programmatic dependent launch: legacy default stream (the demag chain
+    // launched kernel by kernel), block-Jacobi path (no harvest copies)
+    const PdlScope pdl(c->stream == nullptr && !learned_active(c) && !learned_harvest_wanted(c));
     dev_current = false;   // the host path moves the state on
     const size_t vb = sizeof(double) * (size_t)neq;
     if (!started) {
@@ -979,6 +983,7 @@ struct Integrator {
       }
       if ((mxstep > 0) && (nstloc >= mxstep)) {
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
+        pdl_break();
         *tret = tn;
         llg_set_error("mxstep reached before tout");
         return LLG_CV_TOO_MUCH_WORK;
@@ -989,6 +994,7 @@ struct Integrator {
         const int e = state_check(0.0, nrm);
         if (e) {
           cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
+          pdl_break();
           *tret = tn;
           return e;
         }
@@ -996,6 +1002,7 @@ struct Integrator {
       const int kflag = cv_step();
       if (kflag != 0) {
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
+        pdl_break();
         *tret = tn;
         return kflag;
       }

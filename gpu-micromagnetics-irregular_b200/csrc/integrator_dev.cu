@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "llg_internal.h"
+#include "launch.h"
 #include "cvode_consts.h"
 #include "dev_reduce.cuh"
 
@@ -1282,8 +1283,11 @@ int build_graph(DevInteg* d, llg_ctx* c, const DState& hs) {
   c->stream = d->cap[0];
   c->capturing = 1;
   g_count_off = 1;
+  const int pdl_saved = g_no_pdl;
+  g_no_pdl = 1;
   Builder b(c, d, hs);
   b.emit();
+  g_no_pdl = pdl_saved;
   g_count_off = 0;
   c->capturing = 0;
   c->stream = saved;

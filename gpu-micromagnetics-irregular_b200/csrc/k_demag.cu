@@ -39,6 +39,7 @@
 
 #include "dev_fft.cuh"
 #include "llg_internal.h"
+#include "launch.h"
 
 namespace {
 
@@ -61,6 +62,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <typename R, int NB, int EPT>
 __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long long comp_stride, int row_len,
                            int nrows, const double* __restrict__ w, cx_t<R>* __restrict__ S, int ld, int Hx) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   cx_t<R>* sm = reinterpret_cast<cx_t<R>*>(smraw);
   const int c = blockIdx.y;
@@ -111,6 +113,7 @@ template <typename R, int EPT, bool STAGE>
 __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
                             const R* __restrict__ txx, const R* __restrict__ tyy, const R* __restrict__ tzz,
                             const cx_t<R>* __restrict__ txy) {
+  pdl_entry();
   using C = cx_t<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
@@ -165,6 +168,7 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
 // forward column transform only (tensor spectra at init, FP64)
 template <int EPT>
 __global__ void k_cols_fwd(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* sm = reinterpret_cast<double2*>(smraw);
   const int kx = blockIdx.x;
@@ -180,6 +184,7 @@ __global__ void k_cols_fwd(FftPlan pl, double2* __restrict__ S, int ld, int nrow
 template <typename R, int NB, int EPT>
 __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
                            double* __restrict__ h, long long comp_stride, int ng) {
+  pdl_entry();
   using C = cx_t<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
@@ -290,6 +295,7 @@ __device__ __forceinline__ int rep_disp(int i, int n) {
 // T[c][j*px + i] for c < 9; open: the d = -P/2 lines are zeroed (never used
 // by the zero-padded linear convolution).
 __global__ void k_newell(double* __restrict__ T, int px, int py, double thick, int open) {
+  pdl_entry();
   const long long np = (long long)px * py;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < np;
        e += (long long)gridDim.x * blockDim.x) {
@@ -326,6 +332,7 @@ __global__ void k_tensor_finish(const double2* __restrict__ Sxx, const double2* 
                                 const double2* __restrict__ Szy, long long total, double scale,
                                 double* __restrict__ txx, double* __restrict__ tyy, double* __restrict__ tzz,
                                 double2* __restrict__ txy, double* __restrict__ stats) {
+  pdl_entry();
   // stats (per block partial max): [0] max|diag|, [1] max imag diag, [2] max |xz family|, [3] max |xy-yx|
   __shared__ double red[4][256];
   double m0 = 0, m1 = 0, m2 = 0, m3 = 0;
@@ -524,7 +531,7 @@ static int launch_rows_fwd(const DemagPlan* d, cudaStream_t s, const double* in,
   const FftPlanT<R> pl = d->fx.dev<R>();
   const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((nrows + 2 * k.nb - 1) / (2 * k.nb), ncomp), b(d->fx.tx_for(k.ept), k.nb);
-#define ROWS_FWD(NB, E) k_rows_fwd<R, NB, E><<<g, b, sm, s>>>(pl, in, cs, row_len, nrows, w, S, ld, d->hx)
+#define ROWS_FWD(NB, E) klaunch(k_rows_fwd<R, NB, E>, g, b, sm, s, pl, in, cs, row_len, nrows, w, S, ld, d->hx)
   if (k.nb == 1) { if (k.ept == 8) ROWS_FWD(1, 8); else ROWS_FWD(1, 16); }
   else { if (k.ept == 8) ROWS_FWD(2, 8); else ROWS_FWD(2, 16); }
 #undef ROWS_FWD
@@ -538,7 +545,7 @@ static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, const cx_t<R>* S,
   const FftPlanT<R> pl = d->fx.dev<R>();
   const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((d->ny + 2 * k.nb - 1) / (2 * k.nb), 3), b(d->fx.tx_for(k.ept), k.nb);
-#define ROWS_INV(NB, E) k_rows_inv<R, NB, E><<<g, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, h, cs, d->ng)
+#define ROWS_INV(NB, E) klaunch(k_rows_inv<R, NB, E>, g, b, sm, s, pl, S, d->ny, d->ny, d->hx, h, cs, d->ng)
   if (k.nb == 1) { if (k.ept == 8) ROWS_INV(1, 8); else ROWS_INV(1, 16); }
   else { if (k.ept == 8) ROWS_INV(2, 8); else ROWS_INV(2, 16); }
 #undef ROWS_INV
@@ -553,7 +560,7 @@ static int launch_cols_conv(const DemagPlan* d, cudaStream_t s, cx_t<R>* S, cons
   const dim3 b(d->fy.tx_for(k.ept), 3);
   const size_t base = sizeof(cx_t<R>) * 3 * (size_t)d->py;
   const size_t sm = k.stage ? base + (sizeof(R) * 3 + sizeof(cx_t<R>)) * (size_t)d->py : base;
-#define COLS_LAUNCH(E, ST) k_cols_conv<R, E, ST><<<d->hx, b, sm, s>>>(pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy)
+#define COLS_LAUNCH(E, ST) klaunch(k_cols_conv<R, E, ST>, d->hx, b, sm, s, pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy)
   if (k.ept == 8) {
     if (k.stage) COLS_LAUNCH(8, true); else COLS_LAUNCH(8, false);
   } else {
@@ -568,9 +575,9 @@ static int launch_cols_fwd(const DemagPlan* d, cudaStream_t s, double2* S) {
   const FftPlan pl = d->fy.dev<double>();
   const size_t sm = sizeof(double2) * (size_t)d->py;
   if (d->fy.ept == 8)
-    k_cols_fwd<8><<<d->hx, dim3(d->fy.tx, 1), sm, s>>>(pl, S, d->py, d->py, d->hx);
+    klaunch(k_cols_fwd<8>, d->hx, dim3(d->fy.tx, 1), sm, s, pl, S, d->py, d->py, d->hx);
   else
-    k_cols_fwd<16><<<d->hx, dim3(d->fy.tx, 1), sm, s>>>(pl, S, d->py, d->py, d->hx);
+    klaunch(k_cols_fwd<16>, d->hx, dim3(d->fy.tx, 1), sm, s, pl, S, d->py, d->py, d->hx);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -708,6 +715,7 @@ __global__ void k_tensor_to_f32(const double* __restrict__ a, const double* __re
                                 const double* __restrict__ c, const double2* __restrict__ xy, long long n,
                                 float* __restrict__ af, float* __restrict__ bf, float* __restrict__ cf,
                                 float2* __restrict__ xyf) {
+  pdl_entry();
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     af[e] = (float)a[e];
     bf[e] = (float)b[e];
@@ -751,7 +759,7 @@ int demag_create(llg_ctx* c) {
   LLG_CUDA_TRY(cudaMalloc(&d->d_T, sizeof(double) * 9 * np));
 
   cudaStream_t s = c->stream;
-  k_newell<<<c->num_sms * 8, 128, 0, s>>>(d->d_T, d->px, d->py, p.demag_thick, d->open);
+  klaunch(k_newell, c->num_sms * 8, 128, 0, s, d->d_T, d->px, d->py, p.demag_thick, d->open);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   // N(0) (wrapped index 0)
   double n0[9];
@@ -781,7 +789,7 @@ int demag_create(llg_ctx* c) {
   double* d_stats = nullptr;
   LLG_CUDA_TRY(cudaMalloc(&d_stats, sizeof(double) * 4 * nblk));
   const double scale = d->strength / (double)np;
-  k_tensor_finish<<<nblk, 256, 0, s>>>(spec + 0 * nspec, spec + 4 * nspec, spec + 8 * nspec, spec + 1 * nspec,
+  klaunch(k_tensor_finish, nblk, 256, 0, s, spec + 0 * nspec, spec + 4 * nspec, spec + 8 * nspec, spec + 1 * nspec,
                                        spec + 3 * nspec, spec + 2 * nspec, spec + 5 * nspec, spec + 6 * nspec,
                                        spec + 7 * nspec, nspec, scale, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy,
                                        d_stats);
@@ -810,7 +818,7 @@ int demag_create(llg_ctx* c) {
     LLG_CUDA_TRY(cudaMalloc(&d->d_tyyf, sizeof(float) * nspec));
     LLG_CUDA_TRY(cudaMalloc(&d->d_tzzf, sizeof(float) * nspec));
     LLG_CUDA_TRY(cudaMalloc(&d->d_txyf, sizeof(float2) * nspec));
-    k_tensor_to_f32<<<c->num_sms * 4, 256, 0, s>>>(d->d_txx, d->d_tyy, d->d_tzz, d->d_txy, nspec, d->d_txxf,
+    klaunch(k_tensor_to_f32, c->num_sms * 4, 256, 0, s, d->d_txx, d->d_tyy, d->d_tzz, d->d_txy, nspec, d->d_txxf,
                                                    d->d_tyyf, d->d_tzzf, d->d_txyf);
     LLG_CUDA_TRY(cudaPeekAtLastError());
     // tensor-core column stage where the column shape allows it (else FP32 Stockham columns)
@@ -885,7 +893,10 @@ int demag_apply_w(llg_ctx* c, const double* y, const double* w, double* h) {
     cudaGraph_t graph = nullptr;
     LLG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     rc = 0;
+    const int pdl_saved = g_no_pdl;
+    g_no_pdl = 1;
     for (int stage = 0; stage < 3 && rc == 0; stage++) rc = demag_run_stage(c, d, stage, y, w, h);
+    g_no_pdl = pdl_saved;
     const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
     // the capture launched nothing; the replay below is counted instead
     g_kcount[KID_DEMAG_ROWS_FWD].fetch_sub(1);

@@ -45,6 +45,7 @@
 
 #include "dev_tc.cuh"
 #include "llg_internal.h"
+#include "launch.h"
 
 namespace {
 
@@ -105,6 +106,7 @@ __device__ __forceinline__ void acc_ld16(uint32_t tl, uint32_t col, float (&v)[1
 
 template <int D1>
 __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
+  pdl_entry();
   constexpr int K1 = 2 * D1;
   constexpr int oF1h = 0, oF1l = 128 * K1, oF2h = 256 * K1, oF2l = oF2h + 8192, oG1h = oF2h + 16384,
                 oG1l = oG1h + 256 * D1;
@@ -356,6 +358,7 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
 // max |x| over the four FP32 tensor spectra (positive floats order as their bits)
 __global__ void k_absmax4(const float* __restrict__ a, const float* __restrict__ b, const float* __restrict__ c,
                           const float2* __restrict__ d, long long n, unsigned int* out) {
+  pdl_entry();
   float m = 0.f;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
     m = fmaxf(m, fmaxf(fmaxf(fabsf(a[e]), fabsf(b[e])), fmaxf(fabsf(c[e]), fmaxf(fabsf(d[e].x), fabsf(d[e].y)))));
@@ -367,6 +370,7 @@ __global__ void k_absmax4(const float* __restrict__ a, const float* __restrict__
 // ── self-test GEMM: D (128 x 64) = A (128 x 64) * B (64 x 64)^T, FP16 in, FP32 out ──
 __global__ void __launch_bounds__(128, 1) k_tc_selftest(const uint4* __restrict__ ops, int abytes, int bbytes,
                                                         int a_mn, float* __restrict__ D, int* err) {
+  pdl_entry();
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_slot;
@@ -485,7 +489,7 @@ int demag_tc_create(llg_ctx* c, int px, int py, int hx, int ny, const float* txx
   }
   // global tensor scale 2^e_t with max|N| 2^e_t < 1
   unsigned int* d_mx = reinterpret_cast<unsigned int*>(t->d_err + 1);
-  k_absmax4<<<c->num_sms * 4, 256, 0, c->stream>>>(txx, tyy, tzz, txy, (long long)hx * P, d_mx);
+  klaunch(k_absmax4, c->num_sms * 4, 256, 0, c->stream, txx, tyy, tzz, txy, (long long)hx * P, d_mx);
   unsigned int mxb = 0;
   if (cudaMemcpyAsync(&mxb, d_mx, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -526,8 +530,8 @@ int demag_tc_cols(llg_ctx* c, DemagTc* t, float2* Sf) {
   a.s_t = t->s_t;
   a.e_t = t->e_t;
   a.err = t->d_err;
-  if (t->D1 == 16) k_cols_tc<16><<<t->grid, NT, t->smem, c->stream>>>(a);
-  else k_cols_tc<32><<<t->grid, NT, t->smem, c->stream>>>(a);
+  if (t->D1 == 16) klaunch(k_cols_tc<16>, t->grid, NT, t->smem, c->stream, a);
+  else klaunch(k_cols_tc<32>, t->grid, NT, t->smem, c->stream, a);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

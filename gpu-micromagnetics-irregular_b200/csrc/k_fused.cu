@@ -24,6 +24,7 @@
 #include "dev_physics.cuh"
 #include "dev_reduce.cuh"
 #include "llg_internal.h"
+#include "launch.h"
 #include "dev_integ.h"
 
 namespace {
@@ -44,6 +45,7 @@ int cell_blocks(int ncell) { return red_blocks(ncell); }
 __global__ void __launch_bounds__(RT) k_ewt_wrms(double rtol, double atol, const double* __restrict__ y,
                                                  double* __restrict__ ewt, long long n, double* partials,
                                                  unsigned int* counter, double* out, const DevArgs* da) {
+  pdl_entry();
   if (da && !da->run_ewt) return;
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
@@ -66,6 +68,7 @@ __device__ __forceinline__ double ycor_at(const double* ycor, int i) { return yc
 
 __global__ void k_lin_normalize(const double* __restrict__ zn0, const double* __restrict__ ycor,
                                 double* __restrict__ y, int n, int kind, double eps, const DevArgs* da) {
+  pdl_entry();
   if (da && da->ycor_zero) ycor = nullptr;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const double m1 = 1.0 * zn0[k] + 1.0 * ycor_at(ycor, k);
@@ -94,6 +97,7 @@ __global__ void __launch_bounds__(TX * TY) k_rhs_resid_tile(DevProblem P, const 
                                                             const double* __restrict__ ycor, double rl1,
                                                             double gamma, double* __restrict__ negres,
                                                             const DevArgs* da) {
+  pdl_entry();
   __shared__ Tile<1> T;
   if (da) {
     rl1 = da->rl1;
@@ -128,6 +132,7 @@ __global__ void k_rhs_resid_compact(DevProblem P, const double* __restrict__ y, 
                                     const int32_t* __restrict__ inact_ids, int ni,
                                     const double* __restrict__ zn1, const double* __restrict__ ycor, double rl1,
                                     double gamma, double* __restrict__ negres, const DevArgs* da) {
+  pdl_entry();
   const int n = P.ncell;
   if (da) {
     rl1 = da->rl1;
@@ -167,6 +172,7 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
                                                          const double* __restrict__ ewt, double* __restrict__ v0,
                                                          double gamma, double* partials, unsigned int* counter,
                                                          double* out, const DevArgs* da) {
+  pdl_entry();
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
   const int n = P.ncell;
@@ -198,6 +204,7 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
 // z = c0 X0; z = c_k X_k + z (z may alias X0), and sum z^2
 __global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, double* z, long long n,
                                                      double* partials, unsigned int* counter, double* out) {
+  pdl_entry();
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
@@ -212,6 +219,7 @@ __global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, d
 
 __global__ void k_lincomb_div(int nv, CPack c, XPack X, const double* __restrict__ w, double* __restrict__ z,
                               long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     double s = c.c[0] * X.p[0][i];
     for (int k = 1; k < nv; k++) s = c.c[k] * X.p[k][i] + s;
@@ -223,6 +231,7 @@ __global__ void k_lincomb_div(int nv, CPack c, XPack X, const double* __restrict
 __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, double* ycor, const double* __restrict__ del,
                                                      const double* __restrict__ w, long long n, double* partials,
                                                      unsigned int* counter, double* out, const DevArgs* da) {
+  pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
   if (da) {
@@ -250,6 +259,7 @@ __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, doub
 __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X, const double* __restrict__ w,
                                                        double* del, const double* ycor_in, double* ycor, long long n,
                                                        double* partials, unsigned int* counter, double* out) {
+  pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
@@ -272,6 +282,7 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X,
 __global__ void __launch_bounds__(RT) k_wrms2(const double* __restrict__ x1, double a, const double* __restrict__ x2,
                                               double b, const double* __restrict__ x3, const double* __restrict__ w,
                                               long long n, double* partials, unsigned int* counter, double* out) {
+  pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
@@ -297,6 +308,7 @@ __global__ void __launch_bounds__(RT) k_predict_fused(ZPack zn, CPack f, int pen
                                                       double atol, double* __restrict__ ewt, double* __restrict__ y,
                                                       int n, int kind, double eps, double* partials,
                                                       unsigned int* counter, double* out) {
+  pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
   for (int cell = blockIdx.x * RT + threadIdx.x; cell < n; cell += gridDim.x * RT) {
@@ -360,6 +372,7 @@ __global__ void __launch_bounds__(RT) k_complete_norms(int qmax, CPack l, const 
                                                        const double* __restrict__ w,
                                                        long long n, double* partials, unsigned int* counter,
                                                        double* out) {
+  pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
   const bool far = norms && !save && qmax > Q;   // zn[qmax] is read, not updated
@@ -407,7 +420,7 @@ int ew_blocks(const llg_ctx* c, long long n) {
 
 int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot, const DevArgs* da) {
   LLG_COUNT(KID_REDUCE);
-  k_ewt_wrms<<<red_blocks(c->neq), RT, 0, c->stream>>>(rtol, atol, y, ewt, c->neq, c->d_red, c->d_counter,
+  klaunch(k_ewt_wrms, red_blocks(c->neq), RT, 0, c->stream, rtol, atol, y, ewt, c->neq, c->d_red, c->d_counter,
                                                        c->d_scal + slot, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -415,7 +428,7 @@ int fused_ewt_wrms(llg_ctx* c, double rtol, double atol, const double* y, double
 
 int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor, double* y, const DevArgs* da) {
   LLG_COUNT(KID_NORM);
-  k_lin_normalize<<<ew_blocks(c, c->ncell), 256, 0, c->stream>>>(zn0, ycor, y, c->ncell, c->p.norm_kind,
+  klaunch(k_lin_normalize, ew_blocks(c, c->ncell), 256, 0, c->stream, zn0, ycor, y, c->ncell, c->p.norm_kind,
                                                                 c->p.norm_eps, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -428,7 +441,8 @@ int fused_field(llg_ctx* c, const double* y) {
     c->nfe_demag++;
     return 0;
   }
-  LLG_CUDA_TRY(cudaMemsetAsync(c->d_hd, 0, sizeof(double) * 3 * (size_t)c->ncell, c->stream));
+  // no demag: the field buffer was cleared when the context was made and
+  // nothing else writes it
   return 0;
 }
 
@@ -437,12 +451,12 @@ int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* yc
   LLG_COUNT(KID_RHS);
   if (c->p.exec_model == LLG_EXEC_COMPACT) {
     const int tot = c->n_active + c->n_inactive;
-    k_rhs_resid_compact<<<ew_blocks(c, tot), 256, 0, c->stream>>>(c->dp, y, c->d_hd, c->d_active_ids, c->n_active,
+    klaunch(k_rhs_resid_compact, ew_blocks(c, tot), 256, 0, c->stream, c->dp, y, c->d_hd, c->d_active_ids, c->n_active,
                                                                    c->d_inactive_ids, c->n_inactive, zn1, ycor, rl1,
                                                                    gamma, negres, da);
   } else {
     dim3 g((c->p.ng + TX - 1) / TX, (c->p.ny + TY - 1) / TY);
-    k_rhs_resid_tile<<<g, dim3(TX, TY), 0, c->stream>>>(c->dp, y, c->d_hd, zn1, ycor, rl1, gamma, negres, da);
+    klaunch(k_rhs_resid_tile, g, dim3(TX, TY), 0, c->stream, c->dp, y, c->d_hd, zn1, ycor, rl1, gamma, negres, da);
   }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -451,7 +465,7 @@ int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* yc
 int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot, const DevArgs* da) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
-  k_psolve_scale_dot<<<cell_blocks(c->ncell), RT, 0, c->stream>>>(c->dp, c->d_pm, c->d_ph, r, ewt, v0,
+  klaunch(k_psolve_scale_dot, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, ewt, v0,
                                                                   c->gamma_setup, c->d_red, c->d_counter,
                                                                   c->d_scal + slot, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
@@ -464,7 +478,7 @@ int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* con
   XPack xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
   LLG_COUNT(KID_REDUCE);
-  k_lincomb_norm<<<red_blocks(c->neq), RT, 0, c->stream>>>(nv, cp, xp, z, c->neq, c->d_red, c->d_counter,
+  klaunch(k_lincomb_norm, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, z, c->neq, c->d_red, c->d_counter,
                                                            c->d_scal + slot);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -476,7 +490,7 @@ int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* cons
   XPack xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
   LLG_COUNT(KID_ELEMWISE);
-  k_lincomb_div<<<ew_blocks(c, c->neq), 256, 0, c->stream>>>(nv, cp, xp, w, z, c->neq);
+  klaunch(k_lincomb_div, ew_blocks(c, c->neq), 256, 0, c->stream, nv, cp, xp, w, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -484,7 +498,7 @@ int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* cons
 int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot,
                        const DevArgs* da) {
   LLG_COUNT(KID_REDUCE);
-  k_update_wrms2<<<red_blocks(c->neq), RT, 0, c->stream>>>(ycor_zero ? nullptr : ycor, ycor, del, w, c->neq, c->d_red, c->d_counter,
+  klaunch(k_update_wrms2, red_blocks(c->neq), RT, 0, c->stream, ycor_zero ? nullptr : ycor, ycor, del, w, c->neq, c->d_red, c->d_counter,
                                                            c->d_scal + slot, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -493,7 +507,7 @@ int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* d
 int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double b, const double* x3,
                 const double* w, int slot) {
   LLG_COUNT(KID_REDUCE);
-  k_wrms2<<<red_blocks(c->neq), RT, 0, c->stream>>>(x1, a, x2, b, x3, w, c->neq, c->d_red, c->d_counter,
+  klaunch(k_wrms2, red_blocks(c->neq), RT, 0, c->stream, x1, a, x2, b, x3, w, c->neq, c->d_red, c->d_counter,
                                                     c->d_scal + slot);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -506,7 +520,7 @@ int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* c
   XPack xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
   LLG_COUNT(KID_REDUCE);
-  k_lincomb_update<<<red_blocks(c->neq), RT, 0, c->stream>>>(nv, cp, xp, w, del, ycor_zero ? nullptr : ycor, ycor,
+  klaunch(k_lincomb_update, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, w, del, ycor_zero ? nullptr : ycor, ycor,
                                                              c->neq, c->d_red, c->d_counter, c->d_scal + slot);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -526,7 +540,7 @@ int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pe
   const int pe = pend ? 1 : 0, de = do_ewt ? 1 : 0;
   double* out = c->d_scal + slot;
 #define PRED(Q)                                                                                                \
-  k_predict_fused<Q><<<nb, RT, 0, c->stream>>>(zp, fp, pe, de, rtol, atol, ewt, y, c->ncell, c->p.norm_kind,   \
+  klaunch(k_predict_fused<Q>, nb, RT, 0, c->stream, zp, fp, pe, de, rtol, atol, ewt, y, c->ncell, c->p.norm_kind,   \
                                                c->p.norm_eps, c->d_red, c->d_counter, out)
   switch (q) {
     case 1: PRED(1); break;
@@ -550,7 +564,7 @@ int fused_complete(llg_ctx* c, int q, int qmax, const double* l, const double* a
   LLG_COUNT(KID_ELEMWISE);
   const int sv = save ? 1 : 0, nm = norms ? 1 : 0;
 #define COMP(Q)                                                                                    \
-  k_complete_norms<Q><<<red_blocks(c->neq), RT, 0, c->stream>>>(qmax, lp, acor, zp, zn[qmax], sv, nm, -cquot, \
+  klaunch(k_complete_norms<Q>, red_blocks(c->neq), RT, 0, c->stream, qmax, lp, acor, zp, zn[qmax], sv, nm, -cquot, \
                                                                 w, c->neq, c->d_red, c->d_counter,             \
                                                                 c->d_scal + slot)
   switch (q) {

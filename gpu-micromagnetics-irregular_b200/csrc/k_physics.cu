@@ -24,12 +24,14 @@
 #include <math.h>
 
 #include "llg_internal.h"
+#include "launch.h"
 #include "dev_physics.cuh"
 
 namespace {
 
 // ── kernels ────────────────────────────────────────────────────────────
 __global__ void k_normalize(double* __restrict__ y, int n, int kind, double eps) {
+  pdl_entry();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const double m1 = y[k], m2 = y[n + k], m3 = y[2 * n + k];
     const double ymp = sqrt(m1 * m1 + m2 * m2 + m3 * m3);
@@ -46,6 +48,7 @@ __global__ void k_normalize(double* __restrict__ y, int n, int kind, double eps)
 __global__ void __launch_bounds__(TX * TY) k_rhs_tile(DevProblem P, const double* __restrict__ y,
                                                       const double* __restrict__ hd,
                                                       double* __restrict__ ydot) {
+  pdl_entry();
   __shared__ Tile<1> T;
   const double* f[1] = {y};
   load_tile<1>(P, T, f);
@@ -67,6 +70,7 @@ __global__ void __launch_bounds__(TX * TY) k_rhs_tile(DevProblem P, const double
 __global__ void k_rhs_compact(DevProblem P, const double* __restrict__ y, const double* __restrict__ hd,
                               double* __restrict__ ydot, const int32_t* __restrict__ act_ids, int na,
                               const int32_t* __restrict__ inact_ids, int ni) {
+  pdl_entry();
   const int n = P.ncell;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na + ni; t += gridDim.x * blockDim.x) {
     if (t >= na) {
@@ -92,6 +96,7 @@ __global__ void k_rhs_compact(DevProblem P, const double* __restrict__ y, const 
 __global__ void __launch_bounds__(TX * TY) k_jtv_tile(DevProblem P, const double* __restrict__ v,
                                                       double* __restrict__ Jv, const double* __restrict__ y,
                                                       const double* __restrict__ hd) {
+  pdl_entry();
   __shared__ Tile<2> T;
   const double* f[2] = {y, v};
   load_tile<2>(P, T, f);
@@ -125,6 +130,7 @@ __global__ void k_jtv_compact(DevProblem P, const double* __restrict__ v, double
                               const double* __restrict__ y, const double* __restrict__ hd,
                               const int32_t* __restrict__ act_ids, int na, const int32_t* __restrict__ inact_ids,
                               int ni) {
+  pdl_entry();
   const int n = P.ncell;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na + ni; t += gridDim.x * blockDim.x) {
     if (t >= na) {
@@ -161,6 +167,7 @@ __global__ void k_jtv_compact(DevProblem P, const double* __restrict__ v, double
 __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const double* __restrict__ y,
                                                          const double* __restrict__ hd, double* __restrict__ pm,
                                                          double* __restrict__ ph, const DevArgs* da) {
+  pdl_entry();
   if (da && !da->run_setup) return;
   __shared__ Tile<1> T;
   const double* f[1] = {y};
@@ -183,6 +190,7 @@ __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const dou
 
 __global__ void k_psolve(DevProblem P, const double* __restrict__ pm, const double* __restrict__ ph,
                          const double* __restrict__ r, double* __restrict__ z, double gamma, const DevArgs* da) {
+  pdl_entry();
   const int n = P.ncell;
   if (da) gamma = da->gamma_setup;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -212,6 +220,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
                                                           const double* __restrict__ pm,
                                                           const double* __restrict__ ph, double gamma,
                                                           double gamma_p, int scale_out, const DevArgs* da) {
+  pdl_entry();
   __shared__ Tile<2> T;
   if (da) {
     in = da->arn_in;
@@ -317,7 +326,7 @@ int grid_1d(const llg_ctx* c, long long work, int block) {
 int launch_normalize(llg_ctx* c, double* y) {
   if (c->p.norm_kind == LLG_NORM_NONE) return 0;
   LLG_COUNT(KID_NORM);
-  k_normalize<<<grid_1d(c, c->ncell, 256), 256, 0, c->stream>>>(y, c->ncell, c->p.norm_kind, c->p.norm_eps);
+  klaunch(k_normalize, grid_1d(c, c->ncell, 256), 256, 0, c->stream, y, c->ncell, c->p.norm_kind, c->p.norm_eps);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -328,11 +337,11 @@ int launch_rhs(llg_ctx* c, const double* y, const double* hd, double* ydot) {
   if (c->p.exec_model == LLG_EXEC_COMPACT) {
     const int tot = c->n_active + c->n_inactive;
     LLG_COUNT(KID_RHS);
-    k_rhs_compact<<<grid_1d(c, tot, 256), 256, 0, c->stream>>>(c->dp, y, hd, ydot, c->d_active_ids, c->n_active,
+    klaunch(k_rhs_compact, grid_1d(c, tot, 256), 256, 0, c->stream, c->dp, y, hd, ydot, c->d_active_ids, c->n_active,
                                                                c->d_inactive_ids, c->n_inactive);
   } else {
     LLG_COUNT(KID_RHS);
-    k_rhs_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, y, hd, ydot);
+    klaunch(k_rhs_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, y, hd, ydot);
   }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -342,11 +351,11 @@ int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y) {
   if (c->p.exec_model == LLG_EXEC_COMPACT) {
     const int tot = c->n_active + c->n_inactive;
     LLG_COUNT(KID_JTV);
-    k_jtv_compact<<<grid_1d(c, tot, 256), 256, 0, c->stream>>>(c->dp, v, Jv, y, c->d_hd, c->d_active_ids,
+    klaunch(k_jtv_compact, grid_1d(c, tot, 256), 256, 0, c->stream, c->dp, v, Jv, y, c->d_hd, c->d_active_ids,
                                                                c->n_active, c->d_inactive_ids, c->n_inactive);
   } else {
     LLG_COUNT(KID_JTV);
-    k_jtv_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, v, Jv, y, c->d_hd);
+    klaunch(k_jtv_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, v, Jv, y, c->d_hd);
   }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -354,7 +363,7 @@ int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y) {
 
 int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da) {
   LLG_COUNT(KID_PSETUP);
-  k_psetup_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, y, c->d_hd, c->d_pm, c->d_ph, da);
+  klaunch(k_psetup_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, y, c->d_hd, c->d_pm, c->d_ph, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   c->gamma_setup = gamma;
   c->have_setup = 1;
@@ -364,7 +373,7 @@ int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da) 
 int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
-  k_psolve<<<grid_1d(c, c->ncell, 256), 256, 0, c->stream>>>(c->dp, c->d_pm, c->d_ph, r, z, c->gamma_setup, da);
+  klaunch(k_psolve, grid_1d(c, c->ncell, 256), 256, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, z, c->gamma_setup, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -374,7 +383,7 @@ int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* o
   if (!c->have_setup && !da) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_ARNOLDI);
   ktimer_mark(c, KID_ARNOLDI, true);
-  k_arnoldi_tile<<<tile_grid(c), dim3(TX, TY), 0, c->stream>>>(c->dp, in, ewt, out, y, c->d_hd, c->d_pm, c->d_ph,
+  klaunch(k_arnoldi_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, in, ewt, out, y, c->d_hd, c->d_pm, c->d_ph,
                                                                gamma, c->gamma_setup, scale_out, da);
   ktimer_mark(c, KID_ARNOLDI, false);
   LLG_CUDA_TRY(cudaPeekAtLastError());
@@ -385,12 +394,10 @@ int rhs_full(llg_ctx* c, double t, double* y, double* ydot) {
   (void)t;
   int rc = launch_normalize(c, y);
   if (rc) return rc;
-  if (c->demag) {
+  if (c->demag) {   // (without demag the field buffer stays as cleared at creation)
     rc = demag_apply(c, y, c->d_hd);
     if (rc) return rc;
     c->nfe_demag++;
-  } else {
-    LLG_CUDA_TRY(cudaMemsetAsync(c->d_hd, 0, sizeof(double) * 3 * (size_t)c->ncell, c->stream));
   }
   return launch_rhs(c, y, c->d_hd, ydot);
 }

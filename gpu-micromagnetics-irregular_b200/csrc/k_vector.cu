@@ -23,6 +23,7 @@
 #include <chrono>
 
 #include "llg_internal.h"
+#include "launch.h"
 #include "dev_reduce.cuh"
 
 namespace {
@@ -42,6 +43,7 @@ struct CoefPack {
 template <int K>
 __global__ void __launch_bounds__(RT) k_dot_multi(const double* __restrict__ x, PtrPack Y, long long n,
                                                   double* partials, unsigned int* counter, double* out) {
+  pdl_entry();
   __shared__ double sm[K * (RT / 32)];
   double acc[K];
 #pragma unroll
@@ -57,6 +59,7 @@ __global__ void __launch_bounds__(RT) k_dot_multi(const double* __restrict__ x, 
 
 __global__ void __launch_bounds__(RT) k_wrms(const double* __restrict__ x, const double* __restrict__ w,
                                              long long n, double* partials, unsigned int* counter, double* out) {
+  pdl_entry();
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
@@ -72,6 +75,7 @@ __global__ void __launch_bounds__(RT) k_wrms_lin(double a, const double* __restr
                                                  const double* __restrict__ y, const double* __restrict__ w,
                                                  long long n, double* partials, unsigned int* counter,
                                                  double* out) {
+  pdl_entry();
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
@@ -87,6 +91,7 @@ __global__ void __launch_bounds__(RT) k_wrms_lin(double a, const double* __restr
 __global__ void __launch_bounds__(RT) k_set_ewt(double rtol, double atol, const double* __restrict__ y,
                                                 double* __restrict__ ewt, long long n, double* partials,
                                                 unsigned int* counter, double* out) {
+  pdl_entry();
   double bad[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
     const double t = rtol * fabs(y[i]) + atol;
@@ -108,6 +113,7 @@ __global__ void __launch_bounds__(RT) k_set_ewt(double rtol, double atol, const 
 __global__ void __launch_bounds__(RT) k_hin_bound(double rtol, double atol, const double* __restrict__ y,
                                                   const double* __restrict__ f, long long n, double* partials,
                                                   unsigned int* counter, double* out) {
+  pdl_entry();
   double m[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
     const double ay = fabs(y[i]);
@@ -128,29 +134,35 @@ __global__ void __launch_bounds__(RT) k_hin_bound(double rtol, double atol, cons
 
 __global__ void k_lin(double a, const double* __restrict__ x, double b, const double* __restrict__ y,
                       double* __restrict__ z, long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     z[i] = a * x[i] + b * y[i];
 }
 __global__ void k_scale(double a, const double* __restrict__ x, double* __restrict__ z, long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     z[i] = a * x[i];
 }
 __global__ void k_const(double a, double* __restrict__ z, long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     z[i] = a;
 }
 __global__ void k_prod(const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ z,
                        long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     z[i] = x[i] * y[i];
 }
 __global__ void k_div(const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ z,
                       long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     z[i] = x[i] / y[i];
 }
 // z = c0 X0; z = c_k X_k + z   (z may alias X0)
 __global__ void k_lincomb(int nv, CoefPack c, PtrPack X, double* z, long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double s = c.c[0] * X.p[0][i];
@@ -161,6 +173,7 @@ __global__ void k_lincomb(int nv, CoefPack c, PtrPack X, double* z, long long n)
 // Z_j = a_j x + Y_j
 __global__ void k_scale_add_multi(int nv, CoefPack a, const double* __restrict__ x, PtrPack Y, MPtrPack Z,
                                   long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const double xi = x[i];
@@ -170,6 +183,7 @@ __global__ void k_scale_add_multi(int nv, CoefPack a, const double* __restrict__
 // Pascal triangle (sign +1: predictor, -1: restore) over zn[0..Q], in registers
 template <int Q>
 __global__ void k_nordsieck(MPtrPack zn, int sign, long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double v[Q + 1];
@@ -185,6 +199,7 @@ __global__ void k_nordsieck(MPtrPack zn, int sign, long long n) {
 }
 // zn[j] *= f_j for j = 1..q
 __global__ void k_scale_cols(int q, CoefPack f, MPtrPack zn, long long n) {
+  pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     for (int j = 1; j <= q; j++) zn.p[j][i] = f.c[j] * zn.p[j][i];
@@ -195,6 +210,7 @@ __global__ void k_scale_cols(int q, CoefPack f, MPtrPack zn, long long n) {
 // read-back (the host's vscale(1.0 / rnorm) with rnorm = sqrt(ss))
 __global__ void k_scale_rsqrt(const double* __restrict__ ss, const double* __restrict__ x, double* __restrict__ z,
                               long long n) {
+  pdl_entry();
   const double a = 1.0 / sqrt(*ss);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     z[i] = a * x[i];
@@ -204,6 +220,7 @@ __global__ void k_scale_rsqrt(const double* __restrict__ ss, const double* __res
 // as it is for the host to finish
 __global__ void k_scale_gs(const double* __restrict__ vk_dot, const double* __restrict__ ss,
                            const double* __restrict__ x, double* __restrict__ z, long long n) {
+  pdl_entry();
   if (1000.0 * sqrt(*ss) < sqrt(*vk_dot)) return;
   const double a = 1.0 / sqrt(*ss);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -215,6 +232,7 @@ __global__ void k_scale_gs(const double* __restrict__ vk_dot, const double* __re
 __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double* __restrict__ dots, double* z,
                                                   long long n, double* partials, unsigned int* counter,
                                                   double* out) {
+  pdl_entry();
   __shared__ double sm[RT / 32];
   double cf[MAXV - 1];
 #pragma unroll
@@ -236,6 +254,7 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
 // copies visible to the host, then writes the sequence word last
 __global__ void k_publish(const double* __restrict__ src, int lo, int hi, double* mail,
                           unsigned long long seq) {
+  pdl_entry();
   for (int i = lo + (int)threadIdx.x; i < hi; i += 32) mail[i] = src[i];
   __threadfence_system();
   __syncwarp();
@@ -293,7 +312,7 @@ int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y
   double* out = c->d_scal + slot;
   switch (nvec) {
 #define DOTK(K) \
-  case K: LLG_COUNT(KID_REDUCE); k_dot_multi<K><<<nb, RT, 0, c->stream>>>(x, pk, n, c->d_red, c->d_counter, out); break;
+  case K: LLG_COUNT(KID_REDUCE); klaunch(k_dot_multi<K>, nb, RT, 0, c->stream, x, pk, n, c->d_red, c->d_counter, out); break;
     DOTK(1) DOTK(2) DOTK(3) DOTK(4) DOTK(5) DOTK(6) DOTK(7) DOTK(8)
     DOTK(9) DOTK(10) DOTK(11) DOTK(12) DOTK(13) DOTK(14) DOTK(15) DOTK(16)
 #undef DOTK
@@ -305,7 +324,7 @@ int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y
 int vwrms_dev(llg_ctx* c, const double* x, const double* w, int slot) {
   const long long n = c->neq;
   LLG_COUNT(KID_REDUCE);
-  k_wrms<<<red_blocks(n), RT, 0, c->stream>>>(x, w, n, c->d_red, c->d_counter, c->d_scal + slot);
+  klaunch(k_wrms, red_blocks(n), RT, 0, c->stream, x, w, n, c->d_red, c->d_counter, c->d_scal + slot);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -313,7 +332,7 @@ int vwrms_dev(llg_ctx* c, const double* x, const double* w, int slot) {
 int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double* y, const double* w, int slot) {
   const long long n = c->neq;
   LLG_COUNT(KID_REDUCE);
-  k_wrms_lin<<<red_blocks(n), RT, 0, c->stream>>>(a, x, b, y, w, n, c->d_red, c->d_counter, c->d_scal + slot);
+  klaunch(k_wrms_lin, red_blocks(n), RT, 0, c->stream, a, x, b, y, w, n, c->d_red, c->d_counter, c->d_scal + slot);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -327,7 +346,7 @@ int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double
 int fetch_range(llg_ctx* c, int lo, int hi) {
   if (lo < 0 || hi > NSCAL || hi <= lo) { llg_set_error("fetch_range: bad slots"); return LLG_ERR_ARG; }
   const unsigned long long seq = ++c->mail_seq;
-  k_publish<<<1, 32, 0, c->stream>>>(c->d_scal, lo, hi, c->d_mail, seq);
+  klaunch(k_publish, 1, 32, 0, c->stream, c->d_scal, lo, hi, c->d_mail, seq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   volatile unsigned long long* flag = reinterpret_cast<volatile unsigned long long*>(c->h_mail + NSCAL);
   bool seen = false;
@@ -351,14 +370,14 @@ int fetch_range(llg_ctx* c, int lo, int hi) {
 
 int vscale_rsqrt(llg_ctx* c, int slot_ss, double* x) {
   LLG_COUNT(KID_ELEMWISE);
-  k_scale_rsqrt<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(c->d_scal + slot_ss, x, x, c->neq);
+  klaunch(k_scale_rsqrt, ew_grid(c, c->neq), 256, 0, c->stream, c->d_scal + slot_ss, x, x, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
 int vscale_gs(llg_ctx* c, int slot_vk_dot, int slot_ss, double* x) {
   LLG_COUNT(KID_ELEMWISE);
-  k_scale_gs<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(c->d_scal + slot_vk_dot, c->d_scal + slot_ss, x, x, c->neq);
+  klaunch(k_scale_gs, ew_grid(c, c->neq), 256, 0, c->stream, c->d_scal + slot_vk_dot, c->d_scal + slot_ss, x, x, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -368,7 +387,7 @@ int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_
   PtrPack pk{};
   for (int j = 0; j < k; j++) pk.p[j] = V[j];
   LLG_COUNT(KID_REDUCE);
-  k_gs_update<<<red_blocks(c->neq), RT, 0, c->stream>>>(k, pk, c->d_scal + slot_dots, V[k], c->neq, c->d_red,
+  klaunch(k_gs_update, red_blocks(c->neq), RT, 0, c->stream, k, pk, c->d_scal + slot_dots, V[k], c->neq, c->d_red,
                                                        c->d_counter, c->d_scal + slot_ss);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -383,31 +402,31 @@ int fetch_scalars(llg_ctx* c, int slot, int n, double* out) {
 
 int vlin(llg_ctx* c, double a, const double* x, double b, const double* y, double* z) {
   LLG_COUNT(KID_ELEMWISE);
-  k_lin<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(a, x, b, y, z, c->neq);
+  klaunch(k_lin, ew_grid(c, c->neq), 256, 0, c->stream, a, x, b, y, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 int vscale(llg_ctx* c, double a, const double* x, double* z) {
   LLG_COUNT(KID_ELEMWISE);
-  k_scale<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(a, x, z, c->neq);
+  klaunch(k_scale, ew_grid(c, c->neq), 256, 0, c->stream, a, x, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 int vconst(llg_ctx* c, double a, double* z) {
   LLG_COUNT(KID_ELEMWISE);
-  k_const<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(a, z, c->neq);
+  klaunch(k_const, ew_grid(c, c->neq), 256, 0, c->stream, a, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 int vprod(llg_ctx* c, const double* x, const double* y, double* z) {
   LLG_COUNT(KID_ELEMWISE);
-  k_prod<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(x, y, z, c->neq);
+  klaunch(k_prod, ew_grid(c, c->neq), 256, 0, c->stream, x, y, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 int vdiv(llg_ctx* c, const double* x, const double* y, double* z) {
   LLG_COUNT(KID_ELEMWISE);
-  k_div<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(x, y, z, c->neq);
+  klaunch(k_div, ew_grid(c, c->neq), 256, 0, c->stream, x, y, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -417,7 +436,7 @@ int vlincomb(llg_ctx* c, int nvec, const double* coef, const double* const* X, d
   PtrPack pk{};
   for (int k = 0; k < nvec; k++) { cp.c[k] = coef[k]; pk.p[k] = X[k]; }
   LLG_COUNT(KID_ELEMWISE);
-  k_lincomb<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(nvec, cp, pk, z, c->neq);
+  klaunch(k_lincomb, ew_grid(c, c->neq), 256, 0, c->stream, nvec, cp, pk, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -429,7 +448,7 @@ int vscale_add_multi(llg_ctx* c, int nvec, const double* a, const double* x, dou
   MPtrPack zp{};
   for (int k = 0; k < nvec; k++) { cp.c[k] = a[k]; yp.p[k] = Y[k]; zp.p[k] = Z[k]; }
   LLG_COUNT(KID_ELEMWISE);
-  k_scale_add_multi<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(nvec, cp, x, yp, zp, c->neq);
+  klaunch(k_scale_add_multi, ew_grid(c, c->neq), 256, 0, c->stream, nvec, cp, x, yp, zp, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -440,11 +459,11 @@ int vnordsieck_shift(llg_ctx* c, int q, double* const* zn, int sign) {
   LLG_COUNT(KID_ELEMWISE);
   const int g = ew_grid(c, c->neq);
   switch (q) {
-    case 1: k_nordsieck<1><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
-    case 2: k_nordsieck<2><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
-    case 3: k_nordsieck<3><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
-    case 4: k_nordsieck<4><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
-    default: k_nordsieck<5><<<g, 256, 0, c->stream>>>(zp, sign, c->neq); break;
+    case 1: klaunch(k_nordsieck<1>, g, 256, 0, c->stream, zp, sign, c->neq); break;
+    case 2: klaunch(k_nordsieck<2>, g, 256, 0, c->stream, zp, sign, c->neq); break;
+    case 3: klaunch(k_nordsieck<3>, g, 256, 0, c->stream, zp, sign, c->neq); break;
+    case 4: klaunch(k_nordsieck<4>, g, 256, 0, c->stream, zp, sign, c->neq); break;
+    default: klaunch(k_nordsieck<5>, g, 256, 0, c->stream, zp, sign, c->neq); break;
   }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -456,7 +475,7 @@ int vscale_columns(llg_ctx* c, int q, double eta, double* const* zn) {
   double factor = eta;
   for (int j = 1; j <= q; j++) { f.c[j] = factor; factor *= eta; zp.p[j] = zn[j]; }
   LLG_COUNT(KID_ELEMWISE);
-  k_scale_cols<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(q, f, zp, c->neq);
+  klaunch(k_scale_cols, ew_grid(c, c->neq), 256, 0, c->stream, q, f, zp, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -466,14 +485,14 @@ int vscale_columns_f(llg_ctx* c, int q, const double* f, double* const* zn) {
   MPtrPack zp{};
   for (int j = 1; j <= q; j++) { fp.c[j] = f[j]; zp.p[j] = zn[j]; }
   LLG_COUNT(KID_ELEMWISE);
-  k_scale_cols<<<ew_grid(c, c->neq), 256, 0, c->stream>>>(q, fp, zp, c->neq);
+  klaunch(k_scale_cols, ew_grid(c, c->neq), 256, 0, c->stream, q, fp, zp, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 int vset_ewt(llg_ctx* c, double rtol, double atol, const double* y, double* ewt, int slot) {
   const long long n = c->neq;
   LLG_COUNT(KID_REDUCE);
-  k_set_ewt<<<red_blocks(n), RT, 0, c->stream>>>(rtol, atol, y, ewt, n, c->d_red, c->d_counter, c->d_scal + slot);
+  klaunch(k_set_ewt, red_blocks(n), RT, 0, c->stream, rtol, atol, y, ewt, n, c->d_red, c->d_counter, c->d_scal + slot);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -481,7 +500,7 @@ int vhin_bound(llg_ctx* c, double rtol, double atol, const double* y0, const dou
   (void)tmp;
   const long long n = c->neq;
   LLG_COUNT(KID_REDUCE);
-  k_hin_bound<<<red_blocks(n), RT, 0, c->stream>>>(rtol, atol, y0, f0, n, c->d_red, c->d_counter, c->d_scal + 40);
+  klaunch(k_hin_bound, red_blocks(n), RT, 0, c->stream, rtol, atol, y0, f0, n, c->d_red, c->d_counter, c->d_scal + 40);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

@@ -127,6 +127,8 @@ struct llg_ctx {
   std::vector<cudaEvent_t>* timer_ev = nullptr;   // [KID_COUNT] lists, pre-created
   int timer_cap = 0;
   int timer_n[16] = {};
+  int timer_stride = 1;        // time every timer_stride-th launch of a family
+  long long timer_seen[16] = {};
 };
 
 // ── physics kernels (k_physics.cu) ─────────────────────────────────────

@@ -205,7 +205,7 @@ def load(path: str | None = None):
         "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
         "llg_selftest_tcgen05": (I, [I, P(D)]),
         "llg_trace_control": (I, [VP, VP, C.c_int32]),
-        "llg_kernel_timer_start": (I, [VP, C.c_uint32, C.c_int32]),
+        "llg_kernel_timer_start": (I, [VP, C.c_uint32, C.c_int32, C.c_int32]),
         "llg_kernel_timer_stop": (I, [VP, P(D), P(C.c_int64), C.c_int32]),
         "llg_trace_count": (I, [VP]),
         "llg_batch_create": (I, [C.c_int32, P(Params), P(VP)]),

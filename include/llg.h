@@ -300,12 +300,14 @@ void llg_reset_kernel_counts(void);
  * context's stream), measured on the live integrator buffers.              */
 int  llg_time_kernel(llg_ctx* ctx, int kernel_id, int iters, double* avg_ms);
 /* Live kernel timing (no reference counterpart): an event pair on the
- * context's stream around each of the next max_launches launches of every
- * family whose bit (1 << family) is set in family_mask — the fused Arnoldi
- * operator and the three demag stages are instrumented.  _stop waits, then
- * writes per family (arrays of n) the summed device time and the launches
- * timed.                                                                  */
-int  llg_kernel_timer_start(llg_ctx* ctx, uint32_t family_mask, int32_t max_launches);
+ * context's stream around every stride-th launch (the 1st, (stride+1)-th,
+ * ...) of every family whose bit (1 << family) is set in family_mask, up to
+ * max_launches timed launches per family — the fused Arnoldi operator and
+ * the three demag stages are instrumented.  A timed launch waits for its
+ * predecessor in full (no programmatic dependent launch across an event).
+ * _stop waits, then writes per family (arrays of n) the summed device time
+ * and the launches timed.                                                 */
+int  llg_kernel_timer_start(llg_ctx* ctx, uint32_t family_mask, int32_t max_launches, int32_t stride);
 int  llg_kernel_timer_stop(llg_ctx* ctx, double* total_ms, int64_t* launches, int32_t n);
 /* Device-resident integrator only (no reference counterpart): record, for
  * the following llg_integrate calls, one 64-bit word per control step —
