@@ -77,6 +77,7 @@ struct TcArgs {
 
 union H8 {
   __half h[8];
+  __half2 h2[4];
   uint4 u;
 };
 
@@ -98,8 +99,7 @@ __device__ __forceinline__ void issue3(uint32_t d, uint32_t aH, uint32_t aL, uin
 // hi + 2^-11 lo of 16 accumulator columns starting at column `col` of this warp's lanes
 __device__ __forceinline__ void acc_ld16(uint32_t tl, uint32_t col, float (&v)[16]) {
   float lo[16];
-  tmem_ld16(tl + col, v);
-  tmem_ld16(tl + col + 64, lo);
+  tmem_ld16x2(tl + col, tl + col + 64, v, lo);
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = fmaf(lo[i], LO_UNSCALE, v[i]);
 }
@@ -118,11 +118,13 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
   __shared__ int s_fail;
   __shared__ int s_e[3][NCOL];    // per (component, column) input exponent
   __shared__ int s_eo[3][NCOL];   // exponent carried by the tensor product
+  __shared__ float2 s_tw[32][32]; // w1024^(k l) at [k][l]: lane l reads [k][l], no bank conflicts
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int c = warp >> 2, q = warp & 3;
 
   for (int i = tid; i < BB / 16; i += NT) reinterpret_cast<uint4*>(sm)[i] = a.bmat[i];
+  for (int i = tid; i < 32 * 32; i += NT) s_tw[i >> 5][i & 31] = a.tw[((i >> 5) * (i & 31)) & (P - 1)];
   if (warp == 0) tmem_alloc(&tmem_slot, TMEM_COLS);
   if (tid == 0) {
     mbar_init(&mbar, 1);
@@ -211,16 +213,15 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
       int e = 0;
       if (mx > 0.f) frexpf(mx, &e);   // mx < 2^e
+      e = max(e, -127);               // 2^-e stays a finite float (subnormal-only columns)
       if (lane == 0) s_e[c][q] = e;
+      const float sc = ldexpf(1.f, -e);   // v * 2^-e: exact, or rounded as ldexpf rounds
       const int r = 32 * q + lane;
 #pragma unroll
       for (int j = 0; j < K1 / 8; j++) {
         H8 hh, ll;
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
-          split_h(ldexpf(v[4 * j + t].x, -e), hh.h[2 * t], ll.h[2 * t]);
-          split_h(ldexpf(v[4 * j + t].y, -e), hh.h[2 * t + 1], ll.h[2 * t + 1]);
-        }
+        for (int t = 0; t < 4; t++) split_h2(v[4 * j + t].x * sc, v[4 * j + t].y * sc, hh.h2[t], ll.h2[t]);
         const uint32_t o = off_kmajor(r, 8 * j, LBO_K, K1 * 16);
         *reinterpret_cast<uint4*>(Ah + o) = hh.u;
         *reinterpret_cast<uint4*>(Al + o) = ll.u;
@@ -234,12 +235,17 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       acc_ld16(tl, 128 * c + 16 * j, v);
       H8 hr, lr, hi, li;
 #pragma unroll
-      for (int t = 0; t < 8; t++) {
-        const int k1 = 8 * j + t;
-        const float2 w = __ldg(&a.tw[(lane * k1) & (P - 1)]);
-        const float yr = v[2 * t], yi = v[2 * t + 1];
-        split_h((yr * w.x - yi * w.y) * 0.03125f, hr.h[t], lr.h[t]);
-        split_h((yr * w.y + yi * w.x) * 0.03125f, hi.h[t], li.h[t]);
+      for (int t = 0; t < 8; t += 2) {
+        float re[2], im[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const float2 w = s_tw[8 * j + t + u][lane];   // w1024^(n2 k1), n2 = lane
+          const float yr = v[2 * (t + u)], yi = v[2 * (t + u) + 1];
+          re[u] = (yr * w.x - yi * w.y) * 0.03125f;
+          im[u] = (yr * w.y + yi * w.x) * 0.03125f;
+        }
+        split_h2(re[0], re[1], hr.h2[t / 2], lr.h2[t / 2]);
+        split_h2(im[0], im[1], hi.h2[t / 2], li.h2[t / 2]);
       }
       const int m0 = 32 * q + 8 * j;
       const uint32_t ore = off_mnmajor(m0, 2 * lane, LBO_MN, SBO_MN), oim = off_mnmajor(m0, 2 * lane + 1, LBO_MN, SBO_MN);
@@ -256,8 +262,25 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       const float fx = ldexpf(1.f, ex - em), fy = ldexpf(1.f, ey - em);
       const long long tb = (long long)(colok ? kx : 0) * P + lane;
       const int r = 32 * q + lane;
+      const float* tdiag = (c == 0) ? a.txx : ((c == 1) ? a.tyy : a.tzz);
+      // tensor entries of frequency block j (8 frequencies), loaded one block
+      // ahead so their latency overlaps the previous block's arithmetic
+      float tn[8];
+      float2 tq[8];
+      auto load_t = [&](int j, float(&n)[8], float2(&x)[8]) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const long long e = tb + 32LL * (8 * j + i);
+          n[i] = colok ? __ldg(&tdiag[e]) : 0.f;
+          x[i] = (colok && c < 2) ? __ldg(&a.txy[e]) : make_float2(0.f, 0.f);
+        }
+      };
+      load_t(0, tn, tq);
 #pragma unroll 1
       for (int j = 0; j < 4; j++) {
+        float nn[8];
+        float2 nq[8];
+        if (j < 3) load_t(j + 1, nn, nq);
         float X0[16], X1[16];
         if (c < 2) {
           acc_ld16(tl, 16 * j, X0);
@@ -271,35 +294,37 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
 #pragma unroll
           for (int t = 0; t < 4; t++) {
             const int i = 4 * half + t;
-            const long long e = tb + 32LL * (8 * j + i);
             float hr = 0.f, hm = 0.f;
             if (colok) {
+              const float n = tn[i];
+              const float2 nxy = tq[i];
               if (c == 0) {
-                const float n = __ldg(&a.txx[e]);
-                const float2 nxy = __ldg(&a.txy[e]);
                 const float xr = X0[2 * i] * fx, xi = X0[2 * i + 1] * fx;
                 const float yr = X1[2 * i] * fy, yi = X1[2 * i + 1] * fy;
                 hr = n * xr + (nxy.x * yr - nxy.y * yi);
                 hm = n * xi + (nxy.x * yi + nxy.y * yr);
               } else if (c == 1) {
-                const float n = __ldg(&a.tyy[e]);
-                const float2 nxy = __ldg(&a.txy[e]);
                 const float xr = X0[2 * i] * fx, xi = X0[2 * i + 1] * fx;
                 const float yr = X1[2 * i] * fy, yi = X1[2 * i + 1] * fy;
                 hr = (nxy.x * xr - nxy.y * xi) + n * yr;
                 hm = (nxy.x * xi + nxy.y * xr) + n * yi;
               } else {
-                const float n = __ldg(&a.tzz[e]);
                 hr = n * X0[2 * i];
                 hm = n * X0[2 * i + 1];
               }
             }
-            split_h(hr * a.s_t, hh.h[2 * t], ll.h[2 * t]);
-            split_h(-hm * a.s_t, hh.h[2 * t + 1], ll.h[2 * t + 1]);
+            split_h2(hr * a.s_t, -hm * a.s_t, hh.h2[t], ll.h2[t]);
           }
           const uint32_t o = off_kmajor(r, 8 * (2 * j + half), LBO_K, 1024);
           *reinterpret_cast<uint4*>(Ah + o) = hh.u;
           *reinterpret_cast<uint4*>(Al + o) = ll.u;
+        }
+        if (j < 3) {
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            tn[i] = nn[i];
+            tq[i] = nq[i];
+          }
         }
       }
       if (lane == 0) s_eo[c][q] = em;
@@ -312,12 +337,17 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       acc_ld16(tl, 128 * c + 16 * j, v);
       H8 hr, lr, hi, li;
 #pragma unroll
-      for (int t = 0; t < 8; t++) {
-        const int n2 = 8 * j + t;
-        const float2 w = __ldg(&a.tw[(n2 * lane) & (P - 1)]);
-        const float zr = v[2 * t], zi = v[2 * t + 1];
-        split_h((zr * w.x - zi * w.y) * 0.03125f, hr.h[t], lr.h[t]);
-        split_h((zr * w.y + zi * w.x) * 0.03125f, hi.h[t], li.h[t]);
+      for (int t = 0; t < 8; t += 2) {
+        float re[2], im[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const float2 w = s_tw[8 * j + t + u][lane];   // w1024^(n2 k1), k1 = lane
+          const float zr = v[2 * (t + u)], zi = v[2 * (t + u) + 1];
+          re[u] = (zr * w.x - zi * w.y) * 0.03125f;
+          im[u] = (zr * w.y + zi * w.x) * 0.03125f;
+        }
+        split_h2(re[0], re[1], hr.h2[t / 2], lr.h2[t / 2]);
+        split_h2(im[0], im[1], hi.h2[t / 2], li.h2[t / 2]);
       }
       const int m0 = 32 * q + 8 * j;
       const uint32_t ore = off_mnmajor(m0, 2 * lane, LBO_MN, SBO_MN), oim = off_mnmajor(m0, 2 * lane + 1, LBO_MN, SBO_MN);
