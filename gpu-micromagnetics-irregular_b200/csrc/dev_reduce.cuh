@@ -10,6 +10,12 @@
 namespace {
 
 constexpr int RT = 256;         // threads per reduction block
+// Streaming kernels keep UB elements of their grid-stride slice in flight:
+// the loads of UB consecutive slice elements (i, i + stride, ...) are issued
+// before any of them is used or stored, then the elements are finished in
+// slice order, so per-element arithmetic and per-thread summation order are
+// those of the one-element loop.
+constexpr int UB = 4;
 constexpr int RMAXB = 1024;     // max reduction blocks
 
 int red_blocks(long long n) {

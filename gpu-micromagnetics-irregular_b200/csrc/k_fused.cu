@@ -262,17 +262,37 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X,
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
-  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
-    double s = c.c[0] * X.p[0][i];
-    for (int k = 1; k < nv; k++) s = c.c[k] * X.p[k][i] + s;
-    const double wi = w[i];
-    const double d = s / wi;
-    if (del) del[i] = d;
-    const double yc = 1.0 * (ycor_in ? ycor_in[i] : 0.0) + 1.0 * d;
-    ycor[i] = yc;
-    const double p = d * wi, q = yc * wi;
-    acc[0] += p * p;
-    acc[1] += q * q;
+  const long long st = (long long)gridDim.x * RT;
+  for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
+    double s[UB], wv[UB], yv[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const long long i = i0 + u * st;
+      const bool in = i < n;
+      s[u] = in ? c.c[0] * X.p[0][i] : 0.0;
+      wv[u] = in ? w[i] : 1.0;
+      yv[u] = (in && ycor_in) ? ycor_in[i] : 0.0;
+    }
+    for (int k = 1; k < nv; k++) {
+      double xv[UB];
+#pragma unroll
+      for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? X.p[k][i0 + u * st] : 0.0;
+#pragma unroll
+      for (int u = 0; u < UB; u++) s[u] = c.c[k] * xv[u] + s[u];
+    }
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const long long i = i0 + u * st;
+      if (i >= n) continue;
+      const double wi = wv[u];
+      const double d = s[u] / wi;
+      if (del) del[i] = d;
+      const double yc = 1.0 * yv[u] + 1.0 * d;
+      ycor[i] = yc;
+      const double p = d * wi, q = yc * wi;
+      acc[0] += p * p;
+      acc[1] += q * q;
+    }
   }
   block_sum<2>(acc, sm);
   finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);

@@ -48,10 +48,22 @@ __global__ void __launch_bounds__(RT) k_dot_multi(const double* __restrict__ x, 
   double acc[K];
 #pragma unroll
   for (int k = 0; k < K; k++) acc[k] = 0.0;
-  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
-    const double xi = x[i];
+  const long long st = (long long)gridDim.x * RT;
+  for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
+    double xv[UB], yv[UB][K];
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] += xi * Y.p[k][i];
+    for (int u = 0; u < UB; u++) {
+      const long long i = i0 + u * st;
+      xv[u] = (i < n) ? x[i] : 0.0;
+#pragma unroll
+      for (int k = 0; k < K; k++) yv[u][k] = (i < n) ? Y.p[k][i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < UB; u++)
+      if (i0 + u * st < n) {
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[k] += xv[u] * yv[u][k];
+      }
   }
   block_sum<K>(acc, sm);
   finalize<K>(partials, gridDim.x, counter, out, 0, 1.0, acc);
@@ -206,14 +218,26 @@ __global__ void k_scale_cols(int q, CoefPack f, MPtrPack zn, long long n) {
   }
 }
 
+// z = a x over the grid-stride slice, UB elements in flight (x may be z)
+__device__ __forceinline__ void scale_batched(double a, const double* x, double* z, long long n) {
+  const long long st = (long long)gridDim.x * blockDim.x;
+  for (long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += UB * st) {
+    double v[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) v[u] = (i0 + u * st < n) ? x[i0 + u * st] : 0.0;
+#pragma unroll
+    for (int u = 0; u < UB; u++)
+      if (i0 + u * st < n) z[i0 + u * st] = a * v[u];
+  }
+}
+
 // z = x / sqrt(*ss): the first Krylov vector scaled by its norm without a
 // read-back (the host's vscale(1.0 / rnorm) with rnorm = sqrt(ss))
 __global__ void k_scale_rsqrt(const double* __restrict__ ss, const double* __restrict__ x, double* __restrict__ z,
                               long long n) {
   pdl_entry();
   const double a = 1.0 / sqrt(*ss);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    z[i] = a * x[i];
+  scale_batched(a, x, z, n);
 }
 // z = x / sqrt(*ss) unless classical Gram-Schmidt's norm test asks for a
 // second pass (1000 ||x|| < ||x before the update||), in which case x is left
@@ -223,8 +247,7 @@ __global__ void k_scale_gs(const double* __restrict__ vk_dot, const double* __re
   pdl_entry();
   if (1000.0 * sqrt(*ss) < sqrt(*vk_dot)) return;
   const double a = 1.0 / sqrt(*ss);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    z[i] = a * x[i];
+  scale_batched(a, x, z, n);
 }
 // classical Gram-Schmidt update with the dots read on the device:
 // z = 1 z + sum_{i<k} (-dots_i) X_i, and sum z^2 (the arithmetic of
@@ -238,13 +261,26 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
 #pragma unroll
   for (int j = 0; j < MAXV - 1; j++) cf[j] = (j < k) ? -dots[j] : 0.0;
   double acc[1] = {0.0};
-  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
-    double s = 1.0 * z[i];
+  const long long st = (long long)gridDim.x * RT;
+  for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
+    double s[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) s[u] = (i0 + u * st < n) ? 1.0 * z[i0 + u * st] : 0.0;
 #pragma unroll
     for (int j = 0; j < MAXV - 1; j++)
-      if (j < k) s = cf[j] * X.p[j][i] + s;
-    z[i] = s;
-    acc[0] += s * s;
+      if (j < k) {
+        double xv[UB];
+#pragma unroll
+        for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? X.p[j][i0 + u * st] : 0.0;
+#pragma unroll
+        for (int u = 0; u < UB; u++) s[u] = cf[j] * xv[u] + s[u];
+      }
+#pragma unroll
+    for (int u = 0; u < UB; u++)
+      if (i0 + u * st < n) {
+        z[i0 + u * st] = s[u];
+        acc[0] += s[u] * s[u];
+      }
   }
   block_sum<1>(acc, sm);
   finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
