@@ -67,12 +67,12 @@ def algorithmic_bytes(kid, ng, ny, dims, mixed=False):
         return 24 * n + 24 * n + n + 24 * n
     if kid == 1:   # jtv: y, v, mask in; Jv out
         return 24 * n + 24 * n + n + 24 * n
-    if kid == 2:   # arnoldi: V_l, ewt, y, frozen m, frozen h, mask in; V_l+1 out
-        return 5 * 24 * n + n + 24 * n
-    if kid == 3:   # psetup: y, hd, mask in; m, h out
-        return 24 * n + 24 * n + n + 48 * n
-    if kid == 4:   # psolve: m, h, r, mask in; z out
-        return 72 * n + n + 24 * n
+    if kid == 2:   # arnoldi: V_l, ewt, y, stored block inverse (9 doubles), mask in; V_l+1 out
+        return 3 * 24 * n + 72 * n + n + 24 * n
+    if kid == 3:   # psetup: y, hd, mask in; m, h, block inverse out
+        return 24 * n + 24 * n + n + 48 * n + 72 * n
+    if kid == 4:   # psolve: block inverse, r, mask in; z out
+        return 72 * n + 24 * n + n + 24 * n
     if kid == 6:   # rows forward: y in; row spectra out
         return 24 * n + S
     if kid == 7:   # columns: spectra in/out + tensor (xx,yy,zz real, xy complex)

@@ -128,6 +128,12 @@ __device__ __forceinline__ void block_inverse(const DevProblem& P, const double 
   Pi[8] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
 }
 
+// the block inverse of one cell stored by psetup (9 planes of n doubles)
+__device__ __forceinline__ void load_pinv(const double* __restrict__ pinv, int n, int cell, double Pi[9]) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) Pi[k] = pinv[(long long)k * n + cell];
+}
+
 // ── shared-memory tile of NF SoA fields (3 comps each) with 1-cell halo ──
 template <int NF>
 struct Tile {

@@ -17,11 +17,15 @@
 // of 148 SMs.  Compact (EXEC_COMPACT) kernels launch one thread per listed
 // cell and read neighbours through L1.
 //
-// Preconditioner.  psetup stores the frozen cell state (m, h) — 48 B/cell —
-// instead of the 72 B/cell inverse; psolve rebuilds the 3x3 block and its
-// adjugate inverse in registers.  The FP64 work (~200 flop/cell) hides under
-// the memory time, so each psolve moves 96 B/cell instead of 120 B/cell.
+// Preconditioner.  psetup stores the frozen cell state (m, h) and the 3x3
+// block inverse (I - gamma_setup J)^-1 of every cell (9 planes, 72 B/cell),
+// as the reference keeps its P^-1 array.  The Arnoldi operator and psolve
+// read the inverse instead of rebuilding it: rebuilding costs ~230 FP64
+// operations per cell, about half of the Arnoldi operator's arithmetic,
+// which bounds that kernel once its loads are pipelined.
 #include <math.h>
+
+#include <algorithm>
 
 #include "llg_internal.h"
 #include "launch.h"
@@ -166,9 +170,11 @@ __global__ void k_jtv_compact(DevProblem P, const double* __restrict__ v, double
 // psetup: freeze (m, h_total) per cell
 __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const double* __restrict__ y,
                                                          const double* __restrict__ hd, double* __restrict__ pm,
-                                                         double* __restrict__ ph, const DevArgs* da) {
+                                                         double* __restrict__ ph, double* __restrict__ pinv,
+                                                         double gamma, const DevArgs* da) {
   pdl_entry();
   if (da && !da->run_setup) return;
+  if (da) gamma = da->gamma_setup;
   __shared__ Tile<1> T;
   const double* f[1] = {y};
   load_tile<1>(P, T, f);
@@ -186,22 +192,22 @@ __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const dou
     pm[a * n + cell] = m[a];
     ph[a * n + cell] = h[a];
   }
+  const double ws = P.windowed ? P.w[cell] : 1.0;
+  double Pi[9];
+  block_inverse(P, m, h, msk, ws, gamma, Pi);
+#pragma unroll
+  for (int k = 0; k < 9; k++) pinv[(long long)k * n + cell] = Pi[k];
 }
 
-__global__ void k_psolve(DevProblem P, const double* __restrict__ pm, const double* __restrict__ ph,
-                         const double* __restrict__ r, double* __restrict__ z, double gamma, const DevArgs* da) {
+
+__global__ void k_psolve(DevProblem P, const double* __restrict__ pinv, const double* __restrict__ r,
+                         double* __restrict__ z) {
   pdl_entry();
   const int n = P.ncell;
-  if (da) gamma = da->gamma_setup;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
-    const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
     const double rr[3] = {r[k], r[n + k], r[2 * n + k]};
-    double msk[3], nsk[3];
-    cell_axes(P, k, msk, nsk);
-    const double ws = P.windowed ? P.w[k] : 1.0;
     double Pi[9];
-    block_inverse(P, m, h, msk, ws, gamma, Pi);
+    load_pinv(pinv, n, k, Pi);
     double g = 1.0;
     if (!P.windowed && P.act) g = P.act[k] ? 1.0 : 0.0;
     z[k] = g * (Pi[0] * rr[0] + Pi[1] * rr[1] + Pi[2] * rr[2]);
@@ -217,16 +223,14 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
                                                           const double* __restrict__ s,
                                                           double* __restrict__ out, const double* __restrict__ y,
                                                           const double* __restrict__ hd,
-                                                          const double* __restrict__ pm,
-                                                          const double* __restrict__ ph, double gamma,
-                                                          double gamma_p, int scale_out, const DevArgs* da) {
+                                                          const double* __restrict__ pinv, double gamma,
+                                                          int scale_out, const DevArgs* da) {
   pdl_entry();
   __shared__ Tile<2> T;
   if (da) {
     in = da->arn_in;
     out = da->arn_out;
     gamma = da->gamma;
-    gamma_p = da->gamma_setup;
   }
   // stage y and vt = in/s (windowed: w·) with halo
   {
@@ -291,12 +295,8 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
   double u[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) u[a] = 1.0 * vv[a] + (-gamma) * jv[a];
-  // P^-1 from the frozen state
-  const double fm[3] = {pm[cell], pm[n + cell], pm[2 * n + cell]};
-  const double fh[3] = {ph[cell], ph[n + cell], ph[2 * n + cell]};
-  const double ws = P.windowed ? P.w[cell] : 1.0;
   double Pi[9];
-  block_inverse(P, fm, fh, msk, ws, gamma_p, Pi);
+  load_pinv(pinv, n, cell, Pi);
   double gz = 1.0;
   if (!P.windowed && P.act) gz = P.act[cell] ? 1.0 : 0.0;
   const double z0 = gz * (Pi[0] * u[0] + Pi[1] * u[1] + Pi[2] * u[2]);
@@ -311,6 +311,161 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
     out[n + cell] = z1;
     out[2 * n + cell] = z2;
   }
+}
+
+// ── persistent, double-buffered Arnoldi operator (unwindowed problems) ──
+// The same per-cell arithmetic as k_arnoldi_tile.  Each CTA walks tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... and, while it computes one tile,
+// cp.async streams the next tile's inputs into the other shared-memory
+// buffer: the y, in and s stencils (tile + one-cell halo, zero outside a
+// free edge, wrapped on a periodic one) and, when the Jacobian uses the full
+// field, the demag field of the centre cells.  The HBM reads of one tile
+// therefore overlap the FP64 work of the previous one instead of alternating
+// with it.  The gate of a cell is read ahead of the stencil wait, its stored
+// block inverse ahead of the stencil arithmetic.
+constexpr int AP_SLOTS = (TY + 2) * TX + (TY + 2) * 2;   // staged stencil slots per component
+constexpr int AP_PLANE = (TY + 2) * (TX + 2);            // doubles per stencil component
+constexpr int AP_CELLS = TX * TY;
+constexpr int AP_NT = TX * TY;
+__host__ __device__ constexpr int ap_buf_doubles(int jv_full) {
+  return 9 * AP_PLANE + (jv_full ? 3 : 0) * AP_CELLS;
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool ok) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  const int sz = ok ? 8 : 0;   // 0: zero-fill, nothing read
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+__device__ __forceinline__ void ap_slot(int q, int& sx, int& sy) {
+  if (q < (TY + 2) * TX) { sy = q / TX; sx = 1 + (q % TX); }
+  else { const int r2 = q - (TY + 2) * TX; sy = r2 >> 1; sx = (r2 & 1) ? (TX + 1) : 0; }
+}
+
+__global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const double* __restrict__ in,
+                                                           const double* __restrict__ s,
+                                                           double* __restrict__ out, const double* __restrict__ y,
+                                                           const double* __restrict__ hd,
+                                                           const double* __restrict__ pinv, double gamma,
+                                                           int scale_out, const DevArgs* da) {
+  pdl_entry();
+  extern __shared__ __align__(16) double apsm[];
+  if (da) {
+    in = da->arn_in;
+    out = da->arn_out;
+    gamma = da->gamma;
+  }
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int n = P.ncell, ng = P.ng, ny = P.ny;
+  const int gx = (ng + TX - 1) / TX, ntiles = gx * ((ny + TY - 1) / TY);
+  const int bufd = ap_buf_doubles(P.jv_full);
+  typedef double Plane[TY + 2][TX + 2];
+
+  auto issue = [&](int t, double* B) {
+    const int x0 = (t % gx) * TX, y0 = (t / gx) * TY;
+    Plane* Y = reinterpret_cast<Plane*>(B);
+    Plane* V = Y + 3;
+    Plane* S = Y + 6;
+    for (int q = tid; q < AP_SLOTS; q += AP_NT) {
+      int sx, sy;
+      ap_slot(q, sx, sy);
+      int gi = x0 - 1 + sx, gj = y0 - 1 + sy;
+      const bool ok = map_nb(gi, gj, ng, ny, P.bc);
+      const long long cell = ok ? (long long)gj * ng + gi : 0;
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        cp_async8(&Y[a][sy][sx], y + a * (long long)n + cell, ok);
+        cp_async8(&V[a][sy][sx], in + a * (long long)n + cell, ok);
+        cp_async8(&S[a][sy][sx], s + a * (long long)n + cell, ok);
+      }
+    }
+    if (P.jv_full) {
+      double* C = B + 9 * AP_PLANE;
+      const int cx = x0 + tx, cy = y0 + ty;
+      const bool cok = cx < ng && cy < ny;
+      const long long cell = cok ? (long long)cy * ng + cx : 0;
+#pragma unroll
+      for (int a = 0; a < 3; a++) cp_async8(&C[a * AP_CELLS + tid], hd + a * (long long)n + cell, cok);
+    }
+  };
+
+  int t = blockIdx.x, b = 0;
+  if (t < ntiles) issue(t, apsm);
+  cp_async_commit();
+  for (; t < ntiles; t += gridDim.x, b ^= 1) {
+    double* B = apsm + b * bufd;
+    const int tn = t + gridDim.x;
+    if (tn < ntiles) issue(tn, apsm + (b ^ 1) * bufd);
+    cp_async_commit();
+    const int x0 = (t % gx) * TX, y0 = (t / gx) * TY;
+    const int gi = x0 + tx, gj = y0 + ty;
+    const bool cok = gi < ng && gj < ny;
+    const int cell = gj * ng + gi;
+    const double g = (cok && P.act) ? (P.act[cell] ? 1.0 : 0.0) : 1.0;   // gate, loaded while the tile lands
+    cp_async_wait1();
+    __syncthreads();
+    Plane* Y = reinterpret_cast<Plane*>(B);
+    Plane* V = Y + 3;
+    Plane* S = Y + 6;
+    // vt = in / s on every staged slot (0 outside a free edge)
+    for (int q = tid; q < AP_SLOTS; q += AP_NT) {
+      int sx, sy;
+      ap_slot(q, sx, sy);
+      int ii = x0 - 1 + sx, jj = y0 - 1 + sy;
+      const bool ok = map_nb(ii, jj, ng, ny, P.bc);
+#pragma unroll
+      for (int a = 0; a < 3; a++) V[a][sy][sx] = ok ? 1.0 * (V[a][sy][sx] / S[a][sy][sx]) : 0.0;
+    }
+    __syncthreads();
+    if (cok) {
+      double Pi[9];
+      load_pinv(pinv, n, cell, Pi);   // first use after the stencil arithmetic below
+      const double* C = B + 9 * AP_PLANE;
+      const int sx = tx + 1, sy = ty + 1;
+      double m[3], vv[3], ss[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        m[a] = Y[a][sy][sx];
+        vv[a] = V[a][sy][sx];
+        ss[a] = S[a][sy][sx];
+      }
+      double msk[3], nsk[3];
+      cell_axes(P, cell, msk, nsk);
+      double h[3];
+      tile_field(P, Y, sx, sy, m, msk, nsk, h);
+      if (P.jv_full) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) h[a] = h[a] + C[a * AP_CELLS + tid] + P.happ[a];
+      }
+      double K[3][3];
+      aniso_jac(P, m, msk, K);
+      double dh[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        dh_from(P, V[a][sy][sx - 1], V[a][sy][sx + 1], V[a][sy - 1][sx], V[a][sy + 1][sx], a, K, vv, nsk, dh[a]);
+      double jv[3];
+      jv_cell(P, m, vv, h, dh, g, jv);
+      double u[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) u[a] = 1.0 * vv[a] + (-gamma) * jv[a];
+      const double z0 = g * (Pi[0] * u[0] + Pi[1] * u[1] + Pi[2] * u[2]);
+      const double z1 = g * (Pi[3] * u[0] + Pi[4] * u[1] + Pi[5] * u[2]);
+      const double z2 = g * (Pi[6] * u[0] + Pi[7] * u[1] + Pi[8] * u[2]);
+      if (scale_out) {
+        out[cell] = ss[0] * z0;
+        out[n + cell] = ss[1] * z1;
+        out[2 * n + cell] = ss[2] * z2;
+      } else {
+        out[cell] = z0;
+        out[n + cell] = z1;
+        out[2 * n + cell] = z2;
+      }
+    }
+    __syncthreads();   // buffer b is refilled by the next iteration's issue
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");   // (only empty groups remain)
 }
 
 int grid_1d(const llg_ctx* c, long long work, int block) {
@@ -363,7 +518,8 @@ int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y) {
 
 int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da) {
   LLG_COUNT(KID_PSETUP);
-  klaunch(k_psetup_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, y, c->d_hd, c->d_pm, c->d_ph, da);
+  klaunch(k_psetup_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, y, c->d_hd, c->d_pm, c->d_ph, c->d_pinv,
+          gamma, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   c->gamma_setup = gamma;
   c->have_setup = 1;
@@ -372,9 +528,31 @@ int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da) 
 
 int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
+  // (the inverse formed by the last psetup, host- or device-issued, is applied)
   LLG_COUNT(KID_PSOLVE);
-  klaunch(k_psolve, grid_1d(c, c->ncell, 256), 256, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, z, c->gamma_setup, da);
+  klaunch(k_psolve, grid_1d(c, c->ncell, 256), 256, 0, c->stream, c->dp, c->d_pinv, r, z);
   LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+int arnoldi_setup(llg_ctx* c) {
+  const size_t smax = 2 * sizeof(double) * ap_buf_doubles(1);
+  if (cudaFuncSetAttribute((const void*)k_arnoldi_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax) !=
+      cudaSuccess) {
+    llg_set_error("arnoldi operator: shared-memory opt-in failed");
+    return LLG_ERR_CUDA;
+  }
+  const long long ntiles = (long long)((c->p.ng + TX - 1) / TX) * ((c->p.ny + TY - 1) / TY);
+  for (int jf = 0; jf < 2; jf++) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_pipe, AP_NT,
+                                                      2 * sizeof(double) * ap_buf_doubles(jf)) != cudaSuccess ||
+        per_sm < 1) {
+      llg_set_error("arnoldi operator: occupancy query failed");
+      return LLG_ERR_CUDA;
+    }
+    c->arn_grid[jf] = (int)std::min<long long>(ntiles, (long long)per_sm * c->num_sms);
+  }
   return 0;
 }
 
@@ -383,8 +561,14 @@ int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* o
   if (!c->have_setup && !da) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_ARNOLDI);
   ktimer_mark(c, KID_ARNOLDI, true);
-  klaunch(k_arnoldi_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, in, ewt, out, y, c->d_hd, c->d_pm, c->d_ph,
-                                                               gamma, c->gamma_setup, scale_out, da);
+  if (c->dp.windowed) {
+    klaunch(k_arnoldi_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, in, ewt, out, y, c->d_hd, c->d_pinv,
+            gamma, scale_out, da);
+  } else {
+    const int jf = c->dp.jv_full ? 1 : 0;
+    klaunch(k_arnoldi_pipe, c->arn_grid[jf], AP_NT, 2 * sizeof(double) * ap_buf_doubles(jf), c->stream, c->dp, in,
+            ewt, out, y, c->d_hd, c->d_pinv, gamma, scale_out, da);
+  }
   ktimer_mark(c, KID_ARNOLDI, false);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;

@@ -146,7 +146,7 @@ int llg_create(const llg_params* p, llg_ctx** out) {
   const size_t v3 = sizeof(double) * 3 * (size_t)c->ncell;
   auto fail = [&](int r) { llg_destroy(c); return r; };
   if (cudaMalloc(&c->d_hd, v3) != cudaSuccess || cudaMalloc(&c->d_pm, v3) != cudaSuccess ||
-      cudaMalloc(&c->d_ph, v3) != cudaSuccess) {
+      cudaMalloc(&c->d_ph, v3) != cudaSuccess || cudaMalloc(&c->d_pinv, 3 * v3) != cudaSuccess) {
     llg_set_error("cudaMalloc of field buffers failed");
     return fail(LLG_ERR_NOMEM);
   }
@@ -156,6 +156,7 @@ int llg_create(const llg_params* p, llg_ctx** out) {
     if ((rc = demag_create(c))) return fail(rc);
   }
   sync_dp(c);
+  if ((rc = arnoldi_setup(c))) return fail(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) {
     llg_set_error(std::string("llg_create: ") + cudaGetErrorString(cudaGetLastError()));
     return fail(LLG_ERR_CUDA);
@@ -181,6 +182,7 @@ void llg_destroy(llg_ctx* c) {
   cudaFree(c->d_hd);
   cudaFree(c->d_pm);
   cudaFree(c->d_ph);
+  cudaFree(c->d_pinv);
   delete c;
 }
 

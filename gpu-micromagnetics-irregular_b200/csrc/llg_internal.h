@@ -87,6 +87,7 @@ struct llg_ctx {
   cudaStream_t stream = nullptr;
   int device = 0;
   int num_sms = 148;
+  int arn_grid[2] = {0, 0};   // persistent Arnoldi operator: CTAs (without / with the demag field staged)
 
   // geometry
   uint8_t* d_act = nullptr;
@@ -101,6 +102,7 @@ struct llg_ctx {
   double* d_hd = nullptr;    // demag field of the last RHS (3N)
   double* d_pm = nullptr;    // m at the last psetup (3N)
   double* d_ph = nullptr;    // h at the last psetup (3N)
+  double* d_pinv = nullptr;  // (I - gamma_setup J)^-1 per cell at the last psetup, 9 planes (9N)
   double gamma_setup = 0.0;
   int have_setup = 0;
 
@@ -141,6 +143,7 @@ int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da = nu
 // (scale_out 0: out = P^-1 (...) without the s1 factor)
 // (da non-null: in, out, gamma and the setup gamma come from the device-resident
 // integrator's DevArgs at run time; the pointer arguments are ignored)
+int arnoldi_setup(llg_ctx* c);   // shared-memory opt-in and grid of the persistent Arnoldi operator
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out,
                       const double* y, double gamma, int scale_out = 1, const DevArgs* da = nullptr);
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot);
