@@ -71,8 +71,8 @@ def algorithmic_bytes(kid, ng, ny, dims, mixed=False):
         return 3 * 24 * n + 72 * n + n + 24 * n
     if kid == 3:   # psetup: y, hd, mask in; m, h, block inverse out
         return 24 * n + 24 * n + n + 48 * n + 72 * n
-    if kid == 4:   # psolve: block inverse, r, mask in; z out
-        return 72 * n + 24 * n + n + 24 * n
+    if kid == 4:   # psolve: frozen m, h, r, mask in; z out
+        return 72 * n + n + 24 * n
     if kid == 6:   # rows forward: y in; row spectra out
         return 24 * n + S
     if kid == 7:   # columns: spectra in/out + tensor (xx,yy,zz real, xy complex)

@@ -166,18 +166,28 @@ __global__ void k_rhs_resid_compact(DevProblem P, const double* __restrict__ y, 
   }
 }
 
-__global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const double* __restrict__ pinv,
+// (streams at HBM speed, so it rebuilds the block from the frozen (m, h),
+// 48 B/cell, rather than reading the 72 B/cell inverse that psetup stores)
+__global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const double* __restrict__ pm,
+                                                         const double* __restrict__ ph,
                                                          const double* __restrict__ r,
                                                          const double* __restrict__ ewt, double* __restrict__ v0,
-                                                         double* partials, unsigned int* counter, double* out) {
+                                                         double gamma, double* partials, unsigned int* counter,
+                                                         double* out, const DevArgs* da) {
   pdl_entry();
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
   const int n = P.ncell;
+  if (da) gamma = da->gamma_setup;
   for (int k = blockIdx.x * RT + threadIdx.x; k < n; k += gridDim.x * RT) {
+    const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
+    const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
     const double rr[3] = {r[k], r[n + k], r[2 * n + k]};
+    double msk[3], nsk[3];
+    cell_axes(P, k, msk, nsk);
+    const double ws = P.windowed ? P.w[k] : 1.0;
     double Pi[9];
-    load_pinv(pinv, n, k, Pi);
+    block_inverse(P, m, h, msk, ws, gamma, Pi);
     double g = 1.0;
     if (!P.windowed && P.act) g = P.act[k] ? 1.0 : 0.0;
     const double z0 = g * (Pi[0] * rr[0] + Pi[1] * rr[1] + Pi[2] * rr[2]);
@@ -477,9 +487,8 @@ int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* yc
 int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot, const DevArgs* da) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
-  (void)da;   // the inverse formed by the last psetup (host- or device-issued) is applied
-  klaunch(k_psolve_scale_dot, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pinv, r, ewt, v0, c->d_red,
-          c->d_counter, c->d_scal + slot);
+  klaunch(k_psolve_scale_dot, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, ewt, v0,
+          c->gamma_setup, c->d_red, c->d_counter, c->d_scal + slot, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

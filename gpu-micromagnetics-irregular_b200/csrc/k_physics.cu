@@ -19,10 +19,12 @@
 //
 // Preconditioner.  psetup stores the frozen cell state (m, h) and the 3x3
 // block inverse (I - gamma_setup J)^-1 of every cell (9 planes, 72 B/cell),
-// as the reference keeps its P^-1 array.  The Arnoldi operator and psolve
-// read the inverse instead of rebuilding it: rebuilding costs ~230 FP64
-// operations per cell, about half of the Arnoldi operator's arithmetic,
-// which bounds that kernel once its loads are pipelined.
+// as the reference keeps its P^-1 array.  The Arnoldi operator reads the
+// inverse: rebuilding it costs ~230 FP64 operations per cell, about half of
+// that kernel's arithmetic, which bounds it once its loads are pipelined.
+// psolve, a plain stream at HBM speed, rebuilds the block from (m, h) in
+// registers instead (48 B/cell read rather than 72); both forms give the same
+// bits (the same block_inverse on the same inputs).
 #include <math.h>
 
 #include <algorithm>
@@ -200,14 +202,20 @@ __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const dou
 }
 
 
-__global__ void k_psolve(DevProblem P, const double* __restrict__ pinv, const double* __restrict__ r,
-                         double* __restrict__ z) {
+__global__ void k_psolve(DevProblem P, const double* __restrict__ pm, const double* __restrict__ ph,
+                         const double* __restrict__ r, double* __restrict__ z, double gamma, const DevArgs* da) {
   pdl_entry();
   const int n = P.ncell;
+  if (da) gamma = da->gamma_setup;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
+    const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
     const double rr[3] = {r[k], r[n + k], r[2 * n + k]};
+    double msk[3], nsk[3];
+    cell_axes(P, k, msk, nsk);
+    const double ws = P.windowed ? P.w[k] : 1.0;
     double Pi[9];
-    load_pinv(pinv, n, k, Pi);
+    block_inverse(P, m, h, msk, ws, gamma, Pi);
     double g = 1.0;
     if (!P.windowed && P.act) g = P.act[k] ? 1.0 : 0.0;
     z[k] = g * (Pi[0] * rr[0] + Pi[1] * rr[1] + Pi[2] * rr[2]);
@@ -528,9 +536,8 @@ int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da) 
 
 int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
-  // (the inverse formed by the last psetup, host- or device-issued, is applied)
   LLG_COUNT(KID_PSOLVE);
-  klaunch(k_psolve, grid_1d(c, c->ncell, 256), 256, 0, c->stream, c->dp, c->d_pinv, r, z);
+  klaunch(k_psolve, grid_1d(c, c->ncell, 256), 256, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, z, c->gamma_setup, da);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
