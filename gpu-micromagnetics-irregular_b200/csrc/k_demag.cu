@@ -193,20 +193,40 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
   const int n = pl.n;
   const int b = threadIdx.y;
   const bool even = (n % 2) == 0;
-  const int ya = y0 + 2 * b, yb = ya + 1;
   const int np = padded_len<R>(n);
-  C* buf = sm + b * np;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const int kk = (k < Hx) ? k : n - k;
-    C A = mk<R>(R(0), R(0)), B = mk<R>(R(0), R(0));
-    const C* col = S + ((long long)c * Hx + kk) * ld;
-    if (ya < nrows) A = col[ya];
-    if (yb < nrows) B = col[yb];
-    if (kk == 0 || (even && kk == n / 2)) { A.y = R(0); B.y = R(0); }
-    if (k >= Hx) { A.y = -A.y; B.y = -B.y; }
-    buf[fpad<R, true>(k)] = mk<R>(A.x - B.y, A.y + B.x);
+  // Load the CTA's 2*NB rows of every spectrum column once, with lanes laid
+  // out (column, row): the rows of one column are adjacent in memory, so a
+  // warp load covers whole sectors.  The pair partner (row 2p+1 of pair p)
+  // comes from the next lane; the even lane forms entry kk of pair p's
+  // packed transform and, for kk in [1, n - Hx], the mirrored entry n - kk
+  // (conjugated spectrum), exactly as entry k would be formed from kk = n - k.
+  {
+    constexpr int RW = 2 * NB;   // rows per column in this CTA (divides 32)
+    const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int total = Hx * RW;
+    for (int base = 0; base < total; base += T) {
+      const int e = base + tid;
+      const int kk = e / RW, r = e - kk * RW, y = y0 + r;
+      C v = mk<R>(R(0), R(0));
+      if (e < total && y < nrows) v = S[((long long)c * Hx + kk) * ld + y];
+      C w;
+      w.x = __shfl_down_sync(0xffffffffu, v.x, 1);
+      w.y = __shfl_down_sync(0xffffffffu, v.y, 1);
+      if (e < total && (r & 1) == 0) {
+        C* bp = sm + (r >> 1) * np;
+        C A = v, B = w;
+        if (kk == 0 || (even && kk == n / 2)) { A.y = R(0); B.y = R(0); }
+        bp[fpad<R, true>(kk)] = mk<R>(A.x - B.y, A.y + B.x);
+        if (kk >= 1 && kk <= n - Hx) {
+          A.y = -A.y;
+          B.y = -B.y;
+          bp[fpad<R, true>(n - kk)] = mk<R>(A.x - B.y, A.y + B.x);
+        }
+      }
+    }
   }
   __syncthreads();
+  C* buf = sm + b * np;
   fft_stockham<R, +1, EPT, true>(buf, pl);
   double* dst = h + (long long)c * comp_stride;
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
