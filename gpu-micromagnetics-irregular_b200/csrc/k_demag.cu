@@ -96,7 +96,7 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
     const int y = y0 + r;
     if (y >= nrows) continue;
     const cx_t<R> zk = sm[bb * np + fpad<R, true>(kx)];
-    const cx_t<R> zm = sm[bb * np + fpad<R, true>((n - kx) % n)];
+    const cx_t<R> zm = sm[bb * np + fpad<R, true>(kx == 0 ? 0 : n - kx)];   // (n - kx) mod n
     cx_t<R> out;
     if (!which) out = mk<R>(R(0.5) * (zk.x + zm.x), R(0.5) * (zk.y - zm.y));
     else out = mk<R>(R(0.5) * (zk.y + zm.y), R(-0.5) * (zk.x - zm.x));
@@ -230,12 +230,14 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
   fft_stockham<R, +1, EPT, true>(buf, pl);
   double* dst = h + (long long)c * comp_stride;
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
-  for (int e = tid; e < NB * 2 * ng; e += T) {
-    const int r = e / ng, i = e - r * ng;
+#pragma unroll
+  for (int r = 0; r < NB * 2; r++) {
     const int y = y0 + r;
-    if (y >= nrows) continue;
-    const C z = sm[(r >> 1) * np + fpad<R, true>(i)];
-    dst[(long long)y * ng + i] = (double)((r & 1) ? z.y : z.x);
+    if (y >= nrows) break;
+    for (int i = tid; i < ng; i += T) {
+      const C z = sm[(r >> 1) * np + fpad<R, true>(i)];
+      dst[(long long)y * ng + i] = (double)((r & 1) ? z.y : z.x);
+    }
   }
 }
 
