@@ -248,7 +248,7 @@ def timed_run(args, form, world, rank, local, lib, clocks=True):
     # (an event pair around every TIMER_STRIDE-th of their launches inside the
     # timed region)
     timed_mask = sum(1 << k for k in TIMED_FAMILIES)
-    llg._check(lib.llg_kernel_timer_start(ctx.h, timed_mask, 200000, TIMER_STRIDE), "llg_kernel_timer_start")
+    llg._check(lib.llg_kernel_timer_start(ctx.h, timed_mask, 20000, TIMER_STRIDE), "llg_kernel_timer_start")
     torch.cuda.synchronize()
     dist_barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
