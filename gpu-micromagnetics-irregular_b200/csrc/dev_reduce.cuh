@@ -57,8 +57,9 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* sm /* [K][RT/3
 }
 
 // Last-block finalisation: partials[k*nb + b]; out[k] = sum_b partials (fixed tree).
+// Returns true in the last block (where thread 0 wrote out).
 template <int K>
-__device__ __forceinline__ void finalize(double* partials, int nb, unsigned int* counter, double* out,
+__device__ __forceinline__ bool finalize(double* partials, int nb, unsigned int* counter, double* out,
                                          int mode /*0 sum, 1 wrms with n, 2 max*/, double nrm,
                                          const double (&mine)[K]) {
   __shared__ bool last;
@@ -71,7 +72,7 @@ __device__ __forceinline__ void finalize(double* partials, int nb, unsigned int*
     last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (!last) return;
+  if (!last) return false;
   __threadfence();
   double v[K];
 #pragma unroll
@@ -106,6 +107,7 @@ __device__ __forceinline__ void finalize(double* partials, int nb, unsigned int*
     for (int k = 0; k < K; k++) out[k] = (mode == 1) ? sqrt(v[k] / nrm) : v[k];
     *counter = 0u;
   }
+  return true;
 }
 
 

@@ -272,22 +272,38 @@ struct Integrator {
   // decisions as spgmr() below.
   static int slot_it(int l) { return 64 + 24 * l; }       // dots of iteration l (l + 2 values)
   static int slot_ss(int l) { return 64 + 24 * l + 20; }  // sum of squares after its update
+  static int slot_sc(int l) { return 64 + 24 * l + 21; }  // scale of the vector it produces
+  static constexpr int SLOT_V0SC = 62;                    // scale of V0
+  // The basis vectors stay unnormalised in memory; every kernel that reads
+  // V[i] reads it as a_i V[i] (KScale, llg_internal.h).  a_0 = 1/||V0|| is
+  // written by the kernel that forms ||V0||, a_k = 1/||V[k]|| (1 when a second
+  // Gram-Schmidt pass is due; the host then normalises V[k] itself) by the
+  // Gram-Schmidt update that forms ||V[k]||.  This replaces a normalising pass
+  // over each vector with a multiply where it is read; the values used are
+  // the ones that pass would have stored.
+  const double* ka[MAXLL + 1] = {};
+  KScale basis_scales(int k0, int k1, int at) const {   // entries at.. for V[k0..k1)
+    KScale s{};
+    for (int i = k0; i < k1; i++) s.a[at + i - k0] = ka[i];
+    return s;
+  }
   void enqueue_iter(int l) {
     const int k = l + 1;
-    ok(launch_arnoldi_op(c, V[l], ewt, V[k], y, gamma));
+    ok(launch_arnoldi_op(c, V[l], ewt, V[k], y, gamma, 1, nullptr, ka[l]));
     const double* Y[MAXLL + 1];
     for (int i = 0; i <= k; i++) Y[i] = V[i];
-    ok(vdot_multi_dev(c, k + 1, V[k], Y, slot_it(l)));
-    ok(vgs_update_dev(c, k, V, slot_it(l), slot_ss(l)));
-    ok(vscale_gs(c, slot_it(l) + k, slot_ss(l), V[k]));
+    const KScale ys = basis_scales(0, k, 0);   // V[k] itself: the fresh operator output, unscaled
+    ok(vdot_multi_dev(c, k + 1, V[k], Y, slot_it(l), &ys));
+    ok(vgs_update_dev(c, k, V, slot_it(l), slot_ss(l), &ys, slot_sc(l)));
+    ka[k] = c->d_scal + slot_sc(l);
   }
   int spgmr_spec(double* rhs, double delta_tol, bool harvest, double* zb) {
     const int lmax = maxl;
     int nl = 0, krydim = 0, converged = 0;
     nps++;
     if (harvest) ok(launch_psolve(c, rhs, zb));   // u = P_BJ^-1 r, kept with the solution
-    if (!ok(fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A))) return LS_CONV_FAIL;
-    ok(vscale_rsqrt(c, SLOT_A, V[0]));
+    if (!ok(fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A, nullptr, SLOT_V0SC))) return LS_CONV_FAIL;
+    ka[0] = c->d_scal + SLOT_V0SC;
     int queued = (lmax >= 2) ? 2 : 1;
     for (int l = 0; l < queued; l++) enqueue_iter(l);
     ok(fetch_range(c, 0, slot_ss(queued - 1) + 1));
@@ -318,19 +334,20 @@ struct Integrator {
       double nrm = sqrt(hsc[slot_ss(l)]);
       bool second = false;
       if (GS_FACTOR * nrm < vk_norm) {
-        // second pass; the device left V[k] unscaled, so later queued
-        // iterations are void and are enqueued again
+        // second pass; V[k]'s scale is 1 (the device made the same test),
+        // so later queued iterations are void and are enqueued again
         second = true;
         queued = k;
         const double* Y[MAXLL + 1];
         for (int i = 0; i < k; i++) Y[i] = V[i];
         double dots[MAXLL + 1], cf[MAXLL + 1], ss = 0.0;
         const double* X[MAXLL + 1];
-        if (ok(vdot_multi_dev(c, k, V[k], Y, SLOT_DOTS))) ok(fetch_scalars(c, SLOT_DOTS, k, dots));
+        const KScale ys = basis_scales(0, k, 0), xs = basis_scales(0, k, 1);
+        if (ok(vdot_multi_dev(c, k, V[k], Y, SLOT_DOTS, &ys))) ok(fetch_scalars(c, SLOT_DOTS, k, dots));
         cf[0] = 1.0;
         X[0] = V[k];
         for (int i = 0; i < k; i++) { Hes[i][l] += dots[i]; cf[i + 1] = -dots[i]; X[i + 1] = V[i]; }
-        if (ok(fused_lincomb_norm(c, k + 1, cf, X, V[k], SLOT_DOTS))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
+        if (ok(fused_lincomb_norm(c, k + 1, cf, X, V[k], SLOT_DOTS, &xs))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
         nrm = sqrt(ss);
       }
       Hes[k][l] = nrm;
@@ -347,13 +364,14 @@ struct Integrator {
     if (converged || rho < beta) {
       const double* X[MAXLL + 1];
       for (int k = 0; k < krydim; k++) X[k] = V[k];
+      const KScale xs = basis_scales(0, krydim, 0);
       const bool taken = converged || ls_curiter == 0;
       if (taken && fuse_update) {
-        ok(fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A));
+        ok(fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A, &xs));
         ok(fetch_scalars(c, SLOT_A, 2, upd_s));
         update_done = true;
       } else {
-        ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs));
+        ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs, &xs));
       }
       if (converged && harvest) ok(learned_harvest(c, zb, rhs, ewt, c->gamma_setup));
       return converged ? LS_SUCCESS : LS_RES_REDUCED;

@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
                                                          const double* __restrict__ r,
                                                          const double* __restrict__ ewt, double* __restrict__ v0,
                                                          double gamma, double* partials, unsigned int* counter,
-                                                         double* out, const DevArgs* da) {
+                                                         double* out, const DevArgs* da, double* aout) {
   pdl_entry();
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
@@ -200,18 +200,20 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
     acc[0] += a2 * a2;
   }
   block_sum<1>(acc, sm);
-  finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  const bool last = finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  if (last && aout && threadIdx.x == 0) *aout = gs_scale_of(out[0], nullptr);   // 1 / ||V0||
 }
 
 // z = c0 X0; z = c_k X_k + z (z may alias X0), and sum z^2
 __global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, double* z, long long n,
-                                                     double* partials, unsigned int* counter, double* out) {
+                                                     double* partials, unsigned int* counter, double* out,
+                                                     KScale ks) {
   pdl_entry();
   __shared__ double sm[RT / 32];
   double acc[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
-    double s = c.c[0] * X.p[0][i];
-    for (int k = 1; k < nv; k++) s = c.c[k] * X.p[k][i] + s;
+    double s = c.c[0] * (kscale_of(ks.a[0]) * X.p[0][i]);
+    for (int k = 1; k < nv; k++) s = c.c[k] * (kscale_of(ks.a[k]) * X.p[k][i]) + s;
     z[i] = s;
     acc[0] += s * s;
   }
@@ -220,11 +222,11 @@ __global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, d
 }
 
 __global__ void k_lincomb_div(int nv, CPack c, XPack X, const double* __restrict__ w, double* __restrict__ z,
-                              long long n) {
+                              long long n, KScale ks) {
   pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    double s = c.c[0] * X.p[0][i];
-    for (int k = 1; k < nv; k++) s = c.c[k] * X.p[k][i] + s;
+    double s = c.c[0] * (kscale_of(ks.a[0]) * X.p[0][i]);
+    for (int k = 1; k < nv; k++) s = c.c[k] * (kscale_of(ks.a[k]) * X.p[k][i]) + s;
     z[i] = s / w[i];
   }
 }
@@ -260,9 +262,11 @@ __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, doub
 // reduction partition
 __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X, const double* __restrict__ w,
                                                        double* del, const double* ycor_in, double* ycor, long long n,
-                                                       double* partials, unsigned int* counter, double* out) {
+                                                       double* partials, unsigned int* counter, double* out,
+                                                       KScale ks) {
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
+  const double xa0 = kscale_of(ks.a[0]);   // scales of the X vectors (1 when stored normalised)
   double acc[2] = {0.0, 0.0};
   const long long st = (long long)gridDim.x * RT;
   for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
@@ -271,14 +275,15 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X,
     for (int u = 0; u < UB; u++) {
       const long long i = i0 + u * st;
       const bool in = i < n;
-      s[u] = in ? c.c[0] * X.p[0][i] : 0.0;
+      s[u] = in ? c.c[0] * (xa0 * X.p[0][i]) : 0.0;
       wv[u] = in ? w[i] : 1.0;
       yv[u] = (in && ycor_in) ? ycor_in[i] : 0.0;
     }
     for (int k = 1; k < nv; k++) {
+      const double xa = kscale_of(ks.a[k]);
       double xv[UB];
 #pragma unroll
-      for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? X.p[k][i0 + u * st] : 0.0;
+      for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * X.p[k][i0 + u * st] : 0.0;
 #pragma unroll
       for (int u = 0; u < UB; u++) s[u] = c.c[k] * xv[u] + s[u];
     }
@@ -484,34 +489,40 @@ int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* yc
   return 0;
 }
 
-int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot, const DevArgs* da) {
+int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot, const DevArgs* da,
+                           int slot_aout) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
   klaunch(k_psolve_scale_dot, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, ewt, v0,
-          c->gamma_setup, c->d_red, c->d_counter, c->d_scal + slot, da);
+          c->gamma_setup, c->d_red, c->d_counter, c->d_scal + slot, da,
+          slot_aout >= 0 ? c->d_scal + slot_aout : nullptr);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
-int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot) {
+int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot,
+                       const KScale* ks) {
   if (nv < 1 || nv > FV) { llg_set_error("lincomb_norm: bad nvec"); return LLG_ERR_ARG; }
   CPack cp{};
   XPack xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
+  const KScale kz{};
   LLG_COUNT(KID_REDUCE);
   klaunch(k_lincomb_norm, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, z, c->neq, c->d_red, c->d_counter,
-                                                           c->d_scal + slot);
+          c->d_scal + slot, ks ? *ks : kz);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
-int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z) {
+int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z,
+                      const KScale* ks) {
   if (nv < 1 || nv > FV) { llg_set_error("lincomb_div: bad nvec"); return LLG_ERR_ARG; }
   CPack cp{};
   XPack xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
+  const KScale kz{};
   LLG_COUNT(KID_ELEMWISE);
-  klaunch(k_lincomb_div, ew_blocks(c, c->neq), 256, 0, c->stream, nv, cp, xp, w, z, c->neq);
+  klaunch(k_lincomb_div, ew_blocks(c, c->neq), 256, 0, c->stream, nv, cp, xp, w, z, c->neq, ks ? *ks : kz);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -535,14 +546,15 @@ int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double
 }
 
 int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
-                         double* del, bool ycor_zero, double* ycor, int slot) {
+                         double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks) {
   if (nv < 1 || nv > FV) { llg_set_error("lincomb_update: bad nvec"); return LLG_ERR_ARG; }
   CPack cp{};
   XPack xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
+  const KScale kz{};
   LLG_COUNT(KID_REDUCE);
   klaunch(k_lincomb_update, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, w, del, ycor_zero ? nullptr : ycor, ycor,
-                                                             c->neq, c->d_red, c->d_counter, c->d_scal + slot);
+          c->neq, c->d_red, c->d_counter, c->d_scal + slot, ks ? *ks : kz);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
                                                           double* __restrict__ out, const double* __restrict__ y,
                                                           const double* __restrict__ hd,
                                                           const double* __restrict__ pinv, double gamma,
-                                                          int scale_out, const DevArgs* da) {
+                                                          int scale_out, const DevArgs* da, const double* in_a) {
   pdl_entry();
   __shared__ Tile<2> T;
   if (da) {
@@ -240,6 +240,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
     out = da->arn_out;
     gamma = da->gamma;
   }
+  const double ain = kscale_of(in_a);   // the input is read as ain * in
   // stage y and vt = in/s (windowed: w·) with halo
   {
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
 #pragma unroll
       for (int a = 0; a < 3; a++) {
         T.v[0][a][sy][sx] = ok ? ww * y[a * n + cell] : 0.0;
-        T.v[1][a][sy][sx] = ok ? ww * (in[a * n + cell] / s[a * n + cell]) : 0.0;
+        T.v[1][a][sy][sx] = ok ? ww * ((ain * in[a * n + cell]) / s[a * n + cell]) : 0.0;
       }
     }
     __syncthreads();
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       m[a] = y[a * n + cell];
-      vv[a] = in[a * n + cell] / ss[a];
+      vv[a] = (ain * in[a * n + cell]) / ss[a];
     }
   }
   double msk[3], nsk[3];
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
                                                            double* __restrict__ out, const double* __restrict__ y,
                                                            const double* __restrict__ hd,
                                                            const double* __restrict__ pinv, double gamma,
-                                                           int scale_out, const DevArgs* da) {
+                                                           int scale_out, const DevArgs* da, const double* in_a) {
   pdl_entry();
   extern __shared__ __align__(16) double apsm[];
   if (da) {
@@ -365,6 +366,7 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
     out = da->arn_out;
     gamma = da->gamma;
   }
+  const double ain = kscale_of(in_a);   // the input is read as ain * in
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int n = P.ncell, ng = P.ng, ny = P.ny;
   const int gx = (ng + TX - 1) / TX, ntiles = gx * ((ny + TY - 1) / TY);
@@ -417,14 +419,14 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
     Plane* Y = reinterpret_cast<Plane*>(B);
     Plane* V = Y + 3;
     Plane* S = Y + 6;
-    // vt = in / s on every staged slot (0 outside a free edge)
+    // vt = (ain in) / s on every staged slot (0 outside a free edge)
     for (int q = tid; q < AP_SLOTS; q += AP_NT) {
       int sx, sy;
       ap_slot(q, sx, sy);
       int ii = x0 - 1 + sx, jj = y0 - 1 + sy;
       const bool ok = map_nb(ii, jj, ng, ny, P.bc);
 #pragma unroll
-      for (int a = 0; a < 3; a++) V[a][sy][sx] = ok ? 1.0 * (V[a][sy][sx] / S[a][sy][sx]) : 0.0;
+      for (int a = 0; a < 3; a++) V[a][sy][sx] = ok ? 1.0 * ((ain * V[a][sy][sx]) / S[a][sy][sx]) : 0.0;
     }
     __syncthreads();
     if (cok) {
@@ -564,17 +566,17 @@ int arnoldi_setup(llg_ctx* c) {
 }
 
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out, const double* y,
-                      double gamma, int scale_out, const DevArgs* da) {
+                      double gamma, int scale_out, const DevArgs* da, const double* in_a) {
   if (!c->have_setup && !da) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_ARNOLDI);
   ktimer_mark(c, KID_ARNOLDI, true);
   if (c->dp.windowed) {
     klaunch(k_arnoldi_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, in, ewt, out, y, c->d_hd, c->d_pinv,
-            gamma, scale_out, da);
+            gamma, scale_out, da, in_a);
   } else {
     const int jf = c->dp.jv_full ? 1 : 0;
     klaunch(k_arnoldi_pipe, c->arn_grid[jf], AP_NT, 2 * sizeof(double) * ap_buf_doubles(jf), c->stream, c->dp, in,
-            ewt, out, y, c->d_hd, c->d_pinv, gamma, scale_out, da);
+            ewt, out, y, c->d_hd, c->d_pinv, gamma, scale_out, da, in_a);
   }
   ktimer_mark(c, KID_ARNOLDI, false);
   LLG_CUDA_TRY(cudaPeekAtLastError());

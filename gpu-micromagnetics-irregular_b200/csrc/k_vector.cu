@@ -42,9 +42,13 @@ struct CoefPack {
 
 template <int K>
 __global__ void __launch_bounds__(RT) k_dot_multi(const double* __restrict__ x, PtrPack Y, long long n,
-                                                  double* partials, unsigned int* counter, double* out) {
+                                                  double* partials, unsigned int* counter, double* out,
+                                                  KScale ks) {
   pdl_entry();
   __shared__ double sm[K * (RT / 32)];
+  double ya[K];   // scales of the Y vectors (1 when stored normalised)
+#pragma unroll
+  for (int k = 0; k < K; k++) ya[k] = kscale_of(ks.a[k]);
   double acc[K];
 #pragma unroll
   for (int k = 0; k < K; k++) acc[k] = 0.0;
@@ -56,7 +60,7 @@ __global__ void __launch_bounds__(RT) k_dot_multi(const double* __restrict__ x, 
       const long long i = i0 + u * st;
       xv[u] = (i < n) ? x[i] : 0.0;
 #pragma unroll
-      for (int k = 0; k < K; k++) yv[u][k] = (i < n) ? Y.p[k][i] : 0.0;
+      for (int k = 0; k < K; k++) yv[u][k] = (i < n) ? ya[k] * Y.p[k][i] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < UB; u++)
@@ -218,45 +222,15 @@ __global__ void k_scale_cols(int q, CoefPack f, MPtrPack zn, long long n) {
   }
 }
 
-// z = a x over the grid-stride slice, UB elements in flight (x may be z)
-__device__ __forceinline__ void scale_batched(double a, const double* x, double* z, long long n) {
-  const long long st = (long long)gridDim.x * blockDim.x;
-  for (long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; i0 < n; i0 += UB * st) {
-    double v[UB];
-#pragma unroll
-    for (int u = 0; u < UB; u++) v[u] = (i0 + u * st < n) ? x[i0 + u * st] : 0.0;
-#pragma unroll
-    for (int u = 0; u < UB; u++)
-      if (i0 + u * st < n) z[i0 + u * st] = a * v[u];
-  }
-}
-
-// z = x / sqrt(*ss): the first Krylov vector scaled by its norm without a
-// read-back (the host's vscale(1.0 / rnorm) with rnorm = sqrt(ss))
-__global__ void k_scale_rsqrt(const double* __restrict__ ss, const double* __restrict__ x, double* __restrict__ z,
-                              long long n) {
-  pdl_entry();
-  const double a = 1.0 / sqrt(*ss);
-  scale_batched(a, x, z, n);
-}
-// z = x / sqrt(*ss) unless classical Gram-Schmidt's norm test asks for a
-// second pass (1000 ||x|| < ||x before the update||), in which case x is left
-// as it is for the host to finish
-__global__ void k_scale_gs(const double* __restrict__ vk_dot, const double* __restrict__ ss,
-                           const double* __restrict__ x, double* __restrict__ z, long long n) {
-  pdl_entry();
-  if (1000.0 * sqrt(*ss) < sqrt(*vk_dot)) return;
-  const double a = 1.0 / sqrt(*ss);
-  scale_batched(a, x, z, n);
-}
 // classical Gram-Schmidt update with the dots read on the device:
 // z = 1 z + sum_{i<k} (-dots_i) X_i, and sum z^2 (the arithmetic of
 // k_lincomb_norm with coefficients {1, -dots_0, ..., -dots_{k-1}})
 __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double* __restrict__ dots, double* z,
                                                   long long n, double* partials, unsigned int* counter,
-                                                  double* out) {
+                                                  double* out, KScale ks, double* aout) {
   pdl_entry();
   __shared__ double sm[RT / 32];
+
   double cf[MAXV - 1];
 #pragma unroll
   for (int j = 0; j < MAXV - 1; j++) cf[j] = (j < k) ? -dots[j] : 0.0;
@@ -271,7 +245,9 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
       if (j < k) {
         double xv[UB];
 #pragma unroll
-        for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? X.p[j][i0 + u * st] : 0.0;
+        const double xa = kscale_of(ks.a[j]);   // the scale of X_j (1 when stored normalised)
+#pragma unroll
+        for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * X.p[j][i0 + u * st] : 0.0;
 #pragma unroll
         for (int u = 0; u < UB; u++) s[u] = cf[j] * xv[u] + s[u];
       }
@@ -283,7 +259,9 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
       }
   }
   block_sum<1>(acc, sm);
-  finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  const bool last = finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  // the updated vector's scale; dots[k] is its sum of squares before the update
+  if (last && aout && threadIdx.x == 0) *aout = gs_scale_of(out[0], dots + k);
 }
 
 // one warp copies d_scal[lo, hi) into the mapped host mailbox, makes the
@@ -338,7 +316,9 @@ void reductions_free(llg_ctx* c) {
   c->h_mail = c->d_mail = nullptr;
 }
 
-int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot) {
+int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot, const KScale* ks) {
+  const KScale kz{};
+  const KScale& kk = ks ? *ks : kz;
   if (nvec <= 0) return 0;
   if (nvec > 16) { llg_set_error("dot_multi: nvec > 16"); return LLG_ERR_ARG; }
   PtrPack pk{};
@@ -348,7 +328,7 @@ int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y
   double* out = c->d_scal + slot;
   switch (nvec) {
 #define DOTK(K) \
-  case K: LLG_COUNT(KID_REDUCE); klaunch(k_dot_multi<K>, nb, RT, 0, c->stream, x, pk, n, c->d_red, c->d_counter, out); break;
+  case K: LLG_COUNT(KID_REDUCE); klaunch(k_dot_multi<K>, nb, RT, 0, c->stream, x, pk, n, c->d_red, c->d_counter, out, kk); break;
     DOTK(1) DOTK(2) DOTK(3) DOTK(4) DOTK(5) DOTK(6) DOTK(7) DOTK(8)
     DOTK(9) DOTK(10) DOTK(11) DOTK(12) DOTK(13) DOTK(14) DOTK(15) DOTK(16)
 #undef DOTK
@@ -404,27 +384,15 @@ int fetch_range(llg_ctx* c, int lo, int hi) {
   return 0;
 }
 
-int vscale_rsqrt(llg_ctx* c, int slot_ss, double* x) {
-  LLG_COUNT(KID_ELEMWISE);
-  klaunch(k_scale_rsqrt, ew_grid(c, c->neq), 256, 0, c->stream, c->d_scal + slot_ss, x, x, c->neq);
-  LLG_CUDA_TRY(cudaPeekAtLastError());
-  return 0;
-}
-
-int vscale_gs(llg_ctx* c, int slot_vk_dot, int slot_ss, double* x) {
-  LLG_COUNT(KID_ELEMWISE);
-  klaunch(k_scale_gs, ew_grid(c, c->neq), 256, 0, c->stream, c->d_scal + slot_vk_dot, c->d_scal + slot_ss, x, x, c->neq);
-  LLG_CUDA_TRY(cudaPeekAtLastError());
-  return 0;
-}
-
-int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss) {
+int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss, const KScale* ks,
+                   int slot_aout) {
   if (k < 1 || k > MAXV - 1) { llg_set_error("gs_update: bad k"); return LLG_ERR_ARG; }
   PtrPack pk{};
   for (int j = 0; j < k; j++) pk.p[j] = V[j];
+  const KScale kz{};
   LLG_COUNT(KID_REDUCE);
   klaunch(k_gs_update, red_blocks(c->neq), RT, 0, c->stream, k, pk, c->d_scal + slot_dots, V[k], c->neq, c->d_red,
-                                                       c->d_counter, c->d_scal + slot_ss);
+          c->d_counter, c->d_scal + slot_ss, ks ? *ks : kz, slot_aout >= 0 ? c->d_scal + slot_aout : nullptr);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

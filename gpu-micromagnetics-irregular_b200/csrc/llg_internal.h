@@ -144,8 +144,10 @@ int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da = nu
 // (da non-null: in, out, gamma and the setup gamma come from the device-resident
 // integrator's DevArgs at run time; the pointer arguments are ignored)
 int arnoldi_setup(llg_ctx* c);   // shared-memory opt-in and grid of the persistent Arnoldi operator
+// (in_a: the input's KScale scale; null: the input is used as stored)
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out,
-                      const double* y, double gamma, int scale_out = 1, const DevArgs* da = nullptr);
+                      const double* y, double gamma, int scale_out = 1, const DevArgs* da = nullptr,
+                      const double* in_a = nullptr);
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot);
 
 // ── demag (k_demag.cu) ─────────────────────────────────────────────────
@@ -184,8 +186,32 @@ int learned_harvest(llg_ctx* c, const double* u, const double* x, const double* 
 // ── vector ops (k_vector.cu) ───────────────────────────────────────────
 int reductions_init(llg_ctx* c);
 void reductions_free(llg_ctx* c);
+// Krylov basis vectors that the read-back-light SPGMR keeps unnormalised in
+// memory: vector i is read as a_i * V_i, with a_i the device scalar *a[i] (1
+// when a[i] is null).  The kernel that forms a vector's norm also writes its
+// scale (gs_scale_of: 1 / ||v||, or 1 when classical Gram-Schmidt's norm test
+// asks for a second pass, after which the host normalises the vector
+// itself).  Each consumer forms a_i * V_i before using it, the product a
+// normalising pass would have stored, so the results are those of
+// normalising in place.
+constexpr int KS_MAX = 17;
+struct KScale {
+  const double* a[KS_MAX];
+};
+#ifdef __CUDACC__
+__device__ __forceinline__ double kscale_of(const double* a) { return a ? *a : 1.0; }
+// scale of a vector with sum of squares ss; vk (optional): its sum of squares
+// before the Gram-Schmidt update (1000 ||v|| < ||v before||: a second pass is due)
+__device__ __forceinline__ double gs_scale_of(double ss, const double* vk) {
+  if (vk && 1000.0 * sqrt(ss) < sqrt(*vk)) return 1.0;
+  return 1.0 / sqrt(ss);
+}
+#endif
+
 // device-side: results land in c->d_scal[slot..]; host copy via fetch_scalars
-int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot);
+// (ks: scales of the Y vectors; null: none)
+int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot,
+                   const KScale* ks = nullptr);
 int vwrms_dev(llg_ctx* c, const double* x, const double* w, int slot);
 int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double* y,
                    const double* w, int slot);
@@ -193,9 +219,10 @@ int fetch_scalars(llg_ctx* c, int slot, int n, double* out);
 // copy d_scal[lo, hi) to c->h_scal[lo, hi) and wait (one read-back)
 int fetch_range(llg_ctx* c, int lo, int hi);
 // device-coefficient forms used by the read-back-light SPGMR
-int vscale_rsqrt(llg_ctx* c, int slot_ss, double* x);                  // x /= sqrt(d_scal[slot_ss])
-int vscale_gs(llg_ctx* c, int slot_vk_dot, int slot_ss, double* x);    // same, unless a 2nd GS pass is due
-int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss);
+// (aout: also write the updated vector's KScale scale there, gs_scale_of with
+// the vector's pre-update sum of squares at d_scal[slot_dots + k])
+int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss, const KScale* ks = nullptr,
+                   int slot_aout = -1);
 double vmaxnorm_host(llg_ctx* c, const double* x);
 int vlin(llg_ctx* c, double a, const double* x, double b, const double* y, double* z);
 int vscale(llg_ctx* c, double a, const double* x, double* z);
@@ -222,10 +249,13 @@ int fused_lin_normalize(llg_ctx* c, const double* zn0, const double* ycor /* nul
 int fused_field(llg_ctx* c, const double* y);
 int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* ycor /* null: zero */, double rl1,
                 double gamma, double* negres, const DevArgs* da = nullptr);
+// (slot_aout >= 0: also write V0's KScale scale 1 / ||V0|| to d_scal[slot_aout])
 int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot,
-                           const DevArgs* da = nullptr);
-int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot);
-int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z);
+                           const DevArgs* da = nullptr, int slot_aout = -1);
+int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot,
+                       const KScale* ks = nullptr);
+int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z,
+                      const KScale* ks = nullptr);
 int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot,
                        const DevArgs* da = nullptr);
 int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double b, const double* x3,
@@ -241,5 +271,5 @@ int fused_complete(llg_ctx* c, int q, int qmax, const double* l, const double* a
                    bool norms, double cquot, const double* w, int slot);
 // GMRES correction (stored only when del is non-null) + Newton update + both norms
 int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
-                         double* del, bool ycor_zero, double* ycor, int slot);
+                         double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks = nullptr);
 
