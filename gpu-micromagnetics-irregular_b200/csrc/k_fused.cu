@@ -210,10 +210,13 @@ __global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, d
                                                      KScale ks) {
   pdl_entry();
   __shared__ double sm[RT / 32];
+  __shared__ double xs[FV];   // scales of the X vectors, staged once (see k_lincomb_update)
+  if (threadIdx.x < nv) xs[threadIdx.x] = kscale_of(ks.a[threadIdx.x]);
+  __syncthreads();
   double acc[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
-    double s = c.c[0] * (kscale_of(ks.a[0]) * X.p[0][i]);
-    for (int k = 1; k < nv; k++) s = c.c[k] * (kscale_of(ks.a[k]) * X.p[k][i]) + s;
+    double s = c.c[0] * (xs[0] * X.p[0][i]);
+    for (int k = 1; k < nv; k++) s = c.c[k] * (xs[k] * X.p[k][i]) + s;
     z[i] = s;
     acc[0] += s * s;
   }
@@ -224,9 +227,12 @@ __global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, d
 __global__ void k_lincomb_div(int nv, CPack c, XPack X, const double* __restrict__ w, double* __restrict__ z,
                               long long n, KScale ks) {
   pdl_entry();
+  __shared__ double xs[FV];   // scales of the X vectors, staged once (see k_lincomb_update)
+  if (threadIdx.x < nv) xs[threadIdx.x] = kscale_of(ks.a[threadIdx.x]);
+  __syncthreads();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    double s = c.c[0] * (kscale_of(ks.a[0]) * X.p[0][i]);
-    for (int k = 1; k < nv; k++) s = c.c[k] * (kscale_of(ks.a[k]) * X.p[k][i]) + s;
+    double s = c.c[0] * (xs[0] * X.p[0][i]);
+    for (int k = 1; k < nv; k++) s = c.c[k] * (xs[k] * X.p[k][i]) + s;
     z[i] = s / w[i];
   }
 }
@@ -266,7 +272,12 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X,
                                                        KScale ks) {
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
-  const double xa0 = kscale_of(ks.a[0]);   // scales of the X vectors (1 when stored normalised)
+  // scales of the X vectors (1 when stored normalised), staged once: read
+  // through pointers they would be reloaded after every store (aliasing)
+  __shared__ double xs[FV];
+  if (threadIdx.x < nv) xs[threadIdx.x] = kscale_of(ks.a[threadIdx.x]);
+  __syncthreads();
+  const double xa0 = xs[0];
   double acc[2] = {0.0, 0.0};
   const long long st = (long long)gridDim.x * RT;
   for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
@@ -280,7 +291,7 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X,
       yv[u] = (in && ycor_in) ? ycor_in[i] : 0.0;
     }
     for (int k = 1; k < nv; k++) {
-      const double xa = kscale_of(ks.a[k]);
+      const double xa = xs[k];
       double xv[UB];
 #pragma unroll
       for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * X.p[k][i0 + u * st] : 0.0;

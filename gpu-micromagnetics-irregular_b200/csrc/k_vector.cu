@@ -230,7 +230,11 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
                                                   double* out, KScale ks, double* aout) {
   pdl_entry();
   __shared__ double sm[RT / 32];
-
+  // scales of the X vectors, staged once: read through pointers, they would be
+  // reloaded after every store to z (the compiler cannot rule out aliasing)
+  __shared__ double xs[MAXV - 1];
+  if (threadIdx.x < k) xs[threadIdx.x] = kscale_of(ks.a[threadIdx.x]);
+  __syncthreads();
   double cf[MAXV - 1];
 #pragma unroll
   for (int j = 0; j < MAXV - 1; j++) cf[j] = (j < k) ? -dots[j] : 0.0;
@@ -245,7 +249,7 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
       if (j < k) {
         double xv[UB];
 #pragma unroll
-        const double xa = kscale_of(ks.a[j]);   // the scale of X_j (1 when stored normalised)
+        const double xa = xs[j];   // the scale of X_j (1 when stored normalised)
 #pragma unroll
         for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * X.p[j][i0 + u * st] : 0.0;
 #pragma unroll
