@@ -140,7 +140,7 @@ typedef struct llg_stats {
 typedef struct llg_ctx llg_ctx;
 
 /* ── lifecycle ────────────────────────────────────────────────────────── */
-/* Fill p with the physics of BASELINE config 0 (A=1, k=0.1 along +x, …). */
+/* Fill p with the physics of the reference's 128x64 free-edge film (A=1, k=0.1 along +x, …). */
 int  llg_default_params(llg_params* p);
 int  llg_default_solver_opts(llg_solver_opts* o);
 int  llg_create(const llg_params* p, llg_ctx** out);

@@ -45,7 +45,7 @@ def _integrate(p, geo_setup, y0_host, t_end, dt_out, opts):
 
 
 def test_config0_device_resident_matches_oracle(oracle_lib, gpu):
-    """BASELINE config 0 (128x64, no demag, t 0 -> 100) with the step control
+    """The reference's CPU-runnable film (128x64, no demag, t 0 -> 100) with the step control
     on the device: identical counters to the oracle's CVODE restatement."""
     import torch
     p = llg.default_params(128, 64)

@@ -258,7 +258,7 @@ def run_integration(oracle_lib, p, geo, t_end, dt_out, opts, set_geom):
 
 
 def test_integrator_config0_matches_oracle(oracle_lib, gpu):
-    """128x64, free edges, A=1, k=0.1 (+x), h=(0,0,0.05),
+    """The reference's CPU-runnable film: 128x64, free edges, A=1, k=0.1 (+x), h=(0,0,0.05),
     alpha=0.02, jittered uniform IC (srand 12345), rtol 1e-4, atol 1e-6,
     SPGMR(5) + block-Jacobi, t 0→100 in 0.1 output intervals."""
     p = llg.default_params(128, 64)
