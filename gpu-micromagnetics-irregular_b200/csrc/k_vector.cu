@@ -248,7 +248,6 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
     for (int j = 0; j < MAXV - 1; j++)
       if (j < k) {
         double xv[UB];
-#pragma unroll
         const double xa = xs[j];   // the scale of X_j (1 when stored normalised)
 #pragma unroll
         for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * X.p[j][i0 + u * st] : 0.0;
