@@ -1,13 +1,14 @@
 // k_noalloc.cu — the Gram–Schmidt multi-dot without any device allocation.
 //
-// Who needs it: some callers cannot allocate device memory at the moment
-// they need K dot products — code that runs while a CUDA stream is being
-// captured into a graph (cudaMalloc is not permitted during a global-mode
-// capture), real-time or solver loops that forbid allocation after set-up,
-// and applications whose device memory belongs entirely to another
-// allocator.  llg_dot_multi works through an llg_ctx, and creating one
-// allocates; this entry point needs only the caller's input and output
-// buffers.
+// Who needs it: some callers cannot let a library allocate device memory at
+// the moment they need K dot products.  An application whose device memory
+// is owned by another allocator (a framework's caching pool that has
+// reserved the GPU) would see a cudaMalloc fail or fragment its pool; a
+// solver loop with a fixed memory budget, or one with real-time limits,
+// allows no allocation after set-up because cudaMalloc/cudaFree can
+// synchronise the device.  llg_dot_multi works through an llg_ctx, and
+// creating one allocates; this entry point needs only the caller's input
+// and output buffers.
 //
 // Its reduction scratch — the per-block partial sums and the last-block
 // ticket — is one file-scope device array of LLG_NOALLOC_MAX_VECS x
@@ -16,8 +17,11 @@
 // code cannot pass the array's name to a kernel (in host code the name is a
 // host-side stand-in, not a device address), so the first call on each
 // device looks up the device address with cudaGetSymbolAddress, with that
-// device current, and caches it; that first call should come before any
-// stream capture.  All calls share the array and it keeps the last call's
+// device current, and caches it per device ordinal; that first call should
+// come before any stream capture.  The cached address belongs to the CUDA
+// runtime's primary context of the device: callers that make another
+// driver-API context current on the same device must not use this entry
+// point from it.  All calls share the array and it keeps the last call's
 // contents: the ticket is cleared on the caller's stream at the start of
 // every call, and calls that overlap on the GPU (different streams, no
 // ordering between them) race on the array.

@@ -199,16 +199,20 @@ int  llg_wrms_norm(llg_ctx* ctx, const double* d_x, const double* d_w, double* h
 /* d_out[k] = x · Y[k] (k < nvec), d_out a caller-owned device buffer of nvec
  * doubles, on cuda_stream (NULL = legacy default).  No counterpart in the
  * reference: this is the llg_dot_multi reduction for callers that cannot
- * allocate device memory when they need it (during CUDA stream capture, in
- * allocation-free solver loops, or when another allocator owns all device
- * memory).  It needs no llg_ctx and calls no cudaMalloc/cudaFree: its
- * scratch is a fixed file-scope device array of LLG_NOALLOC_MAX_VECS x
- * LLG_NOALLOC_MAX_BLOCKS doubles (~128 KiB) that every GPU loading the
- * library keeps until exit.  nvec > LLG_NOALLOC_MAX_VECS is rejected
- * (LLG_ERR_ARG).  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and should come before any stream capture.
- * Calls share the array: calls that overlap on the GPU race.  Same result,
- * bit for bit, as llg_dot_multi.                                              */
+ * let a library allocate device memory when they need it — an application
+ * whose device memory belongs to another allocator (a framework pool that
+ * has reserved the GPU), or a solver loop that allows no allocation after
+ * set-up because cudaMalloc/cudaFree may synchronise the device.  It needs
+ * no llg_ctx and calls no cudaMalloc/cudaFree: its scratch is a fixed
+ * file-scope device array of LLG_NOALLOC_MAX_VECS x LLG_NOALLOC_MAX_BLOCKS
+ * doubles (~128 KiB) that every GPU loading the library keeps until exit.
+ * nvec > LLG_NOALLOC_MAX_VECS is rejected (LLG_ERR_ARG).  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress) in
+ * the CUDA runtime's primary context of that device and caches it: use the
+ * entry point from that context only, and make the first call on a device
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race.  Same result, bit for bit, as llg_dot_multi for the same
+ * vectors (same block partition, per-thread order and reduction tree).      */
 #define LLG_NOALLOC_MAX_VECS   16
 #define LLG_NOALLOC_MAX_BLOCKS 1024
 int  llg_dot_multi_noalloc(int nvec, const double* d_x, const double* const* d_Y, int64_t n,

@@ -1,13 +1,15 @@
 """llg_dot_multi_noalloc: the multi-dot for callers that cannot allocate.
 
-Callers inside CUDA stream capture, allocation-free solver loops, or
-applications whose device memory is owned by another allocator cannot let a
-library call cudaMalloc when they ask for K dot products.  This entry point
-keeps its reduction scratch in a fixed device array instead; the test checks
-it against the allocating llg_dot_multi through the C ABI on two calls in a
-row (the scratch array keeps the previous call's contents), plus the size
-limit.  This file sorts last so a stop-at-first-failure run has already run
-every other test; it also passes alone in a fresh process.
+Applications whose device memory is owned by another allocator, and solver
+loops that allow no allocation after set-up (cudaMalloc/cudaFree may
+synchronise the device), cannot let a library call cudaMalloc when they ask
+for K dot products.  This entry point keeps its reduction scratch in a fixed
+device array instead; the test checks it against the allocating
+llg_dot_multi through the C ABI on two calls in a row (the scratch array
+keeps the previous call's contents): bit for bit where both reduce the same
+vectors, within 1e-13 of a host sum for the shorter prefixes.  It also
+checks the size limit.  This file sorts last so a stop-at-first-failure run
+has already run every other test; it also passes alone in a fresh process.
 """
 import ctypes as C
 
@@ -49,8 +51,11 @@ def test_noalloc_multi_dot_matches_allocating_entry_point(gpu):
             assert rc == 0, llg.load().llg_last_error()
             torch.cuda.synchronize()
             got = out.cpu().numpy()
-            scale = max(np.abs(ref).max(), 1.0)
-            assert np.abs(got - ref).max() <= 1e-13 * scale, (nvec, length, call, got, ref)
+            if length == n:   # same partition, order and tree as llg_dot_multi
+                assert np.array_equal(got, ref), (nvec, length, call, got, ref)
+            else:             # against a host sum in another order
+                scale = max(np.abs(ref).max(), 1.0)
+                assert np.abs(got - ref).max() <= 1e-13 * scale, (nvec, length, call, got, ref)
             out.fill_(np.nan)
 
 
