@@ -5,24 +5,29 @@ cells, centred square hole of side 0.25*ny, open-boundary FFT demag
 (strength 4, thickness 1, zero-padded 3072x1024 transform grid), exchange
 A=1, uniaxial k=0.1 along +x, Zeeman (0,0,0.05), alpha=0.02, free edges,
 uniform (1,0,0) + seeded +-0.01 jitter, BDF + Newton + SPGMR(5) with 3x3
-block-Jacobi, rtol 1e-4 / atol 1e-6, FP64.  Synthetic data (seeded builders).
+block-Jacobi, rtol 1e-4 / atol 1e-6.  Synthetic data (seeded builders).
 
-A "step" integrates `--dt` units of simulated time (default 1.0) through
-llg_integrate at the reference's 0.1 output cadence.  value = K*dt / device
-time of K steps (CUDA events on the library's stream, max over ranks);
-the state (>= 20 vectors of 18.9 MB) exceeds L2, so no flush is needed.
+Timed window (both arms): a fresh instance integrated from t = 0 over K
+steps of --dt simulated time (default 1.0), each step through llg_integrate
+at the reference's 0.1 output cadence; value = K*dt / device time (CUDA
+events on the library's stream, max over ranks).  Warm-up: W output
+intervals (0.1 each) on a throwaway instance of the same form.  The state
+(>= 20 vectors of 18.9 MB) exceeds L2, so no flush is needed.
 
 Forms (--form): "plain" is the reference method in FP64; "mixed" runs the
 demag transforms in reduced precision (FP32 rows, tensor-core FP16 hi+lo
-column DFT stages with FP32 accumulation).  By default the best form built
-is timed and then a plain FP64 instance of the same workload is timed the
-same way; the line reports both throughputs, their ratio and the max |dm|
-between the two final states.
+column DFT stages with FP32 accumulation); "learned+mixed" adds the learned
+preconditioner (kept only while it pays for itself; the line names what
+ran).  By default the best form is timed, then plain FP64 the same way; the
+line reports both, their ratio and the form's accuracy: max|dm| against
+plain FP64 with both runs taking plain FP64's recorded step sequence
+(step-sequence replay), at t = 1, 5, 20, 200.
 
 --impl reference runs the CPU restatement of the reference path (the oracle;
-the reference itself needs SUNDIALS, which is absent) on all host cores.
-Multi-GPU: independent replicas (one instance per rank, no collective in
-the hot path); only the timing max uses torch.distributed.
+the reference itself needs SUNDIALS, which is absent) on all host cores,
+over the same window.  Multi-GPU: independent replicas (one instance per
+rank, no collective in the hot path); only the timing max uses
+torch.distributed.
 """
 import argparse
 import ctypes as C
@@ -48,13 +53,32 @@ TIMER_STRIDE = 7                # event pair around every 7th launch of a family
                                 # launches of a solve are sampled); the rest keep their chained launch
 
 
-def workload(ng=1536, ny=512, seed=12345):
+# Gram-Schmidt for every form: CVODE's classical Gram-Schmidt with its
+# reorthogonalisation test (one extra pass when the new vector loses 3 digits),
+# which needs one read-back per Arnoldi iteration.  The reference lets SPGMR
+# pick modified Gram-Schmidt at neq >= 5e5 (2d_i2/2d_fft.cu:674-679), a
+# sequential dot-then-update chain; its plain FP64 throughput with that choice
+# is measured beside the headline (plain_fp64_reference_gs_value).
+GS = llg.GS_CLASSICAL
+WORKLOAD = ("1536x512 cells, square hole side 0.25*ny, open FFT demag strength 4 (3072x1024 padded), "
+            "A=1 k=0.1(+x) h=(0,0,0.05) alpha=0.02, free edges, rtol 1e-4 atol 1e-6, SPGMR(5), block-Jacobi")
+
+
+def workload(ng=1536, ny=512, seed=12345, gs=None):
     p = llg.default_params(ng, ny, demag_mode=llg.DEMAG_OPEN, demag_strength=4.0, demag_thick=1.0,
                            bc=llg.BC_FREE, norm_kind=llg.NORM_REG)
     g = llg.default_geom(ng, ny, geometry_kind=llg.GEOM_HOLE_SQUARE, hole_radius_frac_y=0.125,
                          ic_jitter_eps=0.01, init_random_seed=seed)
-    o = llg.default_solver_opts(rtol=1e-4, atol=1e-6, maxl=5, gs_type=llg.GS_CLASSICAL)
+    o = llg.default_solver_opts(rtol=1e-4, atol=1e-6, maxl=5, gs_type=GS if gs is None else gs)
     return p, g, o
+
+
+def bench_config(args, world):
+    """The workload description both arms print (identical dicts)."""
+    return {"workload": WORKLOAD, "sim_time_per_step": args.dt, "output_interval": 0.1,
+            "window": f"fresh instance, t 0 -> {args.steps * args.dt:g}",
+            "warmup": f"{args.warmup} output intervals on a throwaway instance",
+            "parallelism": f"replicas x{world}", "l2": "state > 126 MB L2 (>= 20 vectors x 18.9 MB); no flush"}
 
 
 def algorithmic_bytes(kid, ng, ny, dims, mixed=False):
@@ -167,12 +191,13 @@ def make_ctx(p, g):
 # Forms of the same workload.  "plain" is the reference method in FP64; the
 # others change only the demag transform precision and the preconditioner.
 FORMS = {
-    "plain": dict(demag_precision=llg.DEMAG_FP64, learned=False,
+    "plain": dict(demag_precision=llg.DEMAG_FP64, learned=False, name="plain FP64",
                   desc="plain FP64 (block-Jacobi, FP64 FFT demag)"),
-    "mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=False,
+    "mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=False, name="mixed-precision demag",
                   desc="mixed-precision demag (FP32 row FFTs, tcgen05 FP16 hi+lo column DFT stages with FP32 "
                        "accumulation), block-Jacobi; FP64 state, norms, Newton update, Gram-Schmidt"),
     "learned+mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=True,
+                          name="learned preconditioner + mixed-precision demag",
                           desc="learned preconditioner (3-layer 3x3 conv, 16 channels, BF16 weights, FP32 "
                                "accumulation, fused tcgen05 inference, on top of block-Jacobi, trained on the GPU on "
                                "this workload's own harvested SPGMR solves; every 8th solve probes block-Jacobi and "
@@ -213,24 +238,37 @@ def train_weights(rank):
     return w, info
 
 
-def form_params(form, seed):
-    p, g, o = workload(seed=seed)
+def form_params(form, seed, gs=None):
+    p, g, o = workload(seed=seed, gs=gs)
     p.demag_precision = FORMS[form]["demag_precision"]
     p.precond_kind = llg.PREC_LEARNED if FORMS[form]["learned"] else llg.PREC_BLOCK_JACOBI
     return p, g, o
 
 
-def timed_run(args, form, world, rank, local, lib, clocks=True):
-    """Warm-up W steps, then K timed steps of one fresh instance of `form`."""
+def timed_run(args, form, world, rank, local, lib, clocks=True, gs=None):
+    """W warm-up output intervals on a throwaway instance, then K timed steps
+    of a fresh instance of `form` from t = 0."""
     import torch
-    p, g, o = form_params(form, 12345 + rank)
-    ctx, geo = make_ctx(p, g)
-    if FORMS[form]["learned"]:
-        ctx.learned_set_weights(train_weights(rank)[0])
-    y0 = torch.from_numpy(geo["y0"]).cuda()
-    ctx.integrator_init(0.0, y0, o)
-    yout = torch.zeros_like(y0)
     sub = max(1, int(round(args.dt / 0.1)))
+
+    def instance():
+        p, g, o = form_params(form, 12345 + rank, gs)
+        ctx, geo = make_ctx(p, g)
+        if FORMS[form]["learned"]:
+            ctx.learned_set_weights(train_weights(rank)[0])
+        y0 = torch.from_numpy(geo["y0"]).cuda()
+        ctx.integrator_init(0.0, y0, o)
+        return ctx, y0, p, g, o
+
+    wctx, wy0, *_ = instance()
+    wout = torch.zeros_like(wy0)
+    for k in range(1, args.warmup + 1):
+        wctx.integrate(0.1 * k, wout)
+    torch.cuda.synchronize()
+    wctx.close()
+    del wctx, wy0, wout
+    ctx, y0, p, g, o = instance()
+    yout = torch.zeros_like(y0)
     state = {"t": 0.0}
 
     def step():
@@ -238,8 +276,6 @@ def timed_run(args, form, world, rank, local, lib, clocks=True):
             ctx.integrate(state["t"] + args.dt * (k + 1) / sub, yout)
         state["t"] += args.dt
 
-    for _ in range(args.warmup):
-        step()
     counts0 = (C.c_int64 * 16)()
     counts1 = (C.c_int64 * 16)()
     lib.llg_kernel_counts(counts0, 16)
@@ -276,10 +312,17 @@ def timed_run(args, form, world, rank, local, lib, clocks=True):
     st1 = ctx.stats()
     launches = {KERNEL_NAMES[k]: int(counts1[k] - counts0[k]) for k in range(13)}
     dst = {k: st1[k] - st0[k] for k in ("nst", "nfe", "nni", "nli", "nsetups", "netf", "ncfn")}
+    ran = FORMS[form]["name"]
     if FORMS[form]["learned"]:
-        dst["learned_status"] = ctx.learned_status()
+        ls = ctx.learned_status()
+        dst["learned_status"] = ls
+        if ls["fell_back"]:
+            ran = f"{FORMS['mixed']['name']} (learned preconditioner fell back to block-Jacobi: " + \
+                  ("its cost exceeded its iteration saving" if ls["fell_back"] == 2 else "a learned solve failed") + ")"
+        ran += f"; learned applications {ls['napply']}"
     return {"ctx": ctx, "p": p, "g": g, "o": o, "yout": yout, "t": state["t"], "ms": ms, "launches": launches,
-            "counters": dst, "value": world * args.steps * args.dt / (ms / 1000.0), "clocks": clk, "live": live}
+            "counters": dst, "value": world * args.steps * args.dt / (ms / 1000.0), "clocks": clk, "live": live,
+            "ran": ran}
 
 
 def roofline_for(lib, run, ng, ny, mixed):
@@ -324,8 +367,9 @@ def roofline_for(lib, run, ng, ny, mixed):
                       "families inside the timed region"}
 
 
-def short_run(form, rank, t_out, strength_scale=1.0, rtol=None):
-    """Integrate a fresh instance of `form` from t=0 and return y at each t in t_out."""
+def fixed_run(form, rank, t_out, strength_scale=1.0, rtol=None, record=False, replay=None):
+    """Integrate a fresh instance of `form` from t=0 at the 0.1 output cadence
+    and return y at each t in t_out (and the recorded steps / replay status)."""
     import torch
     p, g, o = form_params(form, 12345 + rank)
     p.demag_strength *= strength_scale
@@ -336,41 +380,54 @@ def short_run(form, rank, t_out, strength_scale=1.0, rtol=None):
         ctx.learned_set_weights(train_weights(rank)[0])
     y0 = torch.from_numpy(geo["y0"]).cuda()
     ctx.integrator_init(0.0, y0, o)
+    if record:
+        ctx.record_steps(10_000_000)
+    if replay is not None:
+        ctx.replay_steps(*replay)
     yout = torch.zeros_like(y0)
     outs = {}
-    for k in range(1, int(round(max(t_out) / 0.1)) + 1):
+    kmax = int(round(max(t_out) / 0.1))
+    want = {int(round(t / 0.1)) for t in t_out}
+    for k in range(1, kmax + 1):
         ctx.integrate(0.1 * k, yout)
-        if any(abs(0.1 * k - t) < 1e-9 for t in t_out):
+        if k in want:
             outs[round(0.1 * k, 6)] = yout.cpu().numpy().copy()
+    extra = {}
+    if record:
+        extra["steps"] = ctx.recorded_steps()
+    if replay is not None:
+        extra["replay"] = ctx.replay_status()
+    if FORMS[form]["learned"]:
+        extra["learned_status"] = ctx.learned_status()
     ctx.close()
-    return outs
+    return outs, extra
 
 
-def accuracy_check(form, rank, t_out=(0.5, 1.0, 2.0, 4.0), t_tight=(0.5, 1.0)):
-    """max|dm| of `form` against plain FP64 on the bench workload, from the same
-    initial state, at early times.
-
-    At the bench tolerance (rtol 1e-4) two forms that take different (equally
-    valid) step sequences differ at the integration-error level, and the
-    jittered uniform state under demag at alpha 0.02 is physically unstable,
-    so every difference grows exponentially — a control (plain FP64 with the
-    demag strength perturbed by 1e-9) shows that growth.  At rtol 1e-6 the
-    integration error is far below 1e-4 and what remains is the form's own
-    (reduced-precision demag, learned preconditioner) contribution."""
-    a = short_run("plain", rank, t_out)
-    b = short_run(form, rank, t_out)
-    c = short_run("plain", rank, t_out, strength_scale=1.0 + 1e-9)
-    at = short_run("plain", rank, t_tight, rtol=1e-6)
-    bt = short_run(form, rank, t_tight, rtol=1e-6)
-    md = lambda x, y, ts: [float(np.abs(x[round(t, 6)] - y[round(t, 6)]).max()) for t in ts]
-    return {"t": list(t_out),
-            "max_dm_form_vs_plain_fp64": md(b, a, t_out),
-            "max_dm_control_fp64_strength_1e-9": md(c, a, t_out),
-            "t_tight": list(t_tight),
-            "max_dm_form_vs_plain_fp64_rtol1e-6": md(bt, at, t_tight),
-            "note": "rows 1-2 at the bench tolerance (rtol 1e-4): different accepted step sequences, amplified by "
-                    "the workload's instability (control: plain FP64 vs plain FP64 with demag strength x(1+1e-9)); "
-                    "rtol 1e-6 row: integration error below 1e-4, the form's own error"}
+def replay_accuracy(form, rank, t_out=(1.0, 5.0, 20.0, 200.0), t_floor=(1.0, 5.0)):
+    """max|dm| of `form` against plain FP64 on the bench workload with both
+    runs taking plain FP64's accepted step sequence (recorded, then replayed):
+    what remains is the form's own arithmetic, not step selection.  Beside
+    it, on the same steps, a plain FP64 run with the demag strength scaled by
+    (1 + 1e-9) shows how much the workload's dynamics amplify a tiny
+    perturbation; and plain FP64 at rtol 1e-6 against rtol 1e-8 shows the
+    integration-error floor of a tighter tolerance."""
+    md = lambda x, y, ts: [float(np.abs(x[round(t, 6)] - y[round(t, 6)]).max()) for t in ts]  # noqa: E731
+    a, ra = fixed_run("plain", rank, t_out, record=True)
+    steps = ra["steps"]
+    b, rb = fixed_run(form, rank, t_out, replay=steps)
+    c, rc = fixed_run("plain", rank, t_out, strength_scale=1.0 + 1e-9, replay=steps)
+    f6, _ = fixed_run("plain", rank, t_floor, rtol=1e-6)
+    f8, _ = fixed_run("plain", rank, t_floor, rtol=1e-8)
+    dm = md(b, a, t_out)
+    ok_t = [t for t, d in zip(t_out, dm) if d <= 1e-4]
+    out = {"t": list(t_out), "max_dm_replayed": dm,
+           "max_dm_control_fp64_strength_1e-9_replayed": md(c, a, t_out),
+           "replay_forced_accepts": rb["replay"]["forced_accepts"], "plain_steps_recorded": int(len(steps[0])),
+           "t_floor": list(t_floor), "max_dm_fp64_rtol1e-6_vs_rtol1e-8": md(f6, f8, t_floor),
+           "bound": 1e-4, "holds_at_t": ok_t, "holds_everywhere": len(ok_t) == len(t_out)}
+    if "learned_status" in rb:
+        out["learned_status_in_replay"] = rb["learned_status"]
+    return out
 
 
 def e2e_run(args, form, world, rank):
@@ -409,8 +466,9 @@ def e2e_run(args, form, world, rank):
     return {"value": world * args.steps * args.dt / (ems / 1000.0), "unit": UNIT,
             "h2d_bytes_per_step": int((y0_h.numel() * 8 + mask_h.numel() * 8) / args.steps),
             "d2h_bytes_per_step": int(frame_h.numel() * 8),
-            "note": "fresh instance from t=0: pinned y0 + mask uploaded once and amortised over the steps; "
-                    "one y(t) frame copied back per step; includes integrator start-up"}
+            "note": "the timed window through the public API from host buffers: fresh instance from t=0, pinned "
+                    "y0 + mask uploaded inside the timed region (amortised over the steps), one y(t) frame "
+                    "copied back per step"}
 
 
 def run_ours(args, world, rank, local):
@@ -422,29 +480,38 @@ def run_ours(args, world, rank, local):
     main = timed_run(args, form, world, rank, local, lib)
     roof = roofline_for(lib, main, ng, ny, FORMS[form]["demag_precision"] == llg.DEMAG_MIXED)
     clk = main["clocks"].summary()
-    y_main = main["yout"].cpu().numpy()
     main["ctx"].close()
+    summary = {"form_ran": main["ran"], "value": main["value"]}
     compare = None
     if form != "plain" and not args.no_compare:
         plain = timed_run(args, "plain", world, rank, local, lib, clocks=False)
-        y_plain = plain["yout"].cpu().numpy()
         plain["ctx"].close()
         compare = {"plain_fp64_value": plain["value"], "plain_fp64_ms_per_step": plain["ms"] / args.steps,
                    "ratio_vs_plain_fp64": main["value"] / plain["value"],
                    "gmres_iters_per_newton": main["counters"]["nli"] / max(main["counters"]["nni"], 1),
                    "plain_gmres_iters_per_newton": plain["counters"]["nli"] / max(plain["counters"]["nni"], 1),
-                   "max_dm_vs_plain_fp64": float(np.abs(y_main - y_plain).max()),
-                   "dm_at_t": main["t"], "plain_counters": plain["counters"],
-                   "dm_note": "both forms integrated from the same state over [0, t]; at rtol 1e-4 they take a "
-                              "few different accepted steps, so the distance is at the integration-tolerance "
-                              "level and grows with the workload's physical instability"}
+                   "bdf_steps": main["counters"]["nst"], "plain_bdf_steps": plain["counters"]["nst"],
+                   "plain_counters": plain["counters"]}
         if FORMS[form]["learned"]:
             mixed = timed_run(args, "mixed", world, rank, local, lib, clocks=False)
             mixed["ctx"].close()
             compare["mixed_only_value"] = mixed["value"]
             compare["mixed_only_gmres_iters_per_newton"] = mixed["counters"]["nli"] / max(mixed["counters"]["nni"], 1)
-        compare["accuracy_early_t"] = accuracy_check(form, rank)
+        if not args.no_reference_gs:
+            mgs = timed_run(args, "plain", world, rank, local, lib, clocks=False, gs=llg.GS_AUTO)
+            mgs["ctx"].close()
+            compare["plain_fp64_reference_gs_value"] = mgs["value"]
+            compare["plain_fp64_reference_gs_note"] = ("plain FP64 with the reference's Gram-Schmidt choice at this "
+                                                       "size (modified, neq >= 5e5)")
+        summary.update(plain_fp64_value=plain["value"], ratio_vs_plain_fp64=compare["ratio_vs_plain_fp64"])
+    accuracy = None
+    if form != "plain" and not args.no_accuracy:
+        accuracy = replay_accuracy(form, rank)
+        summary.update(max_dm_replayed=dict(zip([str(t) for t in accuracy["t"]], accuracy["max_dm_replayed"])),
+                       accuracy_bound=1e-4, accuracy_holds_at_t=accuracy["holds_at_t"])
     e2e = None if args.no_e2e else e2e_run(args, form, world, rank)
+    if e2e:
+        summary["e2e_value"] = e2e["value"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
@@ -453,18 +520,14 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": main["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded geometry/IC builders)",
-        "config": {"workload": "1536x512 cells, square hole side 0.25*ny, open FFT demag strength 4 "
-                               "(3072x1024 padded), A=1 k=0.1(+x) h=(0,0,0.05) alpha=0.02, free edges, "
-                               "rtol 1e-4 atol 1e-6, SPGMR(5), classical GS",
-                   "form": FORMS[form]["desc"], "sim_time_per_step": args.dt,
-                   "output_interval": 0.1, "parallelism": f"replicas x{world}",
-                   "l2": "state > 126 MB L2 (>= 20 vectors x 18.9 MB); no flush",
-                   "solver_counters_timed": main["counters"]},
-        "compare": compare,
-        "training": _weights_cache.get("info") if FORMS[form]["learned"] else None,
+        "config": bench_config(args, world),
+        "form": FORMS[form]["desc"],
         "roofline": roof,
-        "e2e": e2e, "gpu_launches": sum(main["launches"].values()), "launches_by_family": main["launches"],
-        "clocks": clk, "cpu_baseline": cpu,
+        "e2e": e2e, "gpu_launches": sum(main["launches"].values()), "clocks": clk, "cpu_baseline": cpu,
+        "launches_by_family": main["launches"], "solver_counters_timed": main["counters"],
+        "training": _weights_cache.get("info") if FORMS[form]["learned"] else None,
+        "compare": compare, "accuracy": accuracy,
+        "summary": summary,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -533,28 +596,43 @@ def run_config4(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def cpu_oracle_run(dt_step, steps, warmup, threads):
+def cpu_oracle_run(dt_step, steps, warmup_intervals, threads):
+    """The oracle (C, OpenMP) on the bench workload: warm-up output intervals
+    of 0.1 on a throwaway instance, then `steps` steps of dt_step from t = 0
+    on a fresh instance, each at the 0.1 output cadence."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import binding
     binding.build()
     used = binding.set_threads(threads)
     p, g, o = workload()
     geo = binding.build_geometry(g)
-    orc = binding.Oracle(p)
-    orc.set_active(geo["active"])
-    orc.integrator_init(geo["y0"], o)
+
+    def instance():
+        orc = binding.Oracle(p)
+        orc.set_active(geo["active"])
+        orc.integrator_init(geo["y0"], o)
+        return orc
+
+    def advance(orc, t0, t1):
+        k0, k1 = int(round(t0 / 0.1)), int(round(t1 / 0.1))
+        for k in range(k0 + 1, k1 + 1):
+            rc, _, _ = orc.integrate(0.1 * k)
+            if rc != 0:
+                raise RuntimeError(f"oracle integrate rc={rc}")
+        if abs(t1 - 0.1 * k1) > 1e-12:
+            rc, _, _ = orc.integrate(t1)
+            if rc != 0:
+                raise RuntimeError(f"oracle integrate rc={rc}")
+
+    w = instance()
+    advance(w, 0.0, 0.1 * warmup_intervals)
+    del w
+    orc = instance()
     t = 0.0
-    for _ in range(warmup):
-        t += dt_step
-        rc, _, _ = orc.integrate(t)
-        if rc != 0:
-            raise RuntimeError(f"oracle integrate rc={rc}")
     t0 = time.perf_counter()
     for _ in range(steps):
+        advance(orc, t, t + dt_step)
         t += dt_step
-        rc, _, _ = orc.integrate(t)
-        if rc != 0:
-            raise RuntimeError(f"oracle integrate rc={rc}")
     el = time.perf_counter() - t0
     return steps * dt_step / el, used, el, orc.stats()
 
@@ -563,9 +641,9 @@ def cpu_baseline(args):
     threads = os.cpu_count() or 1
     val, used, el, st = cpu_oracle_run(args.cpu_dt, args.cpu_steps, 1, threads)
     return {"value": val, "unit": UNIT, "cores": used, "kind": "port",
-            "sample": f"same 1536x512+open-demag workload, {args.cpu_steps} output steps of {args.cpu_dt} "
-                      f"sim-time after 1 warm-up step from t=0 ({el:.1f} s CPU wall, {st['nst']} BDF steps total); "
-                      "C FP64 restatement of the reference path with OpenMP",
+            "sample": f"same 1536x512+open-demag workload, fresh instance, {args.cpu_steps} steps of {args.cpu_dt} "
+                      f"sim-time from t=0 ({el:.1f} s CPU wall, {st['nst']} BDF steps); C FP64 restatement of the "
+                      "reference path with OpenMP (the full window runs under --impl reference)",
             "cpu_model": cpu_model()}
 
 
@@ -581,22 +659,26 @@ def cpu_model():
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the CPU restatement of the reference path over the
+    same window as the GPU arm (fresh instance, t 0 -> K*dt), all host cores."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    dt = args.cpu_dt
-    val, used, el, st = cpu_oracle_run(dt, args.steps, args.warmup, threads)
+    val, used, el, st = cpu_oracle_run(args.dt, args.steps, args.warmup, threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry/IC builders)",
-        "config": {"workload": "1536x512 cells, square hole, open FFT demag strength 4, rtol 1e-4, SPGMR(5)+BJ",
-                   "sim_time_per_step": dt},
+        "config": bench_config(args, world),
+        "form": "plain FP64 (CPU restatement of the reference path: same RHS, demag, Jv, block-Jacobi, "
+                "CVODE-equivalent BDF/Newton/SPGMR with classical Gram-Schmidt)",
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": used, "kind": "port",
-                         "sample": f"{args.steps} steps of {dt} sim-time after {args.warmup} warm-up steps from t=0; "
-                                   "CPU FP64 restatement of the reference path (SUNDIALS absent, so the reference "
-                                   "solver itself cannot be built)"},
+                         "sample": f"the full window: {args.steps} steps of {args.dt} sim-time from t=0 on a fresh "
+                                   f"instance ({st['nst']} BDF steps, {el:.1f} s); CPU FP64 restatement of the "
+                                   "reference path (SUNDIALS absent, so the reference solver itself cannot be "
+                                   "built)", "cpu_model": cpu_model()},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "solver_counters": {k: st[k] for k in ("nst", "nfe", "nni", "nli", "nsetups", "netf", "ncfn")},
     }
     print(json.dumps(line), flush=True)
 
@@ -604,12 +686,15 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--dt", type=float, default=1.0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-dt", type=float, default=0.02)
+    ap.add_argument("--cpu-dt", type=float, default=0.1)
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the replayed accuracy runs")
+    ap.add_argument("--no-reference-gs", action="store_true",
+                    help="skip the plain FP64 run with the reference's Gram-Schmidt choice")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", choices=sorted(FORMS), default=None,

@@ -787,13 +787,13 @@ __device__ void ctl_exec(DState& s, int op) {
   }
 }
 
-__global__ void k_call_args(DState* s, double tout, double* yout) {
+__global__ void k_call_args(DState* s, double tout, double* yout, long long limit) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     s->tout = tout;
     s->yout = yout;
     s->guard_count = 0;
     s->trace_n = 0;
-    s->guard_max = 200LL * ((s->mxstep > 0 ? s->mxstep : 500) + 10) * (s->maxl + 4);
+    s->guard_max = limit > 0 ? limit : 200LL * ((s->mxstep > 0 ? s->mxstep : 500) + 10) * (s->maxl + 4);
     s->tripped = 0;
     for (int k = 0; k < 16; k++) s->kcount[k] = 0;
   }
@@ -1363,7 +1363,7 @@ int devint_upload(DevInteg* d, const DState& hs_in, llg_ctx* c) {
 }
 
 int devint_run(DevInteg* d, llg_ctx* c, double tout, double* yout, DState& hs) {
-  k_call_args<<<1, 1, 0, c->stream>>>(d->d_s, tout, yout);
+  k_call_args<<<1, 1, 0, c->stream>>>(d->d_s, tout, yout, c->ctl_limit);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   LLG_CUDA_TRY(cudaGraphLaunch(d->exec, c->stream));
   LLG_CUDA_TRY(cudaMemcpyAsync(d->h_s, d->d_s, sizeof(DState), cudaMemcpyDeviceToHost, c->stream));

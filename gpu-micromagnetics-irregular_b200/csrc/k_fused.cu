@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(RT) k_ewt_wrms(double rtol, double atol, const
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
     const double yi = y[i];
     const double t = rtol * fabs(yi) + atol;
-    if (!(t > 0.0)) acc[0] += 1.0;
+    if (t <= 0.0) acc[0] += 1.0;   // (a NaN state is left to the norm check)
     const double w = 1.0 / t;
     ewt[i] = w;
     const double p = yi * w;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(RT) k_predict_fused(ZPack zn, CPack f, int pen
       const long long i = (long long)a * n + cell;
       if (do_ewt) {
         const double t = rtol * fabs(v[a][0]) + atol;
-        if (!(t > 0.0)) acc[0] += 1.0;
+        if (t <= 0.0) acc[0] += 1.0;   // (a NaN state is left to the norm check)
         const double w = 1.0 / t;
         ewt[i] = w;
         const double p = v[a][0] * w;

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(RT) k_set_ewt(double rtol, double atol, const 
   double bad[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
     const double t = rtol * fabs(y[i]) + atol;
-    if (!(t > 0.0)) bad[0] = 1.0;
+    if (t <= 0.0) bad[0] = 1.0;   // (a NaN state is left to the norm check)
     ewt[i] = 1.0 / t;
   }
   const double wm = warp_max(bad[0]);

@@ -31,6 +31,13 @@ int integrator_run(llg_ctx* c, double tout, double* yout, double* tret);
 int integrator_stats(llg_ctx* c, llg_stats* st);
 int integrator_trace(llg_ctx* c, unsigned long long* buf, int cap);
 int integrator_trace_count(llg_ctx* c);
+int integrator_record_steps(llg_ctx* c, int cap);
+int integrator_recorded_steps(llg_ctx* c, double* h, int32_t* q, int cap);
+int integrator_replay_steps(llg_ctx* c, const double* h, const int32_t* q, int n);
+int integrator_replay_status(llg_ctx* c, int32_t* position, int64_t* forced);
+int integrator_checkpoint_size(llg_ctx* c, uint64_t* bytes);
+int integrator_checkpoint_save(llg_ctx* c, void* buf, uint64_t cap, uint64_t* written);
+int integrator_checkpoint_load(llg_ctx* c, const void* buf, uint64_t n);
 void learned_destroy(Learned* l);
 
 static void sync_dp(llg_ctx* c) {
@@ -381,6 +388,84 @@ int llg_get_stats(llg_ctx* c, llg_stats* st) {
   const int rc = integrator_stats(c, st);
   if (rc) return rc;
   return demag_check(c);
+}
+
+int llg_integrator_record_steps(llg_ctx* c, int32_t cap) {
+  if (!c) return LLG_ERR_ARG;
+  return integrator_record_steps(c, cap);
+}
+
+int llg_integrator_recorded_steps(llg_ctx* c, double* h, int32_t* q, int32_t cap) {
+  if (!c || cap < 0) return LLG_ERR_ARG;
+  return integrator_recorded_steps(c, h, q, cap);
+}
+
+int llg_integrator_replay_steps(llg_ctx* c, const double* h, const int32_t* q, int32_t n) {
+  if (!c) return LLG_ERR_ARG;
+  return integrator_replay_steps(c, h, q, n);
+}
+
+int llg_integrator_replay_status(llg_ctx* c, int32_t* position, int64_t* forced_accepts) {
+  if (!c) return LLG_ERR_ARG;
+  return integrator_replay_status(c, position, forced_accepts);
+}
+
+int llg_inject_rhs_failure(llg_ctx* c, int64_t after) {
+  if (!c) return LLG_ERR_ARG;
+  c->inject_rhs_after = after < 0 ? -1 : after;
+  c->inject_rhs_seen = 0;
+  return 0;
+}
+
+int llg_set_control_op_limit(llg_ctx* c, int64_t limit) {
+  if (!c || limit < 0) return LLG_ERR_ARG;
+  c->ctl_limit = limit;
+  return 0;
+}
+
+int llg_checkpoint_size(llg_ctx* c, uint64_t* bytes) {
+  if (!c || !bytes) return LLG_ERR_ARG;
+  return integrator_checkpoint_size(c, bytes);
+}
+
+int llg_checkpoint_save(llg_ctx* c, void* h_buf, uint64_t cap, uint64_t* written) {
+  if (!c) return LLG_ERR_ARG;
+  return integrator_checkpoint_save(c, h_buf, cap, written);
+}
+
+int llg_checkpoint_load(llg_ctx* c, const void* h_buf, uint64_t n) {
+  int rc = ready(c);
+  if (rc) return rc;
+  return integrator_checkpoint_load(c, h_buf, n);
+}
+
+int llg_checkpoint_write_file(llg_ctx* c, const char* path) {
+  if (!c || !path) return LLG_ERR_ARG;
+  uint64_t n = 0;
+  int rc = integrator_checkpoint_size(c, &n);
+  if (rc) return rc;
+  std::vector<unsigned char> buf(n);
+  uint64_t w = 0;
+  rc = integrator_checkpoint_save(c, buf.data(), n, &w);
+  if (rc) return rc;
+  FILE* f = fopen(path, "wb");
+  if (!f) { llg_set_error(std::string("checkpoint: cannot open ") + path); return LLG_ERR_ARG; }
+  const size_t put = fwrite(buf.data(), 1, w, f);
+  const int cl = fclose(f);
+  if (put != w || cl != 0) { llg_set_error(std::string("checkpoint: short write to ") + path); return LLG_ERR_ARG; }
+  return 0;
+}
+
+int llg_checkpoint_read_file(llg_ctx* c, const char* path) {
+  if (!c || !path) return LLG_ERR_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) { llg_set_error(std::string("checkpoint: cannot open ") + path); return LLG_ERR_ARG; }
+  std::vector<unsigned char> buf;
+  unsigned char chunk[1 << 16];
+  size_t got;
+  while ((got = fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+  fclose(f);
+  return integrator_checkpoint_load(c, buf.data(), buf.size());
 }
 
 int llg_kernel_timer_start(llg_ctx* c, uint32_t family_mask, int32_t max_launches, int32_t stride) {

@@ -131,6 +131,11 @@ struct llg_ctx {
   int timer_n[16] = {};
   int timer_stride = 1;        // time every timer_stride-th launch of a family
   long long timer_seen[16] = {};
+  // test hooks: the inject_rhs_after-th and later RHS evaluations of the
+  // integrator fail on the host (< 0: off); bound on the device-resident
+  // integrator's control ops per call (0: its default)
+  long long inject_rhs_after = -1, inject_rhs_seen = 0;
+  long long ctl_limit = 0;
 };
 
 // ── physics kernels (k_physics.cu) ─────────────────────────────────────

@@ -39,7 +39,9 @@ IC_UNIFORM, IC_HEAD_ON_STRIPES, IC_TWO_DOMAIN, IC_GRAIN_BUMPS, IC_CUSTOM, IC_TWO
 
 CV_CODES = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC", -3: "CV_ERR_FAILURE",
             -4: "CV_CONV_FAILURE", -6: "CV_LSETUP_FAIL", -7: "CV_LSOLVE_FAIL", -8: "CV_RHSFUNC_FAIL",
-            -22: "CV_ILL_INPUT", -27: "CV_TOO_CLOSE", -40: "CV_BAD_STATE"}
+            -22: "CV_ILL_INPUT", -27: "CV_TOO_CLOSE", -40: "CV_BAD_STATE", -100: "LLG_ERR_ARG",
+            -101: "LLG_ERR_CUDA", -102: "LLG_ERR_NOMEM", -103: "LLG_ERR_STATE", -104: "LLG_ERR_TIMEOUT",
+            -105: "LLG_ERR_NOTSUP"}
 
 
 class Params(C.Structure):
@@ -82,6 +84,21 @@ class Stats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CkptInfo(C.Structure):
+    _fields_ = [
+        ("magic", C.c_char * 8), ("version", C.c_uint32), ("header_bytes", C.c_uint32),
+        ("scalar_bytes", C.c_uint32), ("reserved0", C.c_uint32), ("ng", C.c_int32), ("ny", C.c_int32),
+        ("neq", C.c_int64), ("qmax", C.c_int32), ("maxl", C.c_int32), ("classical_gs", C.c_int32),
+        ("mxstep", C.c_int32), ("device_resident", C.c_int32), ("have_setup", C.c_int32),
+        ("rtol", C.c_double), ("atol", C.c_double), ("gamma_setup", C.c_double), ("tn", C.c_double),
+        ("nst", C.c_int64), ("nfe_demag", C.c_int64), ("payload_bytes", C.c_uint64), ("checksum", C.c_uint64),
+        ("params", Params),
+    ]
+
+
+FRAME_TRAJECTORY, FRAME_FINAL = 0, 1
 
 
 class GeomSpec(C.Structure):
@@ -214,6 +231,22 @@ def load(path: str | None = None):
         "llg_batch_integrator_init": (I, [VP, D, P(VP), P(SolverOpts)]),
         "llg_batch_integrate": (I, [VP, D, P(VP), C.c_int32, P(C.c_int32)]),
         "llg_batch_destroy": (None, [VP]),
+        "llg_integrator_record_steps": (I, [VP, C.c_int32]),
+        "llg_integrator_recorded_steps": (I, [VP, P(D), P(C.c_int32), C.c_int32]),
+        "llg_integrator_replay_steps": (I, [VP, P(D), P(C.c_int32), C.c_int32]),
+        "llg_integrator_replay_status": (I, [VP, P(C.c_int32), P(C.c_int64)]),
+        "llg_inject_rhs_failure": (I, [VP, C.c_int64]),
+        "llg_set_control_op_limit": (I, [VP, C.c_int64]),
+        "llg_checkpoint_size": (I, [VP, P(C.c_uint64)]),
+        "llg_checkpoint_save": (I, [VP, VP, C.c_uint64, P(C.c_uint64)]),
+        "llg_checkpoint_load": (I, [VP, VP, C.c_uint64]),
+        "llg_checkpoint_inspect": (I, [VP, C.c_uint64, P(CkptInfo)]),
+        "llg_checkpoint_write_file": (I, [VP, C.c_char_p]),
+        "llg_checkpoint_read_file": (I, [VP, C.c_char_p]),
+        "llg_write_frame": (I, [C.c_char_p, C.c_int32, D, C.c_int32, C.c_int32, P(D), C.c_int32]),
+        "llg_write_frame_device": (I, [VP, C.c_char_p, C.c_int32, D, VP, C.c_int32]),
+        "llg_should_write_frame": (I, [C.c_int64, D, D, C.c_int32, C.c_int32]),
+        "llg_write_aux_files": (I, [C.c_char_p, C.c_int32, C.c_int32, P(D), P(C.c_int32)]),
         "llg_learned_harvest": (I, [VP, C.c_int32, C.c_int32]),
         "llg_learned_num_samples": (I, [VP]),
         "llg_learned_train": (I, [VP, P(TrainOpts), P(D), P(D)]),
@@ -377,6 +410,66 @@ class Context:
         st = Stats()
         _check(self.lib.llg_get_stats(self.h, C.byref(st)), "llg_get_stats")
         return st.as_dict()
+
+    # ── step-sequence record / replay ──
+    def record_steps(self, cap: int):
+        """Record the (h, q) of every accepted step from now on (cap <= 0 stops)."""
+        _check(self.lib.llg_integrator_record_steps(self.h, int(cap)), "llg_integrator_record_steps")
+
+    def recorded_steps(self):
+        n = _check(self.lib.llg_integrator_recorded_steps(self.h, None, None, 0), "llg_integrator_recorded_steps")
+        h = np.zeros(n, np.float64)
+        q = np.zeros(n, np.int32)
+        _check(self.lib.llg_integrator_recorded_steps(self.h, h.ctypes.data_as(C.POINTER(C.c_double)),
+                                                      q.ctypes.data_as(C.POINTER(C.c_int32)), n),
+               "llg_integrator_recorded_steps")
+        return h, q
+
+    def replay_steps(self, h, q):
+        """Make the next run (after integrator_init) take exactly these steps."""
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        q = np.ascontiguousarray(q, dtype=np.int32)
+        _check(self.lib.llg_integrator_replay_steps(self.h, h.ctypes.data_as(C.POINTER(C.c_double)),
+                                                    q.ctypes.data_as(C.POINTER(C.c_int32)), len(h)),
+               "llg_integrator_replay_steps")
+
+    def replay_status(self):
+        pos, forced = C.c_int32(), C.c_int64()
+        _check(self.lib.llg_integrator_replay_status(self.h, C.byref(pos), C.byref(forced)),
+               "llg_integrator_replay_status")
+        return {"position": pos.value, "forced_accepts": forced.value}
+
+    # ── test hooks ──
+    def inject_rhs_failure(self, after: int):
+        _check(self.lib.llg_inject_rhs_failure(self.h, int(after)), "llg_inject_rhs_failure")
+
+    def set_control_op_limit(self, limit: int):
+        _check(self.lib.llg_set_control_op_limit(self.h, int(limit)), "llg_set_control_op_limit")
+
+    # ── checkpoint / restart ──
+    def checkpoint(self) -> np.ndarray:
+        """The integrator's complete state as a byte array (host)."""
+        n = C.c_uint64()
+        _check(self.lib.llg_checkpoint_size(self.h, C.byref(n)), "llg_checkpoint_size")
+        buf = np.zeros(n.value, np.uint8)
+        w = C.c_uint64()
+        _check(self.lib.llg_checkpoint_save(self.h, buf.ctypes.data, n.value, C.byref(w)), "llg_checkpoint_save")
+        return buf[: w.value]
+
+    def restore(self, buf):
+        b = np.ascontiguousarray(buf, dtype=np.uint8)
+        _check(self.lib.llg_checkpoint_load(self.h, b.ctypes.data, b.size), "llg_checkpoint_load")
+
+    def write_checkpoint(self, path):
+        _check(self.lib.llg_checkpoint_write_file(self.h, os.fsencode(path)), "llg_checkpoint_write_file")
+
+    def read_checkpoint(self, path):
+        _check(self.lib.llg_checkpoint_read_file(self.h, os.fsencode(path)), "llg_checkpoint_read_file")
+
+    def write_frame(self, path, t, y, append=True, style=FRAME_TRAJECTORY):
+        """One magnetisation frame of device vector y in the reference's text format."""
+        _check(self.lib.llg_write_frame_device(self.h, os.fsencode(path), int(bool(append)), float(t), _ptr(y),
+                                               int(style)), "llg_write_frame_device")
 
     # ── learned preconditioner ──
     def learned_harvest(self, max_samples: int, stride: int = 1):
@@ -547,6 +640,59 @@ def learned_loss_grad(w, u, m, mask, ewt, x, gamma, want_z=True):
                                      C.byref(loss), fp(grad), fp(z) if want_z else None),
            "llg_learned_loss_grad")
     return loss.value, grad, z
+
+
+def checkpoint_inspect(buf):
+    """Validate a checkpoint blob (header, layout, checksum) without a GPU."""
+    lib = load()
+    b = np.ascontiguousarray(buf, dtype=np.uint8)
+    info = CkptInfo()
+    _check(lib.llg_checkpoint_inspect(b.ctypes.data, b.size, C.byref(info)), "llg_checkpoint_inspect")
+    return info
+
+
+def write_frame(path, t, ng, ny, m3, append=True, style=FRAME_TRAJECTORY):
+    """One magnetisation frame (host SoA array) in the reference's text format."""
+    lib = load()
+    a = np.ascontiguousarray(m3, dtype=np.float64)
+    if a.size != 3 * ng * ny:
+        raise LLGError("write_frame: m3 must hold 3*ng*ny values")
+    _check(lib.llg_write_frame(os.fsencode(path), int(bool(append)), float(t), int(ng), int(ny),
+                               a.ctypes.data_as(C.POINTER(C.c_double)), int(style)), "llg_write_frame")
+
+
+def should_write_frame(iout, t, early_until, early_every, late_every):
+    return bool(_check(load().llg_should_write_frame(int(iout), float(t), float(early_until), int(early_every),
+                                                     int(late_every)), "llg_should_write_frame"))
+
+
+def write_aux_files(directory, ng, ny, w=None, grain_id=None):
+    """mask.txt (window w) and grain_id.txt in the reference's format."""
+    lib = load()
+    wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+    ga = None if grain_id is None else np.ascontiguousarray(grain_id, dtype=np.int32)
+    _check(lib.llg_write_aux_files(os.fsencode(directory), int(ng), int(ny),
+                                   None if wa is None else wa.ctypes.data_as(C.POINTER(C.c_double)),
+                                   None if ga is None else ga.ctypes.data_as(C.POINTER(C.c_int32))),
+           "llg_write_aux_files")
+
+
+def read_frames(path):
+    """Parse a frame file (trajectory or final state): list of (t, nx, ny, m[ncell, 3])."""
+    frames = []
+    with open(path) as f:
+        lines = [ln for ln in f.read().split("\n")]
+    i = 0
+    while i < len(lines):
+        if not lines[i].strip():
+            i += 1
+            continue
+        t, nx, ny = lines[i].split()
+        ncell = (int(nx) // 3) * int(ny)
+        m = np.array([[float(v) for v in lines[i + 1 + k].split()] for k in range(ncell)])
+        frames.append((float(t), int(nx), int(ny), m))
+        i += 1 + ncell
+    return frames
 
 
 def selftest_tcgen05(flags: int) -> float:

@@ -228,6 +228,74 @@ int  llg_integrator_init(llg_ctx* ctx, double t0, const double* d_y0,
 int  llg_integrate(llg_ctx* ctx, double tout, double* d_yout, double* tret);
 int  llg_get_stats(llg_ctx* ctx, llg_stats* st);
 
+/* ── step-sequence record / replay (no counterpart in the reference) ──── *
+ * Two forms of one problem (FP64 and mixed-precision demag, block-Jacobi and
+ * learned preconditioner) that choose their own steps differ by the step
+ * selection as much as by their arithmetic.  Recording keeps the (h, q) of
+ * every accepted step of a run (up to cap; cap <= 0 stops); replaying makes
+ * a fresh run (set after llg_integrator_init, before its first
+ * llg_integrate) take exactly that sequence: step n uses order q_n and size
+ * h_n, the local error test is evaluated but does not reject (the steps it
+ * would have rejected are counted), and a Newton failure retries the same
+ * step with a fresh preconditioner setup, at most twice, then returns
+ * LLG_CV_CONV_FAILURE.  A run that needs more steps than were recorded
+ * returns LLG_ERR_STATE.  Host-driven integrator only (the device-resident
+ * form is bypassed while recording or replaying).                          */
+int  llg_integrator_record_steps(llg_ctx* ctx, int32_t cap);
+/* copies min(n, cap) recorded steps; returns n, the number recorded        */
+int  llg_integrator_recorded_steps(llg_ctx* ctx, double* h, int32_t* q, int32_t cap);
+int  llg_integrator_replay_steps(llg_ctx* ctx, const double* h, const int32_t* q, int32_t n);
+/* steps taken so far and error-test rejections overridden by the replay    */
+int  llg_integrator_replay_status(llg_ctx* ctx, int32_t* position, int64_t* forced_accepts);
+
+/* ── failure injection and bounds for tests (no counterpart in the
+ * reference) ──────────────────────────────────────────────────────────── *
+ * llg_inject_rhs_failure: from the after-th RHS evaluation of ctx's
+ * integrator on (counted from this call; after < 0 switches it off), each
+ * evaluation fails on the host without launching anything, as a reference
+ * callback returning -1 after a launch error (2d_i2/2d_fft.cu:404-410); the
+ * integrator then returns LLG_CV_RHSFUNC_FAIL, as CVODE does.
+ * llg_set_control_op_limit: bound on the control operations of one
+ * llg_integrate call of the device-resident integrator (0: the default
+ * 200·(mxstep + 10)·(maxl + 4)); past it every loop of the step graph
+ * exits and the call returns LLG_ERR_TIMEOUT.                              */
+int  llg_inject_rhs_failure(llg_ctx* ctx, int64_t after);
+int  llg_set_control_op_limit(llg_ctx* ctx, int64_t limit);
+
+/* ── checkpoint / restart (no counterpart in the reference, whose runs are
+ * one CVode loop from t0) ──────────────────────────────────────────────── *
+ * A checkpoint is the integrator's complete state between two
+ * llg_integrate calls: CVODE's scalars (t, h, order, step-size history,
+ * counters, order-selection state) and its device vectors (the Nordsieck
+ * history zn[0..qmax], the last correction, the demag field of the last RHS
+ * and, after a preconditioner setup, the frozen block-Jacobi state).  A
+ * context with the same llg_params and geometry that loads it continues
+ * bit for bit as the saved run would have.  The blob starts with
+ * llg_ckpt_info and carries a checksum; load rejects other grids,
+ * other physics parameters, other builds' layouts and corrupt buffers.
+ * A learned-preconditioner context is not checkpointed (LLG_ERR_NOTSUP;
+ * save its weights with llg_learned_get_weights).                         */
+typedef struct llg_ckpt_info {
+  char     magic[8];             /* "LLGCKPT1"                               */
+  uint32_t version, header_bytes, scalar_bytes, reserved0;
+  int32_t  ng, ny;
+  int64_t  neq;
+  int32_t  qmax, maxl, classical_gs, mxstep, device_resident, have_setup;
+  double   rtol, atol, gamma_setup, tn;
+  int64_t  nst, nfe_demag;
+  uint64_t payload_bytes, checksum;
+  llg_params params;
+} llg_ckpt_info;
+int  llg_checkpoint_size(llg_ctx* ctx, uint64_t* bytes);
+/* host buffer of at least llg_checkpoint_size bytes                        */
+int  llg_checkpoint_save(llg_ctx* ctx, void* h_buf, uint64_t cap, uint64_t* written);
+/* replaces the context's integrator (llg_integrator_init not needed)       */
+int  llg_checkpoint_load(llg_ctx* ctx, const void* h_buf, uint64_t n);
+/* header + checksum validation without a GPU; info may be NULL             */
+int  llg_checkpoint_inspect(const void* h_buf, uint64_t n, llg_ckpt_info* info);
+int  llg_checkpoint_write_file(llg_ctx* ctx, const char* path);
+int  llg_checkpoint_read_file(llg_ctx* ctx, const char* path);
+
 /* ── learned preconditioner (no counterpart in the reference) ──────────── *
  * z = (P_BJ^-1 r + gamma * Net(P_BJ^-1 r; m)) on active cells, Net a 3-layer
  * 3x3 convolution 9 -> 16 -> 16 -> 3 channels without bias or activation
@@ -379,6 +447,28 @@ int llg_default_geom_spec(llg_geom_spec* g);
  *   reference's call order.                                                 */
 int llg_build_geometry(const llg_geom_spec* g, uint8_t* active, double* w,
                        double* msk3, double* nsk3, int32_t* grain_id, double* y0);
+
+/* ── text outputs (the reference's formats) ──────────────────────────── *
+ * Magnetisation frames as the reference writes them (WriteFrame,
+ * 2d_i2/2d_fft.cu:437-455; final state 2d_i2/2d_fft.cu:735-757): a
+ * "%f NX NY" header (NX = 3*ng, the reference's doubles per row), one
+ * "mx my mz" line per cell in row-major order, "%f" lines and a closing
+ * empty line for trajectory frames, "%e" lines for the final state.
+ * append != 0 adds the frame to the file (trajectories hold many frames).  */
+#define LLG_FRAME_TRAJECTORY  0
+#define LLG_FRAME_FINAL       1
+int llg_write_frame(const char* path, int32_t append, double t, int32_t ng, int32_t ny,
+                    const double* h_m3, int32_t style);
+/* The same from a device vector of ctx's grid (copied on ctx's stream).     */
+int llg_write_frame_device(llg_ctx* ctx, const char* path, int32_t append, double t,
+                           const double* d_m3, int32_t style);
+/* ShouldWriteFrame (2d_i2/2d_fft.cu:457-463): 1 when output iout is due.   */
+int llg_should_write_frame(int64_t iout, double t, double early_until, int32_t early_every,
+                           int32_t late_every);
+/* write_aux_files (2d_i3/2d_fft.cu:390-408): dir/mask.txt from the window w
+ * and dir/grain_id.txt, each skipped when its array is NULL.                */
+int llg_write_aux_files(const char* dir, int32_t ng, int32_t ny, const double* h_w,
+                        const int32_t* h_grain_id);
 
 /* KEY=VALUE parser using the sim_config.h / params.mk knob names
  * (configs/sim_config.h); lines or whitespace separated; '#' comments.     */

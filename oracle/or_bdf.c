@@ -189,7 +189,7 @@ static int set_ewt(or_bdf* b, const double* ycur) {
   int bad = 0;
   for (long i = 0; i < n; i++) {
     const double t = b->rtol * fabs(ycur[i]) + b->atol;
-    if (!(t > 0.0)) bad = 1;
+    if (t <= 0.0) bad = 1;   /* a NaN state is left to the WRMS-norm check */
     b->ewt[i] = 1.0 / t;
   }
   return bad ? -1 : 0;

@@ -175,4 +175,4 @@ def test_integrator_flags_nonfinite_state(oracle_lib):
     y0[5] = np.nan
     o.integrator_init(y0, llg.default_solver_opts())
     rc, t, y = o.integrate(0.1)
-    assert rc in (-40, -22, -8, -3, -4)
+    assert rc == -40   # CV_BAD_STATE: the weights of a NaN state are not "non-positive"
