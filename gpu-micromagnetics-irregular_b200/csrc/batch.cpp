@@ -108,6 +108,33 @@ int llg_batch_integrate(llg_batch* b, double tout, double* const* d_yout, int32_
   return first;
 }
 
+int llg_partition_lpt(int32_t n, const double* cost, int32_t nparts, int32_t* part_of, double* load) {
+  if (n < 0 || nparts < 1 || (n > 0 && (!cost || !part_of))) {
+    llg_set_error("llg_partition_lpt: bad argument");
+    return LLG_ERR_ARG;
+  }
+  for (int i = 0; i < n; i++)
+    if (!(cost[i] >= 0.0)) { llg_set_error("llg_partition_lpt: costs must be >= 0"); return LLG_ERR_ARG; }
+  // longest processing time first: items by decreasing cost (ties: lower
+  // index first), each to the part with the smallest load so far (ties:
+  // lower part); deterministic, within 4/3 of the optimal makespan
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+  std::vector<double> ld(nparts, 0.0);
+  for (int k = 0; k < n; k++) {
+    const int i = order[k];
+    int best = 0;
+    for (int r = 1; r < nparts; r++)
+      if (ld[r] < ld[best]) best = r;
+    part_of[i] = best;
+    ld[best] += cost[i];
+  }
+  if (load)
+    for (int r = 0; r < nparts; r++) load[r] = ld[r];
+  return 0;
+}
+
 void llg_batch_destroy(llg_batch* b) {
   if (!b) return;
   for (size_t i = 0; i < b->ctx.size(); i++) {

@@ -231,6 +231,7 @@ def load(path: str | None = None):
         "llg_batch_integrator_init": (I, [VP, D, P(VP), P(SolverOpts)]),
         "llg_batch_integrate": (I, [VP, D, P(VP), C.c_int32, P(C.c_int32)]),
         "llg_batch_destroy": (None, [VP]),
+        "llg_partition_lpt": (I, [C.c_int32, P(D), C.c_int32, P(C.c_int32), P(D)]),
         "llg_integrator_record_steps": (I, [VP, C.c_int32]),
         "llg_integrator_recorded_steps": (I, [VP, P(D), P(C.c_int32), C.c_int32]),
         "llg_integrator_replay_steps": (I, [VP, P(D), P(C.c_int32), C.c_int32]),

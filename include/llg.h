@@ -360,6 +360,15 @@ llg_ctx* llg_batch_ctx(llg_batch* b, int32_t i);
 int      llg_batch_integrator_init(llg_batch* b, double t0, const double* const* d_y0, const llg_solver_opts* o);
 int      llg_batch_integrate(llg_batch* b, double tout, double* const* d_yout, int32_t nthreads, int32_t* rcs);
 void     llg_batch_destroy(llg_batch* b);
+/* Split n independent instances across nparts GPUs (host function, no
+ * counterpart in the reference, which runs one geometry per process):
+ * longest-processing-time bin packing on the given cost estimates —
+ * instances by decreasing cost, each to the least-loaded part so far (ties
+ * to the lower index), deterministic, within 4/3 of the optimal makespan.
+ * part_of[i] receives instance i's part; load (optional, nparts values) the
+ * summed cost per part.  No collective is involved: every rank computes the
+ * same split from the same seeded instance list.                          */
+int      llg_partition_lpt(int32_t n, const double* cost, int32_t nparts, int32_t* part_of, double* load);
 
 /* ── instrumentation ──────────────────────────────────────────────────── */
 /* Kernel families, in this order: RHS, JTV, ARNOLDI (fused Krylov operator),
