@@ -70,13 +70,30 @@ __device__ __forceinline__ void aniso_jac(const DevProblem& P, const double m[3]
   }
 }
 
-__device__ __forceinline__ void llg_torque(const DevProblem& P, const double m[3], const double h[3],
+// Damping of the RHS at column gi: uniform, or ramped up towards the x edges
+// in the absorbing layers (src/slit/2d_slit.cu:297-315, same expression)
+__device__ __forceinline__ double alpha_at(const DevProblem& P, int gi) {
+  if (P.pml_cells <= 0) return P.alpha;
+  const int pml = P.pml_cells;
+  double s = 0.0;
+  if (gi < pml) s = 1.0 - (double)gi / (double)pml;
+  else if (gi >= P.ng - pml) s = (double)(gi - (P.ng - pml)) / (double)pml;
+  return P.alpha + (P.pml_alpha_max - P.alpha) * s * s * s;
+}
+
+// Uniform applied field, plus the soft spin-wave source's value for the
+// current evaluation on its column (x component, src/slit/2d_slit.cu:331-349)
+__device__ __forceinline__ double happ_at(const DevProblem& P, int a, int gi) {
+  return (a == 0 && P.src_on && gi == P.src_col) ? P.happ[0] + P.src_h : P.happ[a];
+}
+
+__device__ __forceinline__ void llg_torque(const DevProblem& P, double alpha, const double m[3], const double h[3],
                                            double g, double out[3]) {
   const double m1 = m[0], m2 = m[1], m3 = m[2], h1 = h[0], h2 = h[1], h3 = h[2];
   const double mh = m1 * h1 + m2 * h2 + m3 * h3;
-  out[0] = g * (P.chg * (m3 * h2 - m2 * h3) + P.alpha * (h1 - mh * m1));
-  out[1] = g * (P.chg * (m1 * h3 - m3 * h1) + P.alpha * (h2 - mh * m2));
-  out[2] = g * (P.chg * (m2 * h1 - m1 * h2) + P.alpha * (h3 - mh * m3));
+  out[0] = g * (P.chg * (m3 * h2 - m2 * h3) + alpha * (h1 - mh * m1));
+  out[1] = g * (P.chg * (m1 * h3 - m3 * h1) + alpha * (h2 - mh * m2));
+  out[2] = g * (P.chg * (m2 * h1 - m1 * h2) + alpha * (h3 - mh * m3));
 }
 
 // (I - gamma*ws*J)^-1 at frozen (m, h); closed form of 2d_i2/precond.cu:186-250

@@ -173,6 +173,10 @@ extern "C" int llg_default_geom_spec(llg_geom_spec* g) {
   g->stripe_left_frac = 0.25; g->stripe_right_frac = 0.75;
   g->two_domain_split_frac = 0.875; g->two_domain_tail_my = -0.0175;
   g->ic_core_mz = 0.95; g->ic_jitter_eps = 0.0;
+  // src/2d_fft/2d_fft.cu:94-120 and src/slit/2d_slit.cu:80-90 defaults
+  g->texture_core_mz = -0.998; g->texture_outer_mz = 0.998; g->texture_width_frac = 0.35; g->texture_eps = 1.0e-12;
+  g->circle_cx_frac = 0.5; g->circle_cy_frac = 0.5; g->circle_r_frac_y = 0.22;
+  g->screen_x_frac = 0.5; g->slit_w_frac = 0.10;
   return 0;
 }
 
@@ -258,6 +262,15 @@ extern "C" int llg_build_geometry(const llg_geom_spec* g, uint8_t* active_out, d
         for (size_t k = 0; k < n; k++) { nsk3[k] = gr[gid[k]].nx; nsk3[n + k] = gr[gid[k]].ny; nsk3[2 * n + k] = gr[gid[k]].nz; }
       break;
     }
+    case LLG_GEOM_SLIT: {   // src/slit/2d_slit.cu:482-486, 541-560
+      const int screen_col = (int)(g->screen_x_frac * (double)ng + 0.5);
+      const int slit_w = (int)(g->slit_w_frac * (double)ny + 0.5);
+      const int lo = ny / 2 - slit_w / 2, hi = lo + slit_w;
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < ng; i++)
+          act[(size_t)j * ng + i] = (i == screen_col && !(j >= lo && j < hi)) ? 0 : 1;
+      break;
+    }
     default:
       return LLG_ERR_ARG;
   }
@@ -331,6 +344,30 @@ extern "C" int llg_build_geometry(const llg_geom_spec* g, uint8_t* active_out, d
             put(k, a / nn, b / nn, cc / nn);
           }
         break;
+      case LLG_IC_NEEL: {   // src/2d_fft/2d_fft.cu:460-463, 533-580
+        const double cx = g->circle_cx_frac * (double)(ng - 1), cy = g->circle_cy_frac * (double)(ny - 1);
+        const double radius = g->circle_r_frac_y * (double)ny;
+        const double core = g->texture_core_mz, outer = g->texture_outer_mz;
+        double width = g->texture_width_frac * radius;
+        if (width < 1.0) width = 1.0;
+        for (int j = 0; j < ny; j++)
+          for (int i = 0; i < ng; i++) {
+            const size_t k = (size_t)j * ng + i;
+            if (!act[k]) continue;
+            const double ddx = (double)i - cx, ddy = (double)j - cy;
+            const double rho = sqrt(ddx * ddx + ddy * ddy);
+            const double u = (rho - radius) / width;
+            const double sw = 0.5 * (1.0 - tanh(u));
+            double mz0 = outer + (core - outer) * sw;
+            if (mz0 > 1.0) mz0 = 1.0;
+            if (mz0 < -1.0) mz0 = -1.0;
+            const double mperp = sqrt(fmax(0.0, 1.0 - mz0 * mz0));
+            double mx0 = 0.0, my0 = 0.0;
+            if (rho > g->texture_eps) { mx0 = mperp * (ddx / rho); my0 = mperp * (ddy / rho); }
+            put(k, mx0, my0, mz0);
+          }
+        break;
+      }
       case LLG_IC_GRAIN_BUMPS: {
         if (gr.empty()) break;
         const double core = g->ic_core_mz, epsn = 0.05;
@@ -480,7 +517,7 @@ extern "C" int llg_parse_config(const char* text, llg_params* p, llg_geom_spec* 
   set["GEOMETRY_KIND"] = enm(&g->geometry_kind, {{"GEOMETRY_BULK", 0}, {"GEOMETRY_HOLE_SQUARE", 1},
                                                  {"GEOMETRY_RING", 2}, {"GEOMETRY_POLYCRYSTAL", 3},
                                                  {"GEOMETRY_CUSTOM", 4}, {"GEOMETRY_ELLIPSE", 5},
-                                                 {"GEOMETRY_ANNULUS", 6}});
+                                                 {"GEOMETRY_ANNULUS", 6}, {"GEOMETRY_SLIT", 7}});
   set["HOLE_CENTER_X_FRAC"] = dbl(&g->hole_center_x_frac);
   set["HOLE_CENTER_Y_FRAC"] = dbl(&g->hole_center_y_frac);
   set["HOLE_RADIUS_FRAC_Y"] = dbl(&g->hole_radius_frac_y);
@@ -499,7 +536,24 @@ extern "C" int llg_parse_config(const char* text, llg_params* p, llg_geom_spec* 
   set["ANNULUS_R_OUT_FRAC"] = dbl(&g->annulus_r_out_frac);
   set["IC_KIND"] = enm(&g->ic_kind, {{"IC_UNIFORM", 0}, {"IC_HEAD_ON_STRIPES", 1}, {"IC_TWO_DOMAIN", 2},
                                      {"IC_GRAIN_BUMPS", 3}, {"IC_CUSTOM", 4}, {"IC_TWO_DOMAIN_X", 5},
-                                     {"IC_VORTEX", 6}});
+                                     {"IC_VORTEX", 6}, {"IC_NEEL", 7}});
+  // Néel texture (src/2d_fft/2d_fft.cu:94-120) and slit knobs (src/slit/2d_slit.cu:80-135)
+  set["TEXTURE_CORE_MZ"] = dbl(&g->texture_core_mz);
+  set["TEXTURE_OUTER_MZ"] = dbl(&g->texture_outer_mz);
+  set["TEXTURE_WIDTH_FRAC"] = dbl(&g->texture_width_frac);
+  set["TEXTURE_EPS"] = dbl(&g->texture_eps);
+  set["CIRCLE_CENTER_X_FRAC"] = dbl(&g->circle_cx_frac);
+  set["CIRCLE_CENTER_Y_FRAC"] = dbl(&g->circle_cy_frac);
+  set["CIRCLE_RADIUS_FRAC_Y"] = dbl(&g->circle_r_frac_y);
+  set["SCREEN_X_FRAC"] = dbl(&g->screen_x_frac);
+  set["SLIT_W_FRAC"] = dbl(&g->slit_w_frac);
+  double src_x_frac = -1.0, drive_freq = -1.0;
+  set["SRC_X_FRAC"] = dbl(&src_x_frac);
+  set["DRIVE_FREQ"] = dbl(&drive_freq);
+  set["H_DRIVE"] = dbl(&p->src_amp);
+  set["RAMP_TIME"] = dbl(&p->src_ramp);
+  set["PML_CELLS"] = i32(&p->pml_cells);
+  set["PML_ALPHA_MAX"] = dbl(&p->pml_alpha_max);
   set["INIT_MX"] = dbl(&g->init_m[0]);
   set["INIT_MY"] = dbl(&g->init_m[1]);
   set["INIT_MZ"] = dbl(&g->init_m[2]);
@@ -549,6 +603,8 @@ extern "C" int llg_parse_config(const char* text, llg_params* p, llg_geom_spec* 
     p->ng = nx_val / 3;
   }
   if (ny_val > 0) p->ny = ny_val;
+  if (src_x_frac >= 0.0) p->src_col = (int32_t)(src_x_frac * (double)p->ng + 0.5);
+  if (drive_freq >= 0.0) p->src_omega = 2.0 * 3.14159265358979323846 * drive_freq;
   g->ng = p->ng;
   g->ny = p->ny;
   if (happ_enable == 0) { p->happ[0] = p->happ[1] = p->happ[2] = 0.0; }

@@ -128,7 +128,7 @@ struct Integrator {
   // learned preconditioner and training-pair harvesting stay on the host path
   bool device_applies() {
     return device_resident && started && classical_gs && maxl <= MAXLL - 1 && !learned_active(c) &&
-           !learned_harvest_wanted(c) && !replay && rec_cap == 0;
+           !learned_harvest_wanted(c) && !replay && rec_cap == 0 && !c->dp.src_on;
   }
   int integrate_device(double tout, double* yout, double* tret) {
     if (!dev) {
@@ -618,6 +618,7 @@ struct Integrator {
     nfe++;
     if (rhs_injected()) return LLG_CV_RHSFUNC_FAIL;
     const double* yc = ycor_zero ? nullptr : ycor;
+    set_source_time(c, tn);
     int r = (ycor_zero && y_ready) ? 0 : fused_lin_normalize(c, zn[0], yc, y);
     y_ready = false;
     if (!r) r = fused_field(c, y);

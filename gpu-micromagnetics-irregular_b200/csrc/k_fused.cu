@@ -115,9 +115,9 @@ __global__ void __launch_bounds__(TX * TY) k_rhs_resid_tile(DevProblem P, const 
   double h[3];
   tile_field(P, T.v[0], threadIdx.x + 1, threadIdx.y + 1, m, msk, nsk, h);
 #pragma unroll
-  for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+  for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
   double o[3];
-  llg_torque(P, m, h, gate_of(P, cell), o);
+  llg_torque(P, alpha_at(P, gi), m, h, gate_of(P, cell), o);
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     const int i = a * n + cell;
@@ -153,8 +153,8 @@ __global__ void k_rhs_resid_compact(DevProblem P, const double* __restrict__ y, 
       double h[3];
       gather_field(P, y, gi, gj, m, msk, nsk, h);
 #pragma unroll
-      for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
-      llg_torque(P, m, h, 1.0, o);
+      for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
+      llg_torque(P, alpha_at(P, gi), m, h, 1.0, o);
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {

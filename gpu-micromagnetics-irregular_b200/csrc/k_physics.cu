@@ -67,9 +67,9 @@ __global__ void __launch_bounds__(TX * TY) k_rhs_tile(DevProblem P, const double
   double h[3];
   tile_field(P, T.v[0], threadIdx.x + 1, threadIdx.y + 1, m, msk, nsk, h);
 #pragma unroll
-  for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+  for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
   double o[3];
-  llg_torque(P, m, h, gate_of(P, cell), o);
+  llg_torque(P, alpha_at(P, gi), m, h, gate_of(P, cell), o);
   ydot[cell] = o[0]; ydot[n + cell] = o[1]; ydot[2 * n + cell] = o[2];
 }
 
@@ -92,9 +92,9 @@ __global__ void k_rhs_compact(DevProblem P, const double* __restrict__ y, const 
     double h[3];
     gather_field(P, y, gi, gj, m, msk, nsk, h);
 #pragma unroll
-    for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+    for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
     double o[3];
-    llg_torque(P, m, h, 1.0, o);
+    llg_torque(P, alpha_at(P, gi), m, h, 1.0, o);
     ydot[cell] = o[0]; ydot[n + cell] = o[1]; ydot[2 * n + cell] = o[2];
   }
 }
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(TX * TY) k_jtv_tile(DevProblem P, const double
   tile_field(P, T.v[0], sx, sy, m, msk, nsk, h);
   if (P.jv_full) {
 #pragma unroll
-    for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+    for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
   }
   double K[3][3];
   aniso_jac(P, m, msk, K);
@@ -154,7 +154,7 @@ __global__ void k_jtv_compact(DevProblem P, const double* __restrict__ v, double
     gather_field(P, y, gi, gj, m, msk, nsk, h);
     if (P.jv_full) {
 #pragma unroll
-      for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+      for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
     }
     double K[3][3];
     aniso_jac(P, m, msk, K);
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const dou
   tile_field(P, T.v[0], threadIdx.x + 1, threadIdx.y + 1, m, msk, nsk, h);
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+    h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
     pm[a * n + cell] = m[a];
     ph[a * n + cell] = h[a];
   }
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
   tile_field(P, T.v[0], sx, sy, m, msk, nsk, h);
   if (P.jv_full) {
 #pragma unroll
-    for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + P.happ[a];
+    for (int a = 0; a < 3; a++) h[a] = h[a] + hd[a * n + cell] + happ_at(P, a, gi);
   }
   double K[3][3];
   aniso_jac(P, m, msk, K);
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
       tile_field(P, Y, sx, sy, m, msk, nsk, h);
       if (P.jv_full) {
 #pragma unroll
-        for (int a = 0; a < 3; a++) h[a] = h[a] + C[a * AP_CELLS + tid] + P.happ[a];
+        for (int a = 0; a < 3; a++) h[a] = h[a] + C[a * AP_CELLS + tid] + happ_at(P, a, P.src_on ? cell % P.ng : -1);
       }
       double K[3][3];
       aniso_jac(P, m, msk, K);
@@ -584,7 +584,7 @@ int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* o
 }
 
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot) {
-  (void)t;
+  set_source_time(c, t);
   int rc = launch_normalize(c, y);
   if (rc) return rc;
   if (c->demag) {   // (without demag the field buffer stays as cleared at creation)

@@ -40,6 +40,10 @@ int integrator_checkpoint_save(llg_ctx* c, void* buf, uint64_t cap, uint64_t* wr
 int integrator_checkpoint_load(llg_ctx* c, const void* buf, uint64_t n);
 void learned_destroy(Learned* l);
 
+void set_source_time(llg_ctx* c, double t) {
+  if (c->dp.src_on) c->dp.src_h = llg_source_value(&c->p, t);
+}
+
 static void sync_dp(llg_ctx* c) {
   DevProblem& d = c->dp;
   const llg_params& p = c->p;
@@ -55,6 +59,10 @@ static void sync_dp(llg_ctx* c) {
   double n0[3] = {0, 0, 0};
   if (c->demag) demag_self(c, n0);
   for (int a = 0; a < 3; a++) d.n0[a] = n0[a];
+  d.src_on = (p.src_amp != 0.0 && p.src_col >= 0 && p.src_col < p.ng) ? 1 : 0;
+  d.src_col = d.src_on ? p.src_col : -1;
+  d.pml_cells = p.pml_cells > 0 ? p.pml_cells : 0;
+  d.pml_alpha_max = p.pml_alpha_max;
   d.act = c->d_act;
   d.w = c->d_w;
   d.msk3 = c->d_msk3;
@@ -75,7 +83,9 @@ static int validate(const llg_params* p) {
   if (p->demag_precision != LLG_DEMAG_FP64 && p->demag_precision != LLG_DEMAG_MIXED) { llg_set_error("bad demag_precision"); return LLG_ERR_ARG; }
   if (p->windowed && p->exec_model != LLG_EXEC_YMSK) { llg_set_error("windowed runs use the full-grid execution model"); return LLG_ERR_ARG; }
   if (p->jv_mode != LLG_JV_REFERENCE && p->jv_mode != LLG_JV_FULL_FIELD) { llg_set_error("bad jv_mode"); return LLG_ERR_ARG; }
-  const double vals[] = {p->che, p->chk, p->cha, p->chb, p->alpha, p->chg, p->demag_strength};
+  if (p->pml_cells < 0 || 2LL * p->pml_cells > p->ng) { llg_set_error("pml_cells must be 0..ng/2"); return LLG_ERR_ARG; }
+  const double vals[] = {p->che, p->chk, p->cha, p->chb, p->alpha, p->chg, p->demag_strength,
+                         p->src_amp, p->src_omega, p->src_ramp, p->pml_alpha_max};
   for (double v : vals)
     if (!isfinite(v)) { llg_set_error("non-finite physics constant"); return LLG_ERR_ARG; }
   return 0;
@@ -125,6 +135,17 @@ int llg_default_params(llg_params* p) {
   p->demag_strength = 0.0;
   p->demag_thick = 1.0;
   return 0;
+}
+
+// smoothstep ramp of the source amplitude (src/slit/2d_slit.cu:236-240)
+double llg_source_value(const llg_params* p, double t) {
+  if (!p || p->src_amp == 0.0 || p->src_col < 0 || p->src_col >= p->ng) return 0.0;
+  double ramp = 1.0;
+  if (p->src_ramp > 0.0 && t < p->src_ramp) {
+    const double x = t / p->src_ramp;
+    ramp = x * x * (3.0 - 2.0 * x);
+  }
+  return p->src_amp * ramp * sin(p->src_omega * t);
 }
 
 int llg_default_solver_opts(llg_solver_opts* o) {
@@ -291,19 +312,21 @@ int llg_rhs(llg_ctx* c, double t, double* d_y, double* d_ydot) {
 }
 
 int llg_jtv(llg_ctx* c, const double* d_v, double* d_Jv, double t, const double* d_y, const double* d_fy) {
-  (void)t; (void)d_fy;
+  (void)d_fy;
   int rc = ready(c);
   if (rc) return rc;
   if (!d_v || !d_Jv || !d_y) return LLG_ERR_ARG;
+  set_source_time(c, t);
   return launch_jtv(c, d_v, d_Jv, d_y) ? LLG_ERR_LAUNCH : 0;
 }
 
 int llg_psetup(llg_ctx* c, double t, const double* d_y, const double* d_fy, int jok, int* jcur, double gamma) {
-  (void)t; (void)d_fy; (void)jok;
+  (void)d_fy; (void)jok;
   int rc = ready(c);
   if (rc) return rc;
   if (!d_y) return LLG_ERR_ARG;
   if (jcur) *jcur = 1;
+  set_source_time(c, t);
   return launch_psetup(c, d_y, gamma) ? LLG_ERR_LAUNCH : 0;
 }
 

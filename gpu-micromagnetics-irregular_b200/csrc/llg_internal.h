@@ -68,6 +68,9 @@ struct DevProblem {
   double che, chk, cha, chb, alpha, chg;
   double msk[3], nsk[3], happ[3];
   double n0[3];    // strength-scaled N(0) diagonal
+  int src_on, src_col, pml_cells, pad0;
+  double src_h;          // soft-source field of the current evaluation (set per RHS call)
+  double pml_alpha_max;
   const uint8_t* act;    // nullptr: all active
   const double* w;       // windowed
   const double* msk3;    // windowed
@@ -154,6 +157,9 @@ int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* o
                       const double* y, double gamma, int scale_out = 1, const DevArgs* da = nullptr,
                       const double* in_a = nullptr);
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot);
+// value of the soft source at t into c->dp.src_h (the field the next RHS,
+// residual and setup launches add at the source column)
+void set_source_time(llg_ctx* c, double t);
 
 // ── demag (k_demag.cu) ─────────────────────────────────────────────────
 int demag_create(llg_ctx* c);

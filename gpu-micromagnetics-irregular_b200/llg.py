@@ -34,8 +34,8 @@ DEMAG_FP64, DEMAG_MIXED = 0, 1
 JV_REFERENCE, JV_FULL_FIELD = 0, 1
 GS_AUTO, GS_CLASSICAL, GS_MODIFIED = 0, 1, 2
 PREC_BLOCK_JACOBI, PREC_LEARNED = 0, 1
-GEOM_BULK, GEOM_HOLE_SQUARE, GEOM_RING, GEOM_POLYCRYSTAL, GEOM_CUSTOM, GEOM_ELLIPSE, GEOM_ANNULUS = range(7)
-IC_UNIFORM, IC_HEAD_ON_STRIPES, IC_TWO_DOMAIN, IC_GRAIN_BUMPS, IC_CUSTOM, IC_TWO_DOMAIN_X, IC_VORTEX = range(7)
+GEOM_BULK, GEOM_HOLE_SQUARE, GEOM_RING, GEOM_POLYCRYSTAL, GEOM_CUSTOM, GEOM_ELLIPSE, GEOM_ANNULUS, GEOM_SLIT = range(8)
+IC_UNIFORM, IC_HEAD_ON_STRIPES, IC_TWO_DOMAIN, IC_GRAIN_BUMPS, IC_CUSTOM, IC_TWO_DOMAIN_X, IC_VORTEX, IC_NEEL = range(8)
 
 CV_CODES = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC", -3: "CV_ERR_FAILURE",
             -4: "CV_CONV_FAILURE", -6: "CV_LSETUP_FAIL", -7: "CV_LSOLVE_FAIL", -8: "CV_RHSFUNC_FAIL",
@@ -54,6 +54,8 @@ class Params(C.Structure):
         ("chb", C.c_double), ("alpha", C.c_double), ("chg", C.c_double),
         ("msk", C.c_double * 3), ("nsk", C.c_double * 3), ("happ", C.c_double * 3),
         ("demag_strength", C.c_double), ("demag_thick", C.c_double),
+        ("src_col", C.c_int32), ("pml_cells", C.c_int32), ("src_amp", C.c_double), ("src_omega", C.c_double),
+        ("src_ramp", C.c_double), ("pml_alpha_max", C.c_double),
     ]
 
 
@@ -116,6 +118,9 @@ class GeomSpec(C.Structure):
         ("init_random_eps", C.c_double), ("stripe_left_frac", C.c_double),
         ("stripe_right_frac", C.c_double), ("two_domain_split_frac", C.c_double),
         ("two_domain_tail_my", C.c_double), ("ic_core_mz", C.c_double), ("ic_jitter_eps", C.c_double),
+        ("texture_core_mz", C.c_double), ("texture_outer_mz", C.c_double), ("texture_width_frac", C.c_double),
+        ("texture_eps", C.c_double), ("circle_cx_frac", C.c_double), ("circle_cy_frac", C.c_double),
+        ("circle_r_frac_y", C.c_double), ("screen_x_frac", C.c_double), ("slit_w_frac", C.c_double),
     ]
 
 
@@ -139,6 +144,27 @@ def default_params(ng, ny, **kw) -> Params:
         else:
             setattr(p, k, v)
     return p
+
+
+def slit_params(ng, ny, **kw) -> Params:
+    """The reference's spin-wave single-slit run (src/slit/2d_slit.cu:69-135):
+    easy axis z (cubic form, k = 0.5), exchange 4, DMI 0.1 along x, alpha
+    0.005 with 20-cell absorbing layers ramping to 0.5 at the x edges, a soft
+    source h_x = 0.1 ramp(t) sin(2 pi 0.12 t) (30-unit smoothstep ramp) on
+    column 0.25 ng, periodic neighbours and periodic FFT demag of strength 1,
+    regularised normalisation.  Pair it with GEOM_SLIT and m0 = (0, 0, 1)."""
+    base = dict(bc=BC_PERIODIC, norm_kind=NORM_REG, aniso_kind=ANISO_CUBIC, che=4.0, chk=0.5, chb=0.1,
+                alpha=0.005, chg=1.0, msk=(0.0, 0.0, 1.0), nsk=(1.0, 0.0, 0.0), happ=(0.0, 0.0, 0.0),
+                demag_mode=DEMAG_PERIODIC, demag_strength=1.0, demag_thick=1.0,
+                src_col=int(0.25 * ng + 0.5), src_amp=0.10, src_omega=2.0 * 3.14159265358979323846 * 0.12,
+                src_ramp=30.0, pml_cells=20, pml_alpha_max=0.5)
+    base.update(kw)
+    return default_params(ng, ny, **base)
+
+
+def source_value(params: Params, t: float) -> float:
+    """The soft source's field at time t (0 when inactive)."""
+    return float(load().llg_source_value(C.byref(params), float(t)))
 
 
 def default_solver_opts(**kw) -> SolverOpts:
@@ -167,6 +193,9 @@ def default_geom(ng, ny, **kw) -> GeomSpec:
     g.stripe_left_frac, g.stripe_right_frac = 0.25, 0.75
     g.two_domain_split_frac, g.two_domain_tail_my = 0.875, -0.0175
     g.ic_core_mz, g.ic_jitter_eps = 0.95, 0.0
+    g.texture_core_mz, g.texture_outer_mz, g.texture_width_frac, g.texture_eps = -0.998, 0.998, 0.35, 1e-12
+    g.circle_cx_frac, g.circle_cy_frac, g.circle_r_frac_y = 0.5, 0.5, 0.22
+    g.screen_x_frac, g.slit_w_frac = 0.5, 0.10
     for k, v in kw.items():
         if k == "init_m":
             g.init_m[:] = v
@@ -218,6 +247,7 @@ def load(path: str | None = None):
         "llg_integrate": (I, [VP, D, VP, P(D)]),
         "llg_get_stats": (I, [VP, P(Stats)]),
         "llg_default_geom_spec": (I, [P(GeomSpec)]),
+        "llg_source_value": (D, [P(Params), D]),
         "llg_build_geometry": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
         "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
         "llg_selftest_tcgen05": (I, [I, P(D)]),

@@ -115,6 +115,20 @@ typedef struct llg_params {
   double  happ[3];         /* uniform applied field                               */
   double  demag_strength;  /* DEMAG_STRENGTH                                      */
   double  demag_thick;     /* DEMAG_THICK                                         */
+  /* spin-wave soft source and absorbing edge layers (src/slit/2d_slit.cu:
+   * 80-135, 236-240, 297-340): h_x += src_amp · ramp(t) · sin(src_omega t) on
+   * column src_col (ramp: smoothstep over src_ramp, 1 after it), active when
+   * src_amp != 0 and 0 <= src_col < ng; in the pml_cells columns next to each
+   * x edge the damping of the RHS rises as alpha + (pml_alpha_max - alpha)
+   * s^3, s = 1 at the edge and 0 inside (off when pml_cells = 0).  Jv and the
+   * block-Jacobi preconditioner use the uniform alpha, as the reference's
+   * slit Jacobian does (src/slit/jtv.cu:48).                               */
+  int32_t src_col;         /* source column (SRC_X_FRAC · ng + 0.5)              */
+  int32_t pml_cells;       /* PML_CELLS                                           */
+  double  src_amp;         /* H_DRIVE                                             */
+  double  src_omega;       /* 2π DRIVE_FREQ                                       */
+  double  src_ramp;        /* RAMP_TIME                                           */
+  double  pml_alpha_max;   /* PML_ALPHA_MAX                                       */
 } llg_params;
 
 /* ── integrator options ───────────────────────────────────────────────── */
@@ -412,6 +426,7 @@ int  llg_selftest_tcgen05(int flags, double* max_rel_err);
 #define LLG_GEOM_CUSTOM       4   /* caller builds the arrays              */
 #define LLG_GEOM_ELLIPSE      5   /* GEOMETRY_ELLIPSE (2d_i6)              */
 #define LLG_GEOM_ANNULUS      6   /* circular ring r_in..r_out (no reference twin) */
+#define LLG_GEOM_SLIT         7   /* screen column with a slit (src/slit/2d_slit.cu:482-560) */
 
 #define LLG_IC_UNIFORM        0   /* IC_UNIFORM                            */
 #define LLG_IC_HEAD_ON_STRIPES 1  /* IC_HEAD_ON_STRIPES (2d_i1)            */
@@ -420,6 +435,7 @@ int  llg_selftest_tcgen05(int flags, double* max_rel_err);
 #define LLG_IC_CUSTOM         4
 #define LLG_IC_TWO_DOMAIN_X   5   /* +x left half, −x right half (no reference twin) */
 #define LLG_IC_VORTEX         6   /* (−y, x, 0.1)/norm about the centre (no reference twin) */
+#define LLG_IC_NEEL           7   /* Néel-like circular texture (src/2d_fft/2d_fft.cu:533-580) */
 
 typedef struct llg_geom_spec {
   int32_t ng, ny;
@@ -446,9 +462,19 @@ typedef struct llg_geom_spec {
   double  two_domain_split_frac, two_domain_tail_my;
   double  ic_core_mz;
   double  ic_jitter_eps;          /* U(±eps) on every component, then |m|=1  */
+  /* Néel texture: mz from core to outer across a tanh wall of width
+   * width_frac · radius (>= 1 cell) at radius r_frac_y · ny about
+   * (cx_frac (ng-1), cy_frac (ny-1)); in-plane part radial             */
+  double  texture_core_mz, texture_outer_mz, texture_width_frac, texture_eps;
+  double  circle_cx_frac, circle_cy_frac, circle_r_frac_y;
+  /* slit: screen at column (int)(screen_x_frac ng + 0.5), inactive except
+   * the slit_w = (int)(slit_w_frac ny + 0.5) rows from ny/2 - slit_w/2     */
+  double  screen_x_frac, slit_w_frac;
 } llg_geom_spec;
 
 int llg_default_geom_spec(llg_geom_spec* g);
+/* The soft source's field at time t for parameters p (0 when inactive).    */
+double llg_source_value(const llg_params* p, double t);
 /* Fills the arrays that are non-NULL:
  *   active[ncell] (1 active / 0 hole), w[ncell], msk3[3*ncell], nsk3[3*ncell],
  *   grain_id[ncell], y0[3*ncell].  Returns the number of active cells (≥0)

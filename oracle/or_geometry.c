@@ -12,6 +12,8 @@
  *   IC stripes      2d_i1/2d_fft.cu:540-541, 625-657
  *   IC two-domain   2d_i4/2d_fft.cu:562-595
  *   IC grain bumps  2d_i3/2d_fft.cu:916-984
+ *   slit screen     src/slit/2d_slit.cu:482-486, 541-560
+ *   IC Néel texture src/2d_fft/2d_fft.cu:460-463, 533-580
  * Random numbers come from the C library srand/rand in the reference's
  * call order, so the same seed gives the same geometry and state.
  */
@@ -145,6 +147,17 @@ int or_build_geometry(const llg_geom_spec* g, uint8_t* active_out, double* w_out
         }
       break;
     }
+    case LLG_GEOM_SLIT: {
+      const int screen_col = (int)(g->screen_x_frac * (double)ng + 0.5);
+      const int slit_w = (int)(g->slit_w_frac * (double)ny + 0.5);
+      const int lo = ny / 2 - slit_w / 2, hi = lo + slit_w;
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < ng; i++) {
+          const int in_screen = (i == screen_col) && !((j >= lo) && (j < hi));
+          act[(long)j * ng + i] = in_screen ? 0 : 1;
+        }
+      break;
+    }
     case LLG_GEOM_POLYCRYSTAL: {
       const int NG = g->num_grains;
       if (NG <= 0) { free(act); free(w); free(gid); return LLG_ERR_ARG; }
@@ -268,6 +281,29 @@ int or_build_geometry(const llg_geom_spec* g, uint8_t* active_out, double* w_out
             const double nn = sqrt(mx0 * mx0 + my0 * my0 + mz0 * mz0);
             mx0 /= nn; my0 /= nn; mz0 /= nn;
             y0[cell] = mx0; y0[n + cell] = my0; y0[2 * n + cell] = mz0;
+          }
+        break;
+      }
+      case LLG_IC_NEEL: {
+        const double cx = g->circle_cx_frac * (double)(ng - 1);
+        const double cy = g->circle_cy_frac * (double)(ny - 1);
+        const double radius = g->circle_r_frac_y * (double)ny;
+        double width = g->texture_width_frac * radius;
+        if (width < 1.0) width = 1.0;
+        for (int j = 0; j < ny; j++)
+          for (int i = 0; i < ng; i++) {
+            const long cell = (long)j * ng + i;
+            if (!act[cell]) continue;
+            const double ddx = (double)i - cx, ddy = (double)j - cy;
+            const double rho = sqrt(ddx * ddx + ddy * ddy);
+            const double s = 0.5 * (1.0 - tanh((rho - radius) / width));
+            double mz0 = g->texture_outer_mz + (g->texture_core_mz - g->texture_outer_mz) * s;
+            if (mz0 > 1.0) mz0 = 1.0;
+            if (mz0 < -1.0) mz0 = -1.0;
+            const double mperp = sqrt(fmax(0.0, 1.0 - mz0 * mz0));
+            y0[cell] = (rho > g->texture_eps) ? mperp * (ddx / rho) : 0.0;
+            y0[n + cell] = (rho > g->texture_eps) ? mperp * (ddy / rho) : 0.0;
+            y0[2 * n + cell] = mz0;
           }
         break;
       }

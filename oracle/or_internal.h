@@ -25,6 +25,7 @@ struct or_ctx {
   double* nsk3;
   double* hd;             /* demag field of the last or_rhs call (3*ncell)     */
   double* pinv;           /* 9*ncell block-Jacobi inverses                     */
+  double src_h;           /* soft-source field of the last or_rhs call's t      */
   or_demag* dm;
   or_bdf* bdf;
 };

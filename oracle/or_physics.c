@@ -10,6 +10,8 @@
  *                 2d_i6/2d_i6.cu:250-343 (compact: inactive entries zeroed)
  *                 2d_i3/2d_fft.cu:451-627 (windowed neighbours w·m, per-cell
  *                 axes, output gated by w_self)
+ *                 src/slit/2d_slit.cu:236-240, 297-349 (soft source on one
+ *                 column, damping ramped up in the absorbing edge columns)
  *   or_jtv        2d_i2/jtv.cu:49-122, 2d_i1/jtv.cu:43-96, 2d_i6/jtv.cu:47-130
  *   or_psetup     2d_i2/precond.cu:119-251, 2d_i1/precond.cu:108-241
  *   or_psolve     2d_i2/precond.cu:254-285 (z = ymsk · P^-1 r)
@@ -71,6 +73,29 @@ void or_normalize(or_ctx* c, double* y) {
   }
 }
 
+/* Soft source h_x(t) = H ramp(t) sin(omega t), smoothstep ramp
+ * (src/slit/2d_slit.cu:236-240, 331-340).                                 */
+static double source_at(const llg_params* p, double t) {
+  if (p->src_amp == 0.0 || p->src_col < 0 || p->src_col >= p->ng) return 0.0;
+  double ramp = 1.0;
+  if (p->src_ramp > 0.0 && t < p->src_ramp) {
+    const double x = t / p->src_ramp;
+    ramp = x * x * (3.0 - 2.0 * x);
+  }
+  return p->src_amp * ramp * sin(p->src_omega * t);
+}
+
+/* RHS damping of column i: cubic ramp in the absorbing layers
+ * (src/slit/2d_slit.cu:297-315).                                          */
+static double alpha_at(const llg_params* p, int i) {
+  if (p->pml_cells <= 0) return p->alpha;
+  const int pml = p->pml_cells;
+  double s = 0.0;
+  if (i < pml) s = 1.0 - (double)i / (double)pml;
+  else if (i >= p->ng - pml) s = (double)(i - (p->ng - pml)) / (double)pml;
+  return p->alpha + (p->pml_alpha_max - p->alpha) * s * s * s;
+}
+
 /* Local field pieces shared by f, Jv and P.  exch_a = che·Σ4 nbrs,
  * dmi_a = chb·nsk_a·(L + R) (2d_i1/2d_fft.cu:344-360).                    */
 typedef struct { double h[3]; double msk[3]; double nsk[3]; } local_field;
@@ -96,13 +121,17 @@ static void field_at(const or_ctx* c, const double* y, int i, int j, int with_de
     const double L = nbv(c, y, a, i - 1, j), R = nbv(c, y, a, i + 1, j);
     const double U = nbv(c, y, a, i, j - 1), D = nbv(c, y, a, i, j + 1);
     double h = c->p.che * (L + R + U + D) + aniso[a] + c->p.chb * lf->nsk[a] * (L + R);
-    if (with_demag_app) h = h + c->hd[a * n + cell] + c->p.happ[a];
+    if (with_demag_app) {
+      const int src = (a == 0 && c->p.src_amp != 0.0 && c->p.src_col >= 0 && c->p.src_col < c->p.ng &&
+                       i == c->p.src_col);
+      h = h + c->hd[a * n + cell] + (src ? c->p.happ[0] + c->src_h : c->p.happ[a]);
+    }
     lf->h[a] = h;
   }
 }
 
 int or_rhs(or_ctx* c, double t, double* y, double* ydot) {
-  (void)t;
+  c->src_h = source_at(&c->p, t);
   const long n = c->ncell;
   const int ng = c->p.ng, ny = c->p.ny;
   or_normalize(c, y);
@@ -125,9 +154,10 @@ int or_rhs(or_ctx* c, double t, double* y, double* ydot) {
       const double h1 = lf.h[0], h2 = lf.h[1], h3 = lf.h[2];
       const double mh = m1 * h1 + m2 * h2 + m3 * h3;
       const double g = gate_of(c, cell);
-      ydot[cell]         = g * (c->p.chg * (m3 * h2 - m2 * h3) + c->p.alpha * (h1 - mh * m1));
-      ydot[n + cell]     = g * (c->p.chg * (m1 * h3 - m3 * h1) + c->p.alpha * (h2 - mh * m2));
-      ydot[2 * n + cell] = g * (c->p.chg * (m2 * h1 - m1 * h2) + c->p.alpha * (h3 - mh * m3));
+      const double al = alpha_at(&c->p, i);
+      ydot[cell]         = g * (c->p.chg * (m3 * h2 - m2 * h3) + al * (h1 - mh * m1));
+      ydot[n + cell]     = g * (c->p.chg * (m1 * h3 - m3 * h1) + al * (h2 - mh * m2));
+      ydot[2 * n + cell] = g * (c->p.chg * (m2 * h1 - m1 * h2) + al * (h3 - mh * m3));
     }
   }
   return 0;

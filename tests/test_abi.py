@@ -70,6 +70,9 @@ def _cmp_geometry(oracle_lib, spec):
     (llg.GEOM_POLYCRYSTAL, llg.IC_GRAIN_BUMPS, dict(num_grains=24, dead_grain_frac=0.1)),
     (llg.GEOM_POLYCRYSTAL, llg.IC_TWO_DOMAIN_X, dict(num_grains=72, dead_grain_frac=0.16,
                                                      grain_z_bias=1.0, ic_jitter_eps=0.01)),
+    (llg.GEOM_SLIT, llg.IC_UNIFORM, dict(init_m=(0.0, 0.0, 1.0))),
+    (llg.GEOM_BULK, llg.IC_NEEL, dict()),
+    (llg.GEOM_BULK, llg.IC_NEEL, dict(circle_r_frac_y=0.05, texture_width_frac=0.1, ic_jitter_eps=0.01)),
 ])
 @pytest.mark.parametrize("ng,ny", [(64, 40), (37, 23)])
 def test_geometry_builders_match_oracle_exactly(oracle_lib, kind, ic, kw, ng, ny):
@@ -79,7 +82,8 @@ def test_geometry_builders_match_oracle_exactly(oracle_lib, kind, ic, kw, ng, ny
     y = g["y0"].reshape(3, n)
     nrm = np.linalg.norm(y, axis=0)
     act = g["active"].astype(bool)
-    if kind != llg.GEOM_POLYCRYSTAL:
+    if kind != llg.GEOM_POLYCRYSTAL and not (ic == llg.IC_NEEL and not kw.get("ic_jitter_eps")):
+        # (the reference's Néel texture leaves a cell exactly at the centre at (0, 0, mz0), |m| < 1)
         assert np.allclose(nrm[act], 1.0) and np.all(nrm[~act] == 0.0)
 
 
@@ -93,6 +97,48 @@ def test_square_hole_matches_reference_predicate():
     j = np.arange(ny)[:, None]
     ref = ~((np.abs(i - cx) <= hs) & (np.abs(j - cy) <= hs))
     assert np.array_equal(g["active"].reshape(ny, ng).astype(bool), ref)
+
+
+def test_slit_matches_reference_predicate():
+    """src/slit/2d_slit.cu:482-486, 541-560: the screen column is a hole
+    except the slit rows [ny/2 - w/2, ny/2 - w/2 + w), w = (int)(0.1 ny + 0.5)."""
+    ng, ny = 256, 85
+    g = llg.build_geometry(llg.default_geom(ng, ny, geometry_kind=llg.GEOM_SLIT), want=("active",))
+    act = g["active"].reshape(ny, ng).astype(bool)
+    col, w = int(0.5 * ng + 0.5), int(0.1 * ny + 0.5)
+    lo = ny // 2 - w // 2
+    ref = np.ones((ny, ng), bool)
+    ref[:, col] = False
+    ref[lo:lo + w, col] = True
+    assert np.array_equal(act, ref)
+
+
+def test_neel_texture_matches_reference_formula():
+    """src/2d_fft/2d_fft.cu:533-580 restated in numpy: tanh wall between core
+    and outer mz, radial in-plane part."""
+    ng, ny = 48, 40
+    g = llg.build_geometry(llg.default_geom(ng, ny, ic_kind=llg.IC_NEEL), want=("y0",))
+    cx, cy, r = 0.5 * (ng - 1), 0.5 * (ny - 1), 0.22 * ny
+    width = max(1.0, 0.35 * r)
+    i, j = np.meshgrid(np.arange(ng), np.arange(ny))
+    dx, dy = i - cx, j - cy
+    rho = np.hypot(dx, dy)
+    mz = np.clip(0.998 + (-0.998 - 0.998) * 0.5 * (1 - np.tanh((rho - r) / width)), -1, 1)
+    mp = np.sqrt(np.maximum(0, 1 - mz * mz))
+    y = g["y0"].reshape(3, ny, ng)
+    assert np.allclose(y[2], mz, rtol=0, atol=1e-15)
+    assert np.allclose(y[0], mp * (dx / rho), rtol=0, atol=1e-13)   # sqrt(1 - mz^2) amplifies tanh ulps
+    assert np.allclose(y[1], mp * (dy / rho), rtol=0, atol=1e-13)
+
+
+def test_source_value_smoothstep():
+    """src/slit/2d_slit.cu:236-240, 331-340: H ramp(t) sin(omega t)."""
+    p = llg.slit_params(128, 64)
+    for t in (0.0, 7.5, 29.0, 30.0, 55.0):
+        x = min(t / 30.0, 1.0)
+        ramp = 1.0 if t >= 30.0 else x * x * (3 - 2 * x)
+        assert abs(llg.source_value(p, t) - 0.1 * ramp * np.sin(2 * np.pi * 0.12 * t)) <= 1e-15
+    assert llg.source_value(llg.default_params(16, 8), 5.0) == 0.0
 
 
 def test_polycrystal_window_large_grid_fast(oracle_lib):
@@ -122,6 +168,21 @@ def test_parse_config_reference_knob_names(llg_lib):
     assert p.demag_strength == 4.0 and p.demag_mode == llg.DEMAG_OPEN
     assert o.maxl == 5 and o.rtol == 1e-4 and o.maxord == 5
     assert p.aniso_kind == llg.ANISO_CUBIC and p.che == 50.0 and tuple(p.happ) == (-0.2, 0.0, 0.05)
+
+
+def test_parse_config_slit_and_texture_knobs(llg_lib):
+    lib = llg.load()
+    p, g, o = llg.Params(), llg.GeomSpec(), llg.SolverOpts()
+    lib.llg_default_params(C.byref(p))
+    lib.llg_default_geom_spec(C.byref(g))
+    lib.llg_default_solver_opts(C.byref(o))
+    text = (b"NX_VAL=768 NY_VAL=256 GEOMETRY_KIND=GEOMETRY_SLIT SCREEN_X_FRAC=0.5 SLIT_W_FRAC=0.1 "
+            b"SRC_X_FRAC=0.25 DRIVE_FREQ=0.12 H_DRIVE=0.1 RAMP_TIME=30 PML_CELLS=20 PML_ALPHA_MAX=0.5 "
+            b"IC_KIND=IC_NEEL TEXTURE_CORE_MZ=-0.998 CIRCLE_RADIUS_FRAC_Y=0.22")
+    assert lib.llg_parse_config(text, C.byref(p), C.byref(g), C.byref(o)) == 14
+    assert p.ng == 256 and p.src_col == 64 and abs(p.src_omega - 2 * np.pi * 0.12) < 1e-15
+    assert (p.src_amp, p.src_ramp, p.pml_cells, p.pml_alpha_max) == (0.1, 30.0, 20, 0.5)
+    assert g.geometry_kind == llg.GEOM_SLIT and g.ic_kind == llg.IC_NEEL and g.texture_core_mz == -0.998
 
 
 @pytest.mark.parametrize("bad", [b"NX_VAL=1537", b"NOT_A_KNOB=1", b"RTOL_VAL=abc", b"KRYLOV_DIM"])
