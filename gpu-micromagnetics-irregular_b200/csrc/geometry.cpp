@@ -156,6 +156,22 @@ std::vector<double> hole_dist2(const std::vector<uint8_t>& hole, int ng, int ny)
 
 }  // namespace
 
+// Grains of a polycrystal spec in the reference's rand() order (the device
+// builder, k_geometry.cu, takes its sites and axes from here): per grain
+// sx, sy, ax, ay, az, nx, ny, nz and the dead flag.
+int geom_grains(const llg_geom_spec* g, std::vector<double>& d8, std::vector<int>& dead) {
+  if (!g || g->num_grains <= 0) return LLG_ERR_ARG;
+  const std::vector<Grain> gr = make_grains(*g);
+  d8.resize(gr.size() * 8);
+  dead.resize(gr.size());
+  for (size_t k = 0; k < gr.size(); k++) {
+    const double v[8] = {gr[k].sx, gr[k].sy, gr[k].ax, gr[k].ay, gr[k].az, gr[k].nx, gr[k].ny, gr[k].nz};
+    for (int q = 0; q < 8; q++) d8[k * 8 + q] = v[q];
+    dead[k] = gr[k].dead;
+  }
+  return 0;
+}
+
 extern "C" int llg_default_geom_spec(llg_geom_spec* g) {
   if (!g) return LLG_ERR_ARG;
   memset(g, 0, sizeof(*g));

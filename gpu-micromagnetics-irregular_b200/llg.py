@@ -249,6 +249,7 @@ def load(path: str | None = None):
         "llg_default_geom_spec": (I, [P(GeomSpec)]),
         "llg_source_value": (D, [P(Params), D]),
         "llg_build_geometry": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
+        "llg_build_geometry_device": (I, [P(GeomSpec), VP, VP, VP, VP, VP, VP]),
         "llg_parse_config": (I, [C.c_char_p, P(Params), P(GeomSpec), P(SolverOpts)]),
         "llg_selftest_tcgen05": (I, [I, P(D)]),
         "llg_trace_control": (I, [VP, VP, C.c_int32]),
@@ -733,6 +734,26 @@ def selftest_tcgen05(flags: int) -> float:
     err = C.c_double()
     _check(lib.llg_selftest_tcgen05(int(flags), C.byref(err)), "llg_selftest_tcgen05")
     return err.value
+
+
+def build_geometry_device(spec: GeomSpec, stream=None):
+    """Device geometry builder: torch tensors active (uint8), w, msk3, nsk3,
+    grain_id (int32) on the current CUDA device, plus n_active."""
+    import torch
+    lib = load()
+    n = spec.ng * spec.ny
+    dev = torch.device("cuda")
+    out = {"active": torch.empty(n, dtype=torch.uint8, device=dev),
+           "w": torch.empty(n, dtype=torch.float64, device=dev),
+           "msk3": torch.empty(3 * n, dtype=torch.float64, device=dev),
+           "nsk3": torch.empty(3 * n, dtype=torch.float64, device=dev),
+           "grain_id": torch.empty(n, dtype=torch.int32, device=dev)}
+    rc = lib.llg_build_geometry_device(C.byref(spec), *[out[k].data_ptr() for k in ("active", "w", "msk3", "nsk3",
+                                                                                    "grain_id")],
+                                       None if stream is None else stream.cuda_stream)
+    _check(rc, "llg_build_geometry_device")
+    out["n_active"] = rc
+    return out
 
 
 def build_geometry(spec: GeomSpec, want=("active", "w", "msk3", "nsk3", "grain_id", "y0")):

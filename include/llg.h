@@ -505,6 +505,21 @@ int llg_should_write_frame(int64_t iout, double t, double early_until, int32_t e
 int llg_write_aux_files(const char* dir, int32_t ng, int32_t ny, const double* h_w,
                         const int32_t* h_grain_id);
 
+/* The same active flags, window, per-cell axes and grain ids as
+ * llg_build_geometry, built on the device into device buffers (each may be
+ * NULL) on cuda_stream (NULL = legacy default); returns the number of
+ * active cells.  No counterpart in the reference, whose host builders scan
+ * every grain image per cell for the Voronoi partition
+ * (2d_i3/2d_fft.cu:300-315) and every hole cell per cell for the window
+ * (2d_i3/2d_fft.cu:346-371): here one thread per cell finds its grain with
+ * the host's rounding, and the window's hole distances come from an exact
+ * two-pass distance transform.  Grain ids and flags are identical to the
+ * host builder's; the window agrees to the last bits of tanh.  Initial
+ * states stay with llg_build_geometry (they follow the C library's rand()
+ * sequence).                                                              */
+int llg_build_geometry_device(const llg_geom_spec* g, uint8_t* d_active, double* d_w, double* d_msk3,
+                              double* d_nsk3, int32_t* d_grain_id, void* cuda_stream);
+
 /* KEY=VALUE parser using the sim_config.h / params.mk knob names
  * (configs/sim_config.h); lines or whitespace separated; '#' comments.     */
 int llg_parse_config(const char* text, llg_params* p, llg_geom_spec* g,
