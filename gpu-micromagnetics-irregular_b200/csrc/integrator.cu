@@ -128,7 +128,7 @@ struct Integrator {
   // learned preconditioner and training-pair harvesting stay on the host path
   bool device_applies() {
     return device_resident && started && classical_gs && maxl <= MAXLL - 1 && !learned_active(c) &&
-           !learned_harvest_wanted(c) && !replay && rec_cap == 0 && !c->dp.src_on;
+           !learned_harvest_wanted(c) && !replay && rec_cap == 0 && !c->dp.src_on && !c->d_hv;
   }
   int integrate_device(double tout, double* yout, double* tret) {
     if (!dev) {

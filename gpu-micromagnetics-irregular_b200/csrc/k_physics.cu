@@ -127,6 +127,10 @@ __global__ void __launch_bounds__(TX * TY) k_jtv_tile(DevProblem P, const double
   for (int a = 0; a < 3; a++)
     dh_from(P, T.v[1][a][sy][sx - 1], T.v[1][a][sy][sx + 1], T.v[1][a][sy - 1][sx], T.v[1][a][sy + 1][sx], a, K,
             vv, nsk, dh[a]);
+  if (P.jv_hv) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) dh[a] = dh[a] + P.jv_hv[a * n + cell];
+  }
   double o[3];
   jv_cell(P, m, vv, h, dh, gate_of(P, cell), o);
   Jv[cell] = o[0]; Jv[n + cell] = o[1]; Jv[2 * n + cell] = o[2];
@@ -163,6 +167,10 @@ __global__ void k_jtv_compact(DevProblem P, const double* __restrict__ v, double
     for (int a = 0; a < 3; a++)
       dh_from(P, gather_nb(P, v, a, gi - 1, gj), gather_nb(P, v, a, gi + 1, gj), gather_nb(P, v, a, gi, gj - 1),
               gather_nb(P, v, a, gi, gj + 1), a, K, vv, nsk, dh[a]);
+    if (P.jv_hv) {
+#pragma unroll
+      for (int a = 0; a < 3; a++) dh[a] = dh[a] + P.jv_hv[a * n + cell];
+    }
     double o[3];
     jv_cell(P, m, vv, h, dh, 1.0, o);
     Jv[cell] = o[0]; Jv[n + cell] = o[1]; Jv[2 * n + cell] = o[2];
@@ -298,6 +306,10 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
   for (int a = 0; a < 3; a++)
     dh_from(P, T.v[1][a][sy][sx - 1], T.v[1][a][sy][sx + 1], T.v[1][a][sy - 1][sx], T.v[1][a][sy + 1][sx], a, K,
             vv, nsk, dh[a]);
+  if (P.jv_hv) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) dh[a] = dh[a] + P.jv_hv[a * n + cell];
+  }
   const double g = gate_of(P, cell);
   double jv[3];
   jv_cell(P, m, vv, h, dh, g, jv);
@@ -455,6 +467,10 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
 #pragma unroll
       for (int a = 0; a < 3; a++)
         dh_from(P, V[a][sy][sx - 1], V[a][sy][sx + 1], V[a][sy - 1][sx], V[a][sy + 1][sx], a, K, vv, nsk, dh[a]);
+      if (P.jv_hv) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) dh[a] = dh[a] + P.jv_hv[a * (long long)n + cell];
+      }
       double jv[3];
       jv_cell(P, m, vv, h, dh, g, jv);
       double u[3];
@@ -476,6 +492,15 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
     __syncthreads();   // buffer b is refilled by the next iteration's issue
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");   // (only empty groups remain)
+}
+
+// the Arnoldi operator's input vt = (a in) / s, for the demag derivative of
+// LLG_JV_FULL_DEMAG (the same arithmetic as the operator's staging)
+__global__ void k_arnoldi_input(const double* __restrict__ in, const double* __restrict__ s, const double* in_a,
+                                double* __restrict__ vt, long long n3) {
+  const double ain = kscale_of(in_a);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    vt[i] = 1.0 * ((ain * in[i]) / s[i]);
 }
 
 int grid_1d(const llg_ctx* c, long long work, int block) {
@@ -513,14 +538,20 @@ int launch_rhs(llg_ctx* c, const double* y, const double* hd, double* ydot) {
 }
 
 int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y) {
+  DevProblem P = c->dp;
+  if (c->d_hv) {   // LLG_JV_FULL_DEMAG: the demag field of v enters the field derivative
+    const int rc = demag_apply(c, v, c->d_hv);
+    if (rc) return rc;
+    P.jv_hv = c->d_hv;
+  }
   if (c->p.exec_model == LLG_EXEC_COMPACT) {
     const int tot = c->n_active + c->n_inactive;
     LLG_COUNT(KID_JTV);
-    klaunch(k_jtv_compact, grid_1d(c, tot, 256), 256, 0, c->stream, c->dp, v, Jv, y, c->d_hd, c->d_active_ids,
+    klaunch(k_jtv_compact, grid_1d(c, tot, 256), 256, 0, c->stream, P, v, Jv, y, c->d_hd, c->d_active_ids,
                                                                c->n_active, c->d_inactive_ids, c->n_inactive);
   } else {
     LLG_COUNT(KID_JTV);
-    klaunch(k_jtv_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, v, Jv, y, c->d_hd);
+    klaunch(k_jtv_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, P, v, Jv, y, c->d_hd);
   }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
@@ -568,14 +599,24 @@ int arnoldi_setup(llg_ctx* c) {
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out, const double* y,
                       double gamma, int scale_out, const DevArgs* da, const double* in_a) {
   if (!c->have_setup && !da) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
+  DevProblem P = c->dp;
+  if (c->d_hv) {   // LLG_JV_FULL_DEMAG: demag field of the operator's input vt = (a in) / s
+    if (da) { llg_set_error("the demag-derivative Jacobian runs on the host-driven integrator"); return LLG_ERR_NOTSUP; }
+    LLG_COUNT(KID_ELEMWISE);
+    klaunch(k_arnoldi_input, grid_1d(c, c->neq, 256), 256, 0, c->stream, in, ewt, in_a, c->d_vt, (long long)c->neq);
+    LLG_CUDA_TRY(cudaPeekAtLastError());
+    const int rc = demag_apply(c, c->d_vt, c->d_hv);
+    if (rc) return rc;
+    P.jv_hv = c->d_hv;
+  }
   LLG_COUNT(KID_ARNOLDI);
   ktimer_mark(c, KID_ARNOLDI, true);
   if (c->dp.windowed) {
-    klaunch(k_arnoldi_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, in, ewt, out, y, c->d_hd, c->d_pinv,
+    klaunch(k_arnoldi_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, P, in, ewt, out, y, c->d_hd, c->d_pinv,
             gamma, scale_out, da, in_a);
   } else {
     const int jf = c->dp.jv_full ? 1 : 0;
-    klaunch(k_arnoldi_pipe, c->arn_grid[jf], AP_NT, 2 * sizeof(double) * ap_buf_doubles(jf), c->stream, c->dp, in,
+    klaunch(k_arnoldi_pipe, c->arn_grid[jf], AP_NT, 2 * sizeof(double) * ap_buf_doubles(jf), c->stream, P, in,
             ewt, out, y, c->d_hd, c->d_pinv, gamma, scale_out, da, in_a);
   }
   ktimer_mark(c, KID_ARNOLDI, false);

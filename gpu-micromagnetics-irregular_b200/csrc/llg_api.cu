@@ -53,7 +53,8 @@ static void sync_dp(llg_ctx* c) {
   d.bc = p.bc;
   d.aniso = p.aniso_kind;
   d.windowed = p.windowed;
-  d.jv_full = (p.jv_mode == LLG_JV_FULL_FIELD);
+  d.jv_full = (p.jv_mode == LLG_JV_FULL_FIELD || p.jv_mode == LLG_JV_FULL_DEMAG);
+  d.jv_hv = nullptr;
   d.che = p.che; d.chk = p.chk; d.cha = p.cha; d.chb = p.chb; d.alpha = p.alpha; d.chg = p.chg;
   for (int a = 0; a < 3; a++) { d.msk[a] = p.msk[a]; d.nsk[a] = p.nsk[a]; d.happ[a] = p.happ[a]; }
   double n0[3] = {0, 0, 0};
@@ -82,7 +83,7 @@ static int validate(const llg_params* p) {
   if (p->demag_mode != LLG_DEMAG_OFF && !(p->demag_thick > 0.0)) { llg_set_error("demag_thick must be > 0"); return LLG_ERR_ARG; }
   if (p->demag_precision != LLG_DEMAG_FP64 && p->demag_precision != LLG_DEMAG_MIXED) { llg_set_error("bad demag_precision"); return LLG_ERR_ARG; }
   if (p->windowed && p->exec_model != LLG_EXEC_YMSK) { llg_set_error("windowed runs use the full-grid execution model"); return LLG_ERR_ARG; }
-  if (p->jv_mode != LLG_JV_REFERENCE && p->jv_mode != LLG_JV_FULL_FIELD) { llg_set_error("bad jv_mode"); return LLG_ERR_ARG; }
+  if (p->jv_mode < LLG_JV_REFERENCE || p->jv_mode > LLG_JV_FULL_DEMAG) { llg_set_error("bad jv_mode"); return LLG_ERR_ARG; }
   if (p->pml_cells < 0 || 2LL * p->pml_cells > p->ng) { llg_set_error("pml_cells must be 0..ng/2"); return LLG_ERR_ARG; }
   const double vals[] = {p->che, p->chk, p->cha, p->chb, p->alpha, p->chg, p->demag_strength,
                          p->src_amp, p->src_omega, p->src_ramp, p->pml_alpha_max};
@@ -182,6 +183,11 @@ int llg_create(const llg_params* p, llg_ctx** out) {
   if ((rc = reductions_init(c))) return fail(rc);
   if (p->demag_mode != LLG_DEMAG_OFF && p->demag_strength > 0.0) {
     if ((rc = demag_create(c))) return fail(rc);
+    if (p->jv_mode == LLG_JV_FULL_DEMAG &&
+        (cudaMalloc(&c->d_hv, v3) != cudaSuccess || cudaMalloc(&c->d_vt, v3) != cudaSuccess)) {
+      llg_set_error("cudaMalloc of the Jv demag buffers failed");
+      return fail(LLG_ERR_NOMEM);
+    }
   }
   sync_dp(c);
   if ((rc = arnoldi_setup(c))) return fail(rc);
@@ -211,6 +217,8 @@ void llg_destroy(llg_ctx* c) {
   cudaFree(c->d_pm);
   cudaFree(c->d_ph);
   cudaFree(c->d_pinv);
+  cudaFree(c->d_hv);
+  cudaFree(c->d_vt);
   delete c;
 }
 

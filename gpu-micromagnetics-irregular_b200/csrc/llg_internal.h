@@ -71,6 +71,7 @@ struct DevProblem {
   int src_on, src_col, pml_cells, pad0;
   double src_h;          // soft-source field of the current evaluation (set per RHS call)
   double pml_alpha_max;
+  const double* jv_hv;   // LLG_JV_FULL_DEMAG: demag field of the Jv input (set per launch), else null
   const uint8_t* act;    // nullptr: all active
   const double* w;       // windowed
   const double* msk3;    // windowed
@@ -106,6 +107,8 @@ struct llg_ctx {
   double* d_pm = nullptr;    // m at the last psetup (3N)
   double* d_ph = nullptr;    // h at the last psetup (3N)
   double* d_pinv = nullptr;  // (I - gamma_setup J)^-1 per cell at the last psetup, 9 planes (9N)
+  double* d_hv = nullptr;    // LLG_JV_FULL_DEMAG: demag field of the Jv input (3N)
+  double* d_vt = nullptr;    // LLG_JV_FULL_DEMAG: the Arnoldi operator's scaled input (3N)
   double gamma_setup = 0.0;
   int have_setup = 0;
 

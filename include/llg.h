@@ -82,6 +82,9 @@ extern "C" {
 
 #define LLG_JV_REFERENCE     0     /* Jv field without demag/Zeeman (2d_i2/jtv.cu:87-97) */
 #define LLG_JV_FULL_FIELD    1     /* Jv field includes h_demag and h_app          */
+#define LLG_JV_FULL_DEMAG    2     /* full field and the demag derivative N ⊛ (w v),
+                                      which the reference omits (2d_i2/jtv.h:9-13):
+                                      one more demag evaluation per Jv / Arnoldi step */
 
 #define LLG_GS_AUTO          0     /* classical if neq < 500000 (2d_i2/2d_fft.cu:674) */
 #define LLG_GS_CLASSICAL     1

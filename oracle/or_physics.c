@@ -13,6 +13,8 @@
  *                 src/slit/2d_slit.cu:236-240, 297-349 (soft source on one
  *                 column, damping ramped up in the absorbing edge columns)
  *   or_jtv        2d_i2/jtv.cu:49-122, 2d_i1/jtv.cu:43-96, 2d_i6/jtv.cu:47-130
+ *                 (+ the demag derivative the reference omits, 2d_i2/jtv.h:9-13,
+ *                 in LLG_JV_FULL_DEMAG)
  *   or_psetup     2d_i2/precond.cu:119-251, 2d_i1/precond.cu:108-241
  *   or_psolve     2d_i2/precond.cu:254-285 (z = ymsk · P^-1 r)
  *
@@ -176,10 +178,18 @@ static void aniso_jac(const or_ctx* c, const double m[3], const double msk[3], d
   }
 }
 
+/* LLG_JV_FULL_DEMAG: the field derivative also carries the demag term
+ * N ⊛ (w v) (strength-scaled), the part the reference's Jv omits
+ * (2d_i2/jtv.h:9-13); h is the full field as in LLG_JV_FULL_FIELD.          */
 int or_jtv(or_ctx* c, const double* v, double* Jv, const double* y) {
   const long n = c->ncell;
   const int ng = c->p.ng, ny = c->p.ny;
-  const int full = (c->p.jv_mode == LLG_JV_FULL_FIELD);
+  const int full = (c->p.jv_mode == LLG_JV_FULL_FIELD || c->p.jv_mode == LLG_JV_FULL_DEMAG);
+  double* hv = NULL;
+  if (c->p.jv_mode == LLG_JV_FULL_DEMAG && c->dm) {
+    hv = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    if (!hv || or_demag_run(c, v, hv) != 0) { free(hv); return -1; }
+  }
 #pragma omp parallel for schedule(static)
   for (int j = 0; j < ny; j++) {
     for (int i = 0; i < ng; i++) {
@@ -200,6 +210,7 @@ int or_jtv(or_ctx* c, const double* v, double* Jv, const double* y) {
         const double U = nbv(c, v, a, i, j - 1), D = nbv(c, v, a, i, j + 1);
         const double kv = K[a][0] * vv[0] + K[a][1] * vv[1] + K[a][2] * vv[2];
         dh[a] = c->p.che * (L + R + U + D) + kv + c->p.chb * lf.nsk[a] * (L + R);
+        if (hv) dh[a] = dh[a] + hv[a * n + cell];
       }
       const double h1 = lf.h[0], h2 = lf.h[1], h3 = lf.h[2];
       const double m1 = m[0], m2 = m[1], m3 = m[2];
@@ -213,6 +224,7 @@ int or_jtv(or_ctx* c, const double* v, double* Jv, const double* y) {
       Jv[2 * n + cell] = g * (chg * (v2 * h1 + m2 * dh[0] - v1 * h2 - m1 * dh[1]) + al * (dh[2] - dmh * m3 - mh * v3));
     }
   }
+  free(hv);
   return 0;
 }
 

@@ -86,7 +86,7 @@ def test_rhs_matches_oracle(oracle_lib, gpu, name, ng, ny, pover, gover):
 
 
 @pytest.mark.parametrize("name,ng,ny,pover,gover", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("jv_mode", [llg.JV_REFERENCE, llg.JV_FULL_FIELD])
+@pytest.mark.parametrize("jv_mode", [llg.JV_REFERENCE, llg.JV_FULL_FIELD, llg.JV_FULL_DEMAG])
 def test_jtv_matches_oracle(oracle_lib, gpu, name, ng, ny, pover, gover, jv_mode):
     import torch
     pover = dict(pover, jv_mode=jv_mode)
@@ -103,7 +103,7 @@ def test_jtv_matches_oracle(oracle_lib, gpu, name, ng, ny, pover, gover, jv_mode
     djv = torch.zeros_like(dv)
     ctx.jtv(dv, djv, 0.0, dy)
     torch.cuda.synchronize()
-    tol = 1e-11 if (p.demag_mode != llg.DEMAG_OFF and jv_mode == llg.JV_FULL_FIELD) else 1e-13
+    tol = 1e-11 if (p.demag_mode != llg.DEMAG_OFF and jv_mode != llg.JV_REFERENCE) else 1e-13
     assert rel_err(djv.cpu().numpy(), ref) < tol
 
 
@@ -374,3 +374,73 @@ def test_slit_integration_matches_oracle(oracle_lib, gpu):
     n = p.ng * p.ny
     col = yout.cpu().numpy()[:n].reshape(p.ny, p.ng)[:, p.src_col]
     assert np.abs(col).max() > 1e-3
+
+
+# ── the demag derivative in Jv (LLG_JV_FULL_DEMAG) ──────────────────────────
+@pytest.mark.parametrize("windowed", [0, 1])
+def test_full_demag_jv_is_the_derivative_of_f(oracle_lib, gpu, windowed):
+    """Without normalisation inside f, f is the LLG torque of the full field
+    and LLG_JV_FULL_DEMAG must be its exact derivative: against a central
+    difference (f(y + e v) - f(y - e v)) / 2e the error is O(e^2), while
+    the reference's Jv (no demag term) is off by the demag part."""
+    import torch
+    ng, ny = 48, 40
+    pover = dict(bc=llg.BC_FREE, demag_mode=llg.DEMAG_OPEN, demag_strength=4.0, norm_kind=llg.NORM_NONE,
+                 windowed=windowed)
+    gover = (dict(geometry_kind=llg.GEOM_POLYCRYSTAL, num_grains=8, dead_grain_frac=0.25, ic_jitter_eps=0.05)
+             if windowed else dict(geometry_kind=llg.GEOM_HOLE_SQUARE, hole_radius_frac_y=0.125, ic_jitter_eps=0.05))
+    rng = np.random.default_rng(21)
+    errs = {}
+    for mode in (llg.JV_FULL_DEMAG, llg.JV_FULL_FIELD):
+        p, geo, ctx, o = setup_case(oracle_lib, torch, ng, ny, dict(pover, jv_mode=mode), gover)
+        n = ng * ny
+        y = geo["y0"].copy()
+        v = rng.standard_normal(3 * n) * np.tile(geo["active"], 3) if mode == llg.JV_FULL_DEMAG else v
+        eps = 1e-5
+        fp, fm, f0 = (torch.zeros(3 * n, dtype=torch.float64, device="cuda") for _ in range(3))
+        ctx.rhs(0.0, dev(torch, y + eps * v), fp)
+        ctx.rhs(0.0, dev(torch, y - eps * v), fm)
+        dy = dev(torch, y)
+        ctx.rhs(0.0, dy, f0)   # leaves h_demag(y) for the full field
+        djv = torch.zeros_like(dy)
+        ctx.jtv(dev(torch, v), djv, 0.0, dy)
+        torch.cuda.synchronize()
+        fd = ((fp - fm) / (2 * eps)).cpu().numpy()
+        errs[mode] = rel_err(djv.cpu().numpy(), fd)
+    print(f"windowed={windowed}: |Jv - FD| rel: full demag {errs[llg.JV_FULL_DEMAG]:.2e}, "
+          f"without the demag derivative {errs[llg.JV_FULL_FIELD]:.2e}")
+    assert errs[llg.JV_FULL_DEMAG] < 1e-7
+    assert errs[llg.JV_FULL_FIELD] > 1e-3
+
+
+def test_full_demag_jacobian_integration_matches_oracle(oracle_lib, gpu):
+    """The integrator with the demag derivative in its Krylov operator (one
+    more demag evaluation per Arnoldi step) takes the oracle's step sequence;
+    GMRES iterations per Newton iteration are reported beside the
+    reference's Jacobian."""
+    import torch
+    ng, ny = 64, 48
+    gover = dict(geometry_kind=llg.GEOM_HOLE_SQUARE, hole_radius_frac_y=0.125, ic_jitter_eps=0.01)
+    its = {}
+    for mode in (llg.JV_REFERENCE, llg.JV_FULL_DEMAG):
+        p, geo, ctx, o = setup_case(oracle_lib, torch, ng, ny, dict(bc=llg.BC_FREE, demag_mode=llg.DEMAG_OPEN,
+                                                                     demag_strength=8.0, norm_kind=llg.NORM_REG,
+                                                                     jv_mode=mode), gover)
+        opts = llg.default_solver_opts()
+        y0 = dev(torch, geo["y0"])
+        ctx.integrator_init(0.0, y0, opts)
+        o.integrator_init(geo["y0"], opts)
+        yout = torch.zeros_like(y0)
+        for k in range(1, 11):
+            ctx.integrate(0.1 * k, yout)
+            rc, _, yo = o.integrate(0.1 * k)
+            assert rc == 0
+        torch.cuda.synchronize()
+        a, b = ctx.stats(), o.stats()
+        for key in ("nst", "nfe", "nni", "nli", "netf", "ncfn", "nsetups"):
+            assert a[key] == b[key], (mode, key, a[key], b[key])
+        assert np.abs(yout.cpu().numpy() - yo).max() <= 1e-6
+        its[mode] = a["nli"] / a["nni"]
+    print(f"GMRES iterations per Newton iteration, strength 8: reference Jv {its[llg.JV_REFERENCE]:.3f}, "
+          f"with the demag derivative {its[llg.JV_FULL_DEMAG]:.3f}")
+    assert its[llg.JV_FULL_DEMAG] <= its[llg.JV_REFERENCE] + 1e-12
