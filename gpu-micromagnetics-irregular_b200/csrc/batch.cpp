@@ -10,6 +10,13 @@
 // graph, and every demag plan picks its transform launch shapes by timing
 // (k_demag.cu, autotune; cached per transform size, so instances of one size
 // tune once).
+//
+// llg_batch_integrate_graph is the single-launch form: every instance's
+// device-resident step loop (BDF attempts, Newton and Arnoldi iterations as
+// CUDA graph WHILE / IF nodes driven by control kernels, integrator_dev.cu)
+// is captured as an independent branch of ONE graph, and one cudaGraphLaunch
+// advances all instances to tout; the host only writes each instance's
+// (tout, yout) before the launch and reads its state back after it.
 #include <algorithm>
 #include <atomic>
 #include <numeric>
@@ -23,7 +30,16 @@ struct llg_batch {
   std::vector<llg_ctx*> ctx;
   std::vector<cudaStream_t> streams;
   int device = 0;
+  // single-graph form
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;
+  std::vector<DevInteg*> devs;
 };
+
+int integrator_batch_prepare(llg_ctx* c, DevInteg** d_out, DState* hs_out);
+int integrator_batch_sync(llg_ctx* c);
+int integrator_batch_finish(llg_ctx* c, const DState& hs, double* tret);
+int demag_check_last(llg_ctx* c);
 
 extern "C" {
 
@@ -108,6 +124,71 @@ int llg_batch_integrate(llg_batch* b, double tout, double* const* d_yout, int32_
   return first;
 }
 
+int llg_batch_integrate_graph(llg_batch* b, double tout, double* const* d_yout, int32_t* rcs) {
+  if (!b || !d_yout) return LLG_ERR_ARG;
+  const int n = (int)b->ctx.size();
+  for (int i = 0; i < n; i++)
+    if (b->streams[i] && cudaStreamSynchronize(b->streams[i]) != cudaSuccess) {
+      llg_set_error("llg_batch_integrate_graph: instance stream failed");
+      return LLG_ERR_CUDA;
+    }
+  if (!b->gexec) {
+    std::vector<DState> hs(n);
+    std::vector<DevInteg*> ds(n, nullptr);
+    for (int i = 0; i < n; i++) {
+      const int rc = integrator_batch_prepare(b->ctx[i], &ds[i], &hs[i]);
+      if (rc) {
+        llg_set_error("instance " + std::to_string(i) + ": " + llg_last_error());
+        return rc;
+      }
+    }
+    std::vector<const DState*> hp(n);
+    for (int i = 0; i < n; i++) hp[i] = &hs[i];
+    const int rc = devint_build_batch(b->ctx.data(), ds.data(), hp.data(), n, &b->gexec);
+    if (rc) return rc;
+    b->devs = ds;
+    if (!b->gstream && cudaStreamCreateWithFlags(&b->gstream, cudaStreamNonBlocking) != cudaSuccess) {
+      llg_set_error("llg_batch_integrate_graph: stream creation failed");
+      return LLG_ERR_CUDA;
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    const int rc = integrator_batch_sync(b->ctx[i]);   // after host-path steps: upload the state
+    if (rc) return rc;
+  }
+  for (int i = 0; i < n; i++) {
+    const int rc = devint_batch_args(b->devs[i], b->ctx[i], tout, d_yout[i], b->gstream);
+    if (rc) return rc;
+  }
+  if (cudaGraphLaunch(b->gexec, b->gstream) != cudaSuccess) {
+    llg_set_error("llg_batch_integrate_graph: graph launch failed");
+    return LLG_ERR_CUDA;
+  }
+  for (int i = 0; i < n; i++) {
+    const int rc = devint_batch_fetch(b->devs[i], b->ctx[i], b->gstream);
+    if (rc) return rc;
+  }
+  if (cudaStreamSynchronize(b->gstream) != cudaSuccess) {
+    llg_set_error(std::string("llg_batch_integrate_graph: ") + cudaGetErrorString(cudaGetLastError()));
+    return LLG_ERR_CUDA;
+  }
+  int first = 0;
+  for (int i = 0; i < n; i++) {
+    DState hs;
+    devint_batch_collect(b->devs[i], b->ctx[i], hs);
+    double tret = 0.0;
+    int rc = integrator_batch_finish(b->ctx[i], hs, &tret);
+    const int dc = demag_check_last(b->ctx[i]);
+    if (dc) rc = dc;
+    if (rcs) rcs[i] = rc;
+    if (rc && !first) {
+      first = rc;
+      llg_set_error("instance " + std::to_string(i) + ": step graph returned " + std::to_string(rc));
+    }
+  }
+  return first;
+}
+
 int llg_partition_lpt(int32_t n, const double* cost, int32_t nparts, int32_t* part_of, double* load) {
   if (n < 0 || nparts < 1 || (n > 0 && (!cost || !part_of))) {
     llg_set_error("llg_partition_lpt: bad argument");
@@ -137,6 +218,9 @@ int llg_partition_lpt(int32_t n, const double* cost, int32_t nparts, int32_t* pa
 
 void llg_batch_destroy(llg_batch* b) {
   if (!b) return;
+  if (b->gstream) cudaStreamSynchronize(b->gstream);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->gstream) cudaStreamDestroy(b->gstream);
   for (size_t i = 0; i < b->ctx.size(); i++) {
     if (b->streams[i]) cudaStreamSynchronize(b->streams[i]);
     llg_destroy(b->ctx[i]);

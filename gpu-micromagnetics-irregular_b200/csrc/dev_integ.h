@@ -114,3 +114,12 @@ void devint_destroy(DevInteg* d);
 int devint_upload(DevInteg* d, const DState& hs, llg_ctx* c);
 // one llg_integrate call on the device; the final state comes back in hs
 int devint_run(DevInteg* d, llg_ctx* c, double tout, double* yout, DState& hs);
+// batches (batch.cpp): one graph holding every instance's step loop as an
+// independent branch; per call, set each instance's arguments, launch once,
+// fetch each state, synchronise, collect
+int devint_mark_batched(DevInteg* d);
+int devint_build_batch(llg_ctx* const* cs, DevInteg* const* ds, const DState* const* hss, int n,
+                       cudaGraphExec_t* exec);
+int devint_batch_args(DevInteg* d, llg_ctx* c, double tout, double* yout, cudaStream_t s);
+int devint_batch_fetch(DevInteg* d, llg_ctx* c, cudaStream_t s);
+int devint_batch_collect(DevInteg* d, llg_ctx* c, DState& hs);

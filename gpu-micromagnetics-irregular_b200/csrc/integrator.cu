@@ -1489,3 +1489,54 @@ int integrator_checkpoint_load(llg_ctx* c, const void* buf, uint64_t n) {
   b->ycor_zero = false;
   return 0;
 }
+
+// ── batch graph support (batch.cpp) ─────────────────────────────────────
+// An instance joins a batch graph once its host-driven start is done (the
+// initial step size and first step run on the host) and its settings are
+// covered by the device-resident form.
+int integrator_batch_prepare(llg_ctx* c, DevInteg** d_out, DState* hs_out) {
+  Integrator* b = c->integ;
+  if (!b) { llg_set_error("batch graph: llg_batch_integrator_init first"); return LLG_ERR_STATE; }
+  if (!b->started) {
+    llg_set_error("batch graph: advance the batch once with llg_batch_integrate (host start-up) first");
+    return LLG_ERR_STATE;
+  }
+  const bool dr = b->device_resident;
+  b->device_resident = 1;
+  const bool ok_dev = b->device_applies();
+  b->device_resident = dr;
+  if (!ok_dev) {
+    llg_set_error("batch graph: an instance uses a setting the device-resident step graph does not cover "
+                  "(modified Gram-Schmidt, learned preconditioner, harvesting, replay/recording, a source "
+                  "term or the demag-derivative Jacobian)");
+    return LLG_ERR_NOTSUP;
+  }
+  if (!b->dev) {
+    const int rc = devint_create(c, &b->dev);
+    if (rc) return rc;
+  }
+  devint_mark_batched(b->dev);
+  b->export_state(*hs_out);
+  *d_out = b->dev;
+  return 0;
+}
+
+// the device copy of the state, current (after the graph was built)
+int integrator_batch_sync(llg_ctx* c) {
+  Integrator* b = c->integ;
+  if (b->dev_current) return 0;
+  DState hs;
+  b->export_state(hs);
+  const int rc = devint_upload(b->dev, hs, c);
+  if (rc) return rc;
+  b->dev_current = true;
+  return 0;
+}
+
+int integrator_batch_finish(llg_ctx* c, const DState& hs, double* tret) {
+  Integrator* b = c->integ;
+  b->y_ready = false;
+  b->import_state(hs);
+  *tret = hs.tret;
+  return hs.status;
+}

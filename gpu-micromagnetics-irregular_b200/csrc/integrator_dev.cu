@@ -1103,6 +1103,7 @@ struct DevInteg {
   cudaGraphConditionalHandle hnd[H_COUNT] = {};
   int depth = 0;
   long long neq = 0;
+  bool batched = false;         // its step loop lives in a batch graph (no graph of its own)
 };
 
 namespace {
@@ -1265,18 +1266,17 @@ struct Builder {
   }
 };
 
-int build_graph(DevInteg* d, llg_ctx* c, const DState& hs) {
+// Capture one instance's step loop into graph g as a new independent branch
+// (no dependencies on what g already holds).
+int capture_into(DevInteg* d, llg_ctx* c, const DState& hs, cudaGraph_t g) {
   // the capture runs the host wrappers once; keep what they record on the host
   const double gs_saved = c->gamma_setup;
   const int hv_saved = c->have_setup;
   const long long nd_saved = c->nfe_demag;
   cudaStream_t saved = c->stream;
-  cudaGraph_t g = nullptr;
-  LLG_CUDA_TRY(cudaGraphCreate(&g, 0));
   d->depth = 0;
   cudaError_t e = cudaStreamBeginCaptureToGraph(d->cap[0], g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
   if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
     llg_set_error(std::string("device-resident graph: begin capture: ") + cudaGetErrorString(e));
     return LLG_ERR_CUDA;
   }
@@ -1296,13 +1296,20 @@ int build_graph(DevInteg* d, llg_ctx* c, const DState& hs) {
   c->nfe_demag = nd_saved;
   cudaGraph_t outg = nullptr;
   e = cudaStreamEndCapture(d->cap[0], &outg);
-  if (b.rc) { cudaGraphDestroy(g); return b.rc; }
+  if (b.rc) return b.rc;
   if (e != cudaSuccess) {
-    cudaGraphDestroy(g);
     llg_set_error(std::string("device-resident graph: end capture: ") + cudaGetErrorString(e));
     return LLG_ERR_CUDA;
   }
-  e = cudaGraphInstantiate(&d->exec, g, 0);
+  return 0;
+}
+
+int build_graph(DevInteg* d, llg_ctx* c, const DState& hs) {
+  cudaGraph_t g = nullptr;
+  LLG_CUDA_TRY(cudaGraphCreate(&g, 0));
+  const int rc = capture_into(d, c, hs, g);
+  if (rc) { cudaGraphDestroy(g); return rc; }
+  cudaError_t e = cudaGraphInstantiate(&d->exec, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
     d->exec = nullptr;
@@ -1344,7 +1351,7 @@ void devint_destroy(DevInteg* d) {
 }
 
 int devint_upload(DevInteg* d, const DState& hs_in, llg_ctx* c) {
-  if (!d->exec) {
+  if (!d->exec && !d->batched) {
     const int rc = build_graph(d, c, hs_in);
     if (rc) return rc;
   }
@@ -1370,6 +1377,62 @@ int devint_run(DevInteg* d, llg_ctx* c, double tout, double* yout, DState& hs) {
   LLG_CUDA_TRY(cudaMemcpyAsync(c->h_scal + SLOT_TCERR, c->d_scal + SLOT_TCERR, sizeof(double), cudaMemcpyDeviceToHost,
                                c->stream));
   LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  hs = *d->h_s;
+  g_kcount[KID_OTHER].fetch_add(1, std::memory_order_relaxed);   // k_call_args
+  for (int k = 0; k < KID_COUNT && k < 16; k++) g_kcount[k].fetch_add(hs.kcount[k], std::memory_order_relaxed);
+  c->gamma_setup = hs.da.gamma_setup;
+  c->have_setup = hs.have_setup;
+  c->nfe_demag = hs.nfe_demag;
+  return 0;
+}
+
+// ── batches: the step loops of many instances in ONE graph ───────────────
+// Conditional nodes cannot live in child graphs, so each instance's WHILE /
+// IF structure is captured directly into the shared graph as an independent
+// branch; one cudaGraphLaunch then advances every instance to its tout, the
+// branches running concurrently on the device with no host work between
+// steps.  Each instance keeps its own DState, conditional handles, buffers
+// and capture streams.
+int devint_mark_batched(DevInteg* d) {
+  d->batched = true;
+  return 0;
+}
+
+int devint_build_batch(llg_ctx* const* cs, DevInteg* const* ds, const DState* const* hss, int n,
+                       cudaGraphExec_t* exec) {
+  cudaGraph_t g = nullptr;
+  LLG_CUDA_TRY(cudaGraphCreate(&g, 0));
+  for (int i = 0; i < n; i++) {
+    const int rc = capture_into(ds[i], cs[i], *hss[i], g);
+    if (rc) { cudaGraphDestroy(g); return rc; }
+  }
+  const cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    *exec = nullptr;
+    llg_set_error(std::string("batch graph: instantiate: ") + cudaGetErrorString(e));
+    return LLG_ERR_CUDA;
+  }
+  return 0;
+}
+
+// per call: set tout / yout of one instance on stream s (before the launch)
+int devint_batch_args(DevInteg* d, llg_ctx* c, double tout, double* yout, cudaStream_t s) {
+  k_call_args<<<1, 1, 0, s>>>(d->d_s, tout, yout, c->ctl_limit);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
+
+// per call: bring one instance's state home on stream s (after the launch)
+int devint_batch_fetch(DevInteg* d, llg_ctx* c, cudaStream_t s) {
+  LLG_CUDA_TRY(cudaMemcpyAsync(d->h_s, d->d_s, sizeof(DState), cudaMemcpyDeviceToHost, s));
+  LLG_CUDA_TRY(cudaMemcpyAsync(c->h_scal + SLOT_TCERR, c->d_scal + SLOT_TCERR, sizeof(double), cudaMemcpyDeviceToHost,
+                               s));
+  return 0;
+}
+
+// after the stream synchronised: the instance's final state (as devint_run)
+int devint_batch_collect(DevInteg* d, llg_ctx* c, DState& hs) {
   hs = *d->h_s;
   g_kcount[KID_OTHER].fetch_add(1, std::memory_order_relaxed);   // k_call_args
   for (int k = 0; k < KID_COUNT && k < 16; k++) g_kcount[k].fetch_add(hs.kcount[k], std::memory_order_relaxed);

@@ -262,6 +262,7 @@ def load(path: str | None = None):
         "llg_batch_integrator_init": (I, [VP, D, P(VP), P(SolverOpts)]),
         "llg_batch_integrate": (I, [VP, D, P(VP), C.c_int32, P(C.c_int32)]),
         "llg_batch_destroy": (None, [VP]),
+        "llg_batch_integrate_graph": (I, [VP, D, P(VP), P(C.c_int32)]),
         "llg_partition_lpt": (I, [C.c_int32, P(D), C.c_int32, P(C.c_int32), P(D)]),
         "llg_integrator_record_steps": (I, [VP, C.c_int32]),
         "llg_integrator_recorded_steps": (I, [VP, P(D), P(C.c_int32), C.c_int32]),
@@ -572,6 +573,13 @@ class Batch:
         ptrs = (C.c_void_p * len(youts))(*[_ptr(y) for y in youts])
         rcs = (C.c_int32 * len(youts))()
         _check(self.lib.llg_batch_integrate(self.h, float(tout), ptrs, int(nthreads), rcs), "llg_batch_integrate")
+        return list(rcs)
+
+    def integrate_graph(self, tout, youts):
+        """Every instance to tout in one CUDA graph launch (see llg.h)."""
+        ptrs = (C.c_void_p * len(youts))(*[_ptr(y) for y in youts])
+        rcs = (C.c_int32 * len(youts))()
+        _check(self.lib.llg_batch_integrate_graph(self.h, float(tout), ptrs, rcs), "llg_batch_integrate_graph")
         return list(rcs)
 
     def stats(self):

@@ -377,6 +377,16 @@ llg_ctx* llg_batch_ctx(llg_batch* b, int32_t i);
 int      llg_batch_integrator_init(llg_batch* b, double t0, const double* const* d_y0, const llg_solver_opts* o);
 int      llg_batch_integrate(llg_batch* b, double tout, double* const* d_yout, int32_t nthreads, int32_t* rcs);
 void     llg_batch_destroy(llg_batch* b);
+/* The same step for every instance as ONE CUDA graph launch: each
+ * instance's device-resident step loop (BDF attempts, Newton and Arnoldi
+ * iterations as graph WHILE / IF nodes set by control kernels) is an
+ * independent branch of a single graph, built on the first call.  Every
+ * instance must have advanced once with llg_batch_integrate (the host-side
+ * start-up: initial step size and first step) and use settings the
+ * device-resident form covers (classical Gram-Schmidt, block-Jacobi, no
+ * source term, no recording/replay; LLG_ERR_NOTSUP otherwise).  Either
+ * entry point may be used after the other.                                */
+int      llg_batch_integrate_graph(llg_batch* b, double tout, double* const* d_yout, int32_t* rcs);
 /* Split n independent instances across nparts GPUs (host function, no
  * counterpart in the reference, which runs one geometry per process):
  * longest-processing-time bin packing on the given cost estimates —
