@@ -551,7 +551,10 @@ def run_config4(args, world, rank, local):
     insts = llg.config4_instances(64, 12345)
     mine = shard.my_instances(insts, world, rank)
     part, load = shard.partition_lpt([shard.instance_cost(x["params"]) for x in insts], world)
-    opts = llg.default_solver_opts()
+    # classical Gram-Schmidt for every instance: the single-graph form runs the
+    # device-resident step loop, which covers it (the reference would pick
+    # modified Gram-Schmidt for the 1024x512 instances, neq >= 5e5)
+    opts = llg.default_solver_opts(gs_type=llg.GS_CLASSICAL)
     t0 = time.perf_counter()
     b = llg.Batch([insts[i]["params"] for i in mine])
     y0 = [torch.from_numpy(llg.setup_instance(b.ctx[k], insts[i])).cuda() for k, i in enumerate(mine)]
@@ -561,7 +564,7 @@ def run_config4(args, world, rank, local):
     setup_s = time.perf_counter() - t0
     t = 0.0
 
-    def run(k, nthreads):
+    def run(k, nthreads, graph=False):
         nonlocal t
         torch.cuda.synchronize()
         dist_barrier(world)
@@ -569,21 +572,29 @@ def run_config4(args, world, rank, local):
         e0.record()
         for _ in range(k):
             t += args.dt
-            b.integrate(t, outs, nthreads=nthreads)
+            if graph:
+                b.integrate_graph(t, outs)
+            else:
+                b.integrate(t, outs, nthreads=nthreads)
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    # warm-up: W output intervals of 0.1 (every instance)
+    # warm-up: W output intervals of 0.1 (every instance; the first one is the
+    # host start-up, the next ones build and run the single graph)
     for k in range(args.warmup):
         t += 0.1
-        b.integrate(t, outs, nthreads=0)
+        if k == 0:
+            b.integrate(t, outs, nthreads=0)
+        else:
+            b.integrate_graph(t, outs)
     torch.cuda.synchronize()
     st0 = [s_["nst"] for s_ in b.stats()]
     with Clocks(local) as clk:
-        ms_local = run(args.steps, 0)
+        ms_local = run(args.steps, 0, graph=True)
     ms = dist_max(ms_local, world)
     st1 = [s_["nst"] for s_ in b.stats()]
+    ms_pool = dist_max(run(args.steps, 0), world)
     local_res = {i: {"rank": rank, "nst": int(st1[k]), "nst_timed": int(st1[k] - st0[k]),
                      "m_norm": float(torch.linalg.vector_norm(outs[k]).item())} for k, i in enumerate(mine)}
     merged = shard.gather_results(local_res, world, rank)
@@ -603,11 +614,16 @@ def run_config4(args, world, rank, local):
                                "annulus 0.15-0.35 N, ellipse 0.3x0.2 (compact), polycrystal 24 grains 10% dead "
                                "(windowed)}, open demag U[1,4], rtol 1e-4", "instances": len(insts),
                    "cells_total": cells, "sim_time_per_step": args.dt,
-                   "form": "mixed-precision demag, block-Jacobi",
-                   "parallelism": f"LPT split of the instances over {world} GPU(s), one stream per instance",
+                   "form": "mixed-precision demag, block-Jacobi, classical Gram-Schmidt",
+                   "launch": "every instance's device-resident step loop as one branch of ONE CUDA graph; one graph "
+                             "launch per step advances all instances",
+                   "parallelism": f"LPT split of the instances over {world} GPU(s)",
                    "setup_s": setup_s},
         "split": {"instances_per_rank": [int((part == r).sum()) for r in range(world)],
                   "cost_per_rank": [float(x) for x in load]},
+        "host_driven_thread_pool": {"ms_per_step": ms_pool / args.steps,
+                                    "value": len(insts) * args.steps * args.dt / (ms_pool / 1000.0),
+                                    "note": "the same instances driven from a host thread pool, one stream each"},
         "sequential_same_instances": seq,
         "clocks": clk.summary(),
     }
@@ -615,6 +631,112 @@ def run_config4(args, world, rank, local):
         line["bdf_steps_timed"] = int(sum(v["nst_timed"] for v in merged.values()))
         line["gathered_instances"] = len(merged)
     b.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def harvest_train(ctx, y0, o, t_end, w_init=None, seed=5):
+    """Harvest block-Jacobi SPGMR solves of one instance over [0, t_end] and
+    train on them (continuing from w_init when given)."""
+    import torch
+    if w_init is not None:
+        ctx.learned_set_weights(w_init)
+    ctx.learned_harvest(TRAIN["max_samples"], TRAIN["stride"])
+    ctx.integrator_init(0.0, y0, o)
+    yout = torch.zeros_like(y0)
+    for k in range(1, int(round(t_end / 0.1)) + 1):
+        ctx.integrate(0.1 * k, yout)
+    l0, l1 = ctx.learned_train(iters=TRAIN["iters"], batch=TRAIN["batch"], patch=TRAIN["patch"], seed=seed,
+                               lr=TRAIN["lr"], init_scale=TRAIN["init_scale"])
+    return ctx.learned_get_weights(), {"samples": ctx.learned_num_samples(), "loss_first": l0, "loss_last": l1}
+
+
+def run_config3(args, world, rank, local):
+    """The compact-circle workload with the learned preconditioner: 2048x2048
+    cells, EXEC_COMPACT active-index lists of the centred circle r = 0.25 N
+    (19.6 % active), periodic FFT demag of strength 2 (the reference's
+    un-padded convention), vortex state (-y, x, 0.1)/norm + 0.01 jitter,
+    mixed-precision demag, rtol 1e-4, SPGMR(5).  The network is trained on
+    solves harvested from the square-hole film (1536x512, open demag 4) and
+    then the 72-grain polycrystal (1536x512, windowed demag 1); the circle is
+    then integrated over t 0 -> --steps * --dt with block-Jacobi, with the
+    learned preconditioner on every solve, and with the cost-aware policy.
+    Reported: GMRES iterations per Newton iteration and sim-time/s of each."""
+    import torch
+    torch.cuda.set_device(local)
+    lib = llg.load()
+    t0 = time.perf_counter()
+    # training on the two 1536x512 workloads
+    p1, g1, o1 = workload(seed=12345 + rank)
+    p1.demag_precision = llg.DEMAG_MIXED
+    c1, geo1 = make_ctx(p1, g1)
+    w, info1 = harvest_train(c1, torch.from_numpy(geo1["y0"]).cuda(), o1, 1.0)
+    c1.close()
+    p2 = llg.default_params(1536, 512, demag_mode=llg.DEMAG_OPEN, demag_strength=1.0, windowed=1, chb=0.0,
+                            norm_kind=llg.NORM_REG, demag_precision=llg.DEMAG_MIXED, bc=llg.BC_FREE)
+    g2 = llg.default_geom(1536, 512, geometry_kind=llg.GEOM_POLYCRYSTAL, num_grains=72, dead_grain_frac=0.16,
+                          grain_z_bias=1.0, ic_kind=llg.IC_TWO_DOMAIN_X, ic_jitter_eps=0.01, init_random_seed=12345)
+    geo2 = llg.build_geometry(g2)
+    c2 = llg.Context(p2)
+    c2.set_window(geo2["w"], geo2["msk3"], geo2["nsk3"])
+    w, info2 = harvest_train(c2, torch.from_numpy(geo2["y0"]).cuda(), o1, 0.5, w_init=w, seed=6)
+    c2.close()
+    train_s = time.perf_counter() - t0
+    n = 2048
+    g3 = llg.default_geom(n, n, geometry_kind=llg.GEOM_ELLIPSE, active_rx_frac=0.25, active_ry_frac=0.25,
+                          ic_kind=llg.IC_VORTEX, ic_jitter_eps=0.01, init_random_seed=12345 + rank)
+    geo3 = llg.build_geometry(g3)
+    ids = np.arange(n * n, dtype=np.int32)
+    act = geo3["active"]
+    res = {}
+    for name, kind, policy in (("block_jacobi", llg.PREC_BLOCK_JACOBI, None), ("learned_every_solve", llg.PREC_LEARNED, 0),
+                               ("learned_cost_aware", llg.PREC_LEARNED, 1)):
+        p3 = llg.default_params(n, n, exec_model=llg.EXEC_COMPACT, bc=llg.BC_PERIODIC, demag_mode=llg.DEMAG_PERIODIC,
+                                demag_strength=2.0, norm_kind=llg.NORM_REG, demag_precision=llg.DEMAG_MIXED,
+                                precond_kind=kind)
+        ctx = llg.Context(p3)
+        ctx.set_active_ids(ids[act == 1], ids[act == 0])
+        if kind == llg.PREC_LEARNED:
+            ctx.learned_set_weights(w)
+            ctx.learned_set_policy(bool(policy))
+        y0 = torch.from_numpy(geo3["y0"]).cuda()
+        ctx.integrator_init(0.0, y0, llg.default_solver_opts())
+        yout = torch.zeros_like(y0)
+        for k in range(1, args.warmup + 1):   # warm-up output intervals (0.1 each)
+            ctx.integrate(0.1 * k, yout)
+        torch.cuda.synchronize()
+        st0 = ctx.stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tstart = 0.1 * args.warmup
+        sub = max(1, int(round(args.dt / 0.1)))
+        e0.record()
+        for s_ in range(args.steps):
+            for k in range(sub):
+                ctx.integrate(tstart + s_ * args.dt + args.dt * (k + 1) / sub, yout)
+        e1.record()
+        torch.cuda.synchronize()
+        st1 = ctx.stats()
+        ms = e0.elapsed_time(e1)
+        d = {k: st1[k] - st0[k] for k in ("nst", "nni", "nli", "nfe")}
+        res[name] = {"gmres_iters_per_newton": d["nli"] / max(d["nni"], 1), "sim_time_per_s":
+                     args.steps * args.dt / (ms / 1000.0), "counters": d}
+        if kind == llg.PREC_LEARNED:
+            res[name]["learned_status"] = ctx.learned_status()
+        ctx.close()
+    line = {
+        "metric": "GMRES iterations per Newton iteration @2048x2048 compact circle, learned vs block-Jacobi",
+        "value": res["learned_every_solve"]["gmres_iters_per_newton"], "unit": "iterations/Newton",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+        "dtype": "f64", "data": "synthetic (seeded builders)",
+        "config": {"workload": "2048x2048 cells, EXEC_COMPACT circle r=0.25 N (19.6 % active), periodic FFT demag "
+                               "strength 2, vortex (-y,x,0.1)/norm + 0.01 jitter, mixed-precision demag, rtol 1e-4, "
+                               "SPGMR(5)", "window": f"t {0.1 * args.warmup:g} -> "
+                                                     f"{0.1 * args.warmup + args.steps * args.dt:g}",
+                   "n_active": int(act.sum())},
+        "block_jacobi": res["block_jacobi"], "learned_every_solve": res["learned_every_solve"],
+        "learned_cost_aware": res["learned_cost_aware"],
+        "training": {"square_hole_1536x512": info1, "polycrystal_1536x512": info2, "train_s": train_s},
+    }
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -725,8 +847,9 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--profile-window", action="store_true",
                     help="cudaProfilerStart/Stop around the timed steps (ncu --profile-from-start off)")
-    ap.add_argument("--workload", choices=["1536x512", "config4"], default="1536x512",
-                    help="config4: the 64-instance batched workload (its own JSON line)")
+    ap.add_argument("--workload", choices=["1536x512", "config3", "config4"], default="1536x512",
+                    help="config3: the compact circle with the learned preconditioner; config4: the 64-instance "
+                         "batched workload (each its own JSON line)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
@@ -734,6 +857,8 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "config4":
             run_config4(args, world, rank, local)
+        elif args.workload == "config3":
+            run_config3(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
