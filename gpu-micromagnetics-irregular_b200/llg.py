@@ -31,7 +31,7 @@ NORM_NONE, NORM_EXACT, NORM_REG = 0, 1, 2
 ANISO_LINEAR, ANISO_CUBIC = 0, 1
 DEMAG_OFF, DEMAG_PERIODIC, DEMAG_OPEN = 0, 1, 2
 DEMAG_FP64, DEMAG_MIXED = 0, 1
-JV_REFERENCE, JV_FULL_FIELD = 0, 1
+JV_REFERENCE, JV_FULL_FIELD, JV_FULL_DEMAG = 0, 1, 2
 GS_AUTO, GS_CLASSICAL, GS_MODIFIED = 0, 1, 2
 PREC_BLOCK_JACOBI, PREC_LEARNED = 0, 1
 GEOM_BULK, GEOM_HOLE_SQUARE, GEOM_RING, GEOM_POLYCRYSTAL, GEOM_CUSTOM, GEOM_ELLIPSE, GEOM_ANNULUS, GEOM_SLIT = range(8)
