@@ -7,6 +7,11 @@
 // pointer); everything main() would need to run CVODE is a stub that
 // reports failure — the checker never runs main().
 #include <stdio.h>
+#include <stdlib.h>
+
+#include <vector>
+
+#include <cuda_runtime.h>
 
 #include <cvode/cvode.h>
 #include <nvector/nvector_cuda.h>
@@ -54,9 +59,29 @@ int SUNLinSolFree(SUNLinearSolver) { return 0; }
 SUNNonlinearSolver SUNNonlinSol_Newton(N_Vector, SUNContext) { return nullptr; }
 int SUNNonlinSolFree(SUNNonlinearSolver) { return 0; }
 
-// the reference's fused-vector layer (deferred_nvector.cu) is not compiled
-// here: main() alone installs it
-void FusedNVec_Init(N_Vector) {}
-void FusedNVec_FreePool(void) {}
+// host dot product of two device vectors (the slot's generic fallback)
+sunrealtype N_VDotProd(N_Vector x, N_Vector y) {
+  std::vector<double> a((size_t)x->n), b((size_t)y->n);
+  cudaMemcpy(a.data(), x->dev, a.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(b.data(), y->dev, b.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  double s = 0.0;
+  for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
+  return s;
+}
+
+// clone: a new device vector of the same length sharing the operation table
+N_Vector llg_shim_nv_clone(N_Vector w) {
+  N_Vector v = (N_Vector)calloc(1, sizeof(*v));
+  if (!v) return nullptr;
+  v->n = w->n;
+  v->ops = w->ops;
+  if (cudaMalloc(&v->dev, (size_t)w->n * sizeof(double)) != cudaSuccess) { free(v); return nullptr; }
+  return v;
+}
+void llg_shim_nv_free(N_Vector v) {
+  if (!v) return;
+  cudaFree(v->dev);
+  free(v);
+}
 
 }  // extern "C"
