@@ -506,9 +506,13 @@ def run_ours(args, world, rank, local):
         summary.update(plain_fp64_value=plain["value"], ratio_vs_plain_fp64=compare["ratio_vs_plain_fp64"])
     accuracy = None
     if form != "plain" and not args.no_accuracy:
-        accuracy = replay_accuracy(form, rank)
-        summary.update(max_dm_replayed=dict(zip([str(t) for t in accuracy["t"]], accuracy["max_dm_replayed"])),
-                       accuracy_bound=1e-4, accuracy_holds_at_t=accuracy["holds_at_t"])
+        try:
+            accuracy = replay_accuracy(form, rank)
+            summary.update(max_dm_replayed=dict(zip([str(t) for t in accuracy["t"]], accuracy["max_dm_replayed"])),
+                           accuracy_bound=1e-4, accuracy_holds_at_t=accuracy["holds_at_t"])
+        except llg.LLGError as e:   # reported, not hidden: the line says the check did not complete
+            accuracy = {"error": str(e)}
+            summary.update(accuracy_error=str(e))
     e2e = None if args.no_e2e else e2e_run(args, form, world, rank)
     if e2e:
         summary["e2e_value"] = e2e["value"]

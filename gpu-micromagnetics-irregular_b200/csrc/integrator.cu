@@ -92,13 +92,16 @@ struct Integrator {
   // accepted step; replaying makes step n use the recorded (h_n, q_n): the
   // order changes and the Nordsieck rescale are CVODE's own, the error test
   // is evaluated but does not reject (replay_forced counts the steps it
-  // would have rejected), and a Newton failure retries the same step with a
-  // fresh preconditioner setup (twice at most) instead of shrinking h.
+  // would have rejected), the Newton iteration may take up to REPLAY_MAXCOR
+  // iterations without the divergence test, and a Newton failure retries the
+  // same step with a fresh preconditioner setup (twice at most) instead of
+  // shrinking h.
   std::vector<double> rec_h, rp_h;
   std::vector<int> rec_q, rp_q;
   int rec_cap = 0;
   bool replay = false;
   long long replay_forced = 0;
+  static constexpr int REPLAY_MAXCOR = 10;   // Newton iterations per attempt while replaying
 
   void export_state(DState& s) const {
     memset(&s, 0, sizeof(s));
@@ -131,6 +134,7 @@ struct Integrator {
            !learned_harvest_wanted(c) && !replay && rec_cap == 0 && !c->dp.src_on && !c->d_hv;
   }
   int integrate_device(double tout, double* yout, double* tret) {
+    materialise();
     if (!dev) {
       const int rc = devint_create(c, &dev);
       if (rc) return rc;
@@ -541,15 +545,36 @@ struct Integrator {
   bool resc_pending = false;  // zn[j] *= resc_f[j] still to be applied
   double resc_f[QMAXL + 1] = {};
   bool y_ready = false;       // y = normalise(zn0) for the current zn0
+  // Lazy completion: complete_step records zn[j] += l_j acor (j = 0..q, and
+  // zn[qmax] = acor when saving) instead of running it, and the next predict
+  // pass applies it first, element by element with the same arithmetic, so
+  // the Nordsieck array is read and written once per step instead of twice.
+  // Anything that reads zn between the two (order change, output
+  // interpolation, state export, a copy of zn0 to the caller) materialises it
+  // first with the eager pass.
+  bool lazy = false;
+  int lazy_q = 0;
+  bool lazy_save = false;
+  double lazy_l[QMAXL + 2] = {};
+  void materialise() {
+    if (!lazy) return;
+    ok(fused_complete(c, lazy_q, qmax, lazy_l, acor, zn, lazy_save, false, 0.0, ewt, SLOT_A, true));
+    lazy = false;
+  }
   void predict() {
     tn += h;
-    ok(fused_predict(c, q, zn, resc_f, resc_pending, ewt_due, rtol, atol, ewt, y, SLOT_EWT));
+    const bool lz = lazy && lazy_q == q;
+    if (lazy && !lz) materialise();
+    ok(fused_predict(c, q, zn, resc_f, resc_pending, ewt_due, rtol, atol, ewt, y, SLOT_EWT, lz ? lazy_l : nullptr,
+                     acor, lazy_save ? zn[qmax] : nullptr));
+    lazy = false;
     if (ewt_due) ewt_pending = true;
     ewt_due = false;
     resc_pending = false;
     y_ready = true;
   }
   void restore(double saved_t) {
+    materialise();   // (nothing is pending after a predict)
     tn = saved_t;
     ok(vnordsieck_shift(c, q, zn, -1));
     y_ready = false;
@@ -604,6 +629,7 @@ struct Integrator {
   }
   void adjust_params() {
     if (qprime != q) {
+      materialise();
       adjust_order(qprime - q);
       q = qprime;
       L = q + 1;
@@ -691,7 +717,9 @@ struct Integrator {
       acnrm = (m == 0) ? dn : wrms_of(s[1]);
       return 0;
     }
-    if ((m >= 1) && (dn > RDIV * delp)) return NLS_CONV_RECVR;
+    // (a replay keeps its recorded step size, so it lets the iteration run
+    // on past a slow start instead of declaring divergence)
+    if (!replay && (m >= 1) && (dn > RDIV * delp)) return NLS_CONV_RECVR;
     delp = dn;
     return NLS_CONTINUE;
   }
@@ -726,7 +754,7 @@ struct Integrator {
         if (retval == 0) { jcur_nls = 0; return 0; }
         if (retval != NLS_CONTINUE) break;
         m++;
-        if (m >= NLS_MAXCOR) { retval = NLS_CONV_RECVR; break; }
+        if (m >= (replay ? REPLAY_MAXCOR : NLS_MAXCOR)) { retval = NLS_CONV_RECVR; break; }
         retval = nls_residual(ycor, del);
         if (retval != 0) break;
       }
@@ -831,7 +859,12 @@ struct Integrator {
     norms_ready = (etamax != 1.0) && (qwait == 0);
     const double cquot =
         (norms_ready && q != qmax && saved_tq5 != 0.0) ? (tq[5] / saved_tq5) * powi(h / tau[2], L) : 0.0;
-    ok(fused_complete(c, q, qmax, l, acor, zn, save, norms_ready, cquot, ewt, SLOT_A));
+    // the norms (of the completed values) now; the completion itself with the next predict
+    ok(fused_complete(c, q, qmax, l, acor, zn, save, norms_ready, cquot, ewt, SLOT_A, false));
+    lazy = true;
+    lazy_q = q;
+    lazy_save = save;
+    for (int j = 0; j <= q; j++) lazy_l[j] = l[j];
     y_ready = false;
   }
   void set_eta() {
@@ -876,6 +909,7 @@ struct Integrator {
     qwait = 2;
     // ||zn[q]|| and ||acor - cquot zn[qmax]||, summed by complete_step's pass
     double s[2] = {0.0, 0.0};
+    if (!norms_ready) materialise();
     if (norms_ready) ok(fetch_scalars(c, SLOT_A, 2, s));
     else if (ok(fused_wrms2(c, zn[q], -((q != qmax && saved_tq5 != 0.0) ? (tq[5] / saved_tq5) * powi(h / tau[2], L)
                                                                           : 0.0),
@@ -950,6 +984,7 @@ struct Integrator {
     return err ? LLG_CV_RHSFUNC_FAIL : 0;
   }
   int get_dky(double t, double* dky) {
+    materialise();
     double tfuzz = FUZZ_FACTOR * UROUND * (fabs(tn) + fabs(hu));
     if (hu < 0.0) tfuzz = -tfuzz;
     const double tp = tn - hu - tfuzz;
@@ -1061,6 +1096,7 @@ struct Integrator {
         ewt_due = true;
       }
       if ((mxstep > 0) && (nstloc >= mxstep)) {
+        materialise();
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
         pdl_break();
         *tret = tn;
@@ -1080,6 +1116,7 @@ struct Integrator {
       }
       const int kflag = cv_step();
       if (kflag != 0) {
+        materialise();
         cudaMemcpyAsync(yout, zn[0], vb, cudaMemcpyDeviceToDevice, c->stream);
         pdl_break();
         *tret = tn;
@@ -1368,6 +1405,7 @@ int integrator_checkpoint_size(llg_ctx* c, uint64_t* bytes) {
 int integrator_checkpoint_save(llg_ctx* c, void* buf, uint64_t cap, uint64_t* written) {
   Integrator* b = c->integ;
   if (!b) { llg_set_error("checkpoint needs llg_integrator_init first"); return LLG_ERR_STATE; }
+  b->materialise();
   if (b->err) { llg_set_error("checkpoint: the integrator is in an error state"); return LLG_ERR_STATE; }
   if (learned_active(c)) {
     llg_set_error("checkpoint: a learned-preconditioner context is not checkpointed (save its weights instead)");
@@ -1516,6 +1554,7 @@ int integrator_batch_prepare(llg_ctx* c, DevInteg** d_out, DState* hs_out) {
     if (rc) return rc;
   }
   devint_mark_batched(b->dev);
+  b->materialise();
   b->export_state(*hs_out);
   *d_out = b->dev;
   return 0;
@@ -1525,6 +1564,7 @@ int integrator_batch_prepare(llg_ctx* c, DevInteg** d_out, DState* hs_out) {
 int integrator_batch_sync(llg_ctx* c) {
   Integrator* b = c->integ;
   if (b->dev_current) return 0;
+  b->materialise();
   DState hs;
   b->export_state(hs);
   const int rc = devint_upload(b->dev, hs, c);

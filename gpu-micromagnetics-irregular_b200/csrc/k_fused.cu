@@ -345,7 +345,8 @@ template <int Q>
 __global__ void __launch_bounds__(RT) k_predict_fused(ZPack zn, CPack f, int pend, int do_ewt, double rtol,
                                                       double atol, double* __restrict__ ewt, double* __restrict__ y,
                                                       int n, int kind, double eps, double* partials,
-                                                      unsigned int* counter, double* out) {
+                                                      unsigned int* counter, double* out, int lazy, CPack lc,
+                                                      const double* __restrict__ acor, double* zsave) {
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
@@ -355,10 +356,20 @@ __global__ void __launch_bounds__(RT) k_predict_fused(ZPack zn, CPack f, int pen
     for (int a = 0; a < 3; a++)
 #pragma unroll
       for (int j = 0; j <= Q; j++) v[a][j] = zn.p[j][(long long)a * n + cell];
+    double xc[3] = {0.0, 0.0, 0.0};
+    if (lazy) {
+#pragma unroll
+      for (int a = 0; a < 3; a++) xc[a] = acor[(long long)a * n + cell];
+    }
     double m[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const long long i = (long long)a * n + cell;
+      if (lazy) {   // the previous step's completion (k_complete_norms' arithmetic)
+#pragma unroll
+        for (int j = 0; j <= Q; j++) v[a][j] = lc.c[j] * xc[a] + v[a][j];
+        if (zsave) zsave[i] = 1.0 * xc[a];
+      }
       if (do_ewt) {
         const double t = rtol * fabs(v[a][0]) + atol;
         if (t <= 0.0) acc[0] += 1.0;   // (a NaN state is left to the norm check)
@@ -377,7 +388,7 @@ __global__ void __launch_bounds__(RT) k_predict_fused(ZPack zn, CPack f, int pen
         for (int j = Q; j >= k; j--) v[a][j - 1] = v[a][j - 1] + v[a][j];
 #pragma unroll
       for (int j = 0; j < Q; j++) zn.p[j][i] = v[a][j];
-      if (pend) zn.p[Q][i] = v[a][Q];
+      if (pend || lazy) zn.p[Q][i] = v[a][Q];
       m[a] = 1.0 * v[a][0] + 1.0 * 0.0;
     }
     double o[3] = {m[0], m[1], m[2]};
@@ -404,12 +415,14 @@ __global__ void __launch_bounds__(RT) k_predict_fused(ZPack zn, CPack f, int pen
 // (zn[Q] w)^2 and ((-cquot zn[qmax] + 1 acor) w)^2 of the updated vectors —
 // the arithmetic of k_scale_add_multi, k_scale and k_wrms2, with k_wrms2's
 // reduction partition.  Every load of an element is issued before its stores.
+// (store 0: the norms alone, of the completed values, nothing written — the
+// completion itself is then applied by the next predict pass)
 template <int Q>
 __global__ void __launch_bounds__(RT) k_complete_norms(int qmax, CPack l, const double* __restrict__ acor, ZPack zn,
                                                        double* zmaxp, int save, int norms, double a2,
                                                        const double* __restrict__ w,
                                                        long long n, double* partials, unsigned int* counter,
-                                                       double* out) {
+                                                       double* out, int store) {
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
@@ -417,19 +430,27 @@ __global__ void __launch_bounds__(RT) k_complete_norms(int qmax, CPack l, const 
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
     const double xi = acor[i];
     double v[Q + 1];
+    if (store) {
 #pragma unroll
-    for (int j = 0; j <= Q; j++) v[j] = zn.p[j][i];
+      for (int j = 0; j <= Q; j++) v[j] = zn.p[j][i];
+    } else {
+      v[Q] = zn.p[Q][i];
+    }
     const double zfar = far ? zmaxp[i] : 0.0;
     const double wi = norms ? w[i] : 0.0;
+    if (store) {
 #pragma unroll
-    for (int j = 0; j <= Q; j++) {
-      v[j] = l.c[j] * xi + v[j];
-      zn.p[j][i] = v[j];
+      for (int j = 0; j <= Q; j++) {
+        v[j] = l.c[j] * xi + v[j];
+        zn.p[j][i] = v[j];
+      }
+    } else {
+      v[Q] = l.c[Q] * xi + v[Q];
     }
     double zmax = (qmax == Q) ? v[Q] : zfar;
     if (save) {
       const double z = 1.0 * xi;
-      zmaxp[i] = z;
+      if (store) zmaxp[i] = z;
       zmax = z;
     }
     if (norms) {
@@ -571,11 +592,13 @@ int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* c
 }
 
 int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pend, bool do_ewt, double rtol,
-                  double atol, double* ewt, double* y, int slot) {
+                  double atol, double* ewt, double* y, int slot, const double* lazy_l, const double* acor,
+                  double* zsave) {
   if (q < 1 || q > 5) { llg_set_error("predict: bad order"); return LLG_ERR_ARG; }
   ZPack zp{};
-  CPack fp{};
-  for (int j = 0; j <= q; j++) { zp.p[j] = zn[j]; fp.c[j] = f ? f[j] : 1.0; }
+  CPack fp{}, lp{};
+  for (int j = 0; j <= q; j++) { zp.p[j] = zn[j]; fp.c[j] = f ? f[j] : 1.0; lp.c[j] = lazy_l ? lazy_l[j] : 0.0; }
+  const int lz = lazy_l ? 1 : 0;
   LLG_COUNT(KID_ELEMWISE);
   long long nbl = (c->ncell + RT - 1) / RT;   // ~one cell per thread, up to the partials' capacity
   if (nbl > RMAXB) nbl = RMAXB;
@@ -585,7 +608,8 @@ int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pe
   double* out = c->d_scal + slot;
 #define PRED(Q)                                                                                                \
   klaunch(k_predict_fused<Q>, nb, RT, 0, c->stream, zp, fp, pe, de, rtol, atol, ewt, y, c->ncell, c->p.norm_kind,   \
-                                               c->p.norm_eps, c->d_red, c->d_counter, out)
+                                               c->p.norm_eps, c->d_red, c->d_counter, out, lz, lp, acor,         \
+                                               lz ? zsave : nullptr)
   switch (q) {
     case 1: PRED(1); break;
     case 2: PRED(2); break;
@@ -599,18 +623,19 @@ int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pe
 }
 
 int fused_complete(llg_ctx* c, int q, int qmax, const double* l, const double* acor, double* const* zn, bool save,
-                   bool norms, double cquot, const double* w, int slot) {
+                   bool norms, double cquot, const double* w, int slot, bool store) {
+  if (!store && !norms) return 0;
   if (q < 0 || q > 5 || qmax < q || qmax > 5) { llg_set_error("complete: bad order"); return LLG_ERR_ARG; }
   ZPack zp{};
   CPack lp{};
   for (int j = 0; j <= qmax; j++) zp.p[j] = zn[j];
   for (int j = 0; j <= q; j++) lp.c[j] = l[j];
   LLG_COUNT(KID_ELEMWISE);
-  const int sv = save ? 1 : 0, nm = norms ? 1 : 0;
+  const int sv = save ? 1 : 0, nm = norms ? 1 : 0, st = store ? 1 : 0;
 #define COMP(Q)                                                                                    \
   klaunch(k_complete_norms<Q>, red_blocks(c->neq), RT, 0, c->stream, qmax, lp, acor, zp, zn[qmax], sv, nm, -cquot, \
                                                                 w, c->neq, c->d_red, c->d_counter,             \
-                                                                c->d_scal + slot)
+                                                                c->d_scal + slot, st)
   switch (q) {
     case 0: COMP(0); break;
     case 1: COMP(1); break;

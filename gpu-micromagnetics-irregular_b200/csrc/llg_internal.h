@@ -277,12 +277,16 @@ int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double
 
 // start of a BDF attempt: (do_ewt) weights + checks, (pend) zn[j] *= f[j], the
 // Nordsieck predictor and y = normalise(zn0)  [k_fused.cu]
+// (lazy_l non-null: the previous step's completion zn[j] += lazy_l[j] acor,
+// j = 0..q, and zsave (non-null) = acor, applied first in the same pass)
 int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pend, bool do_ewt, double rtol,
-                  double atol, double* ewt, double* y, int slot);
+                  double atol, double* ewt, double* y, int slot, const double* lazy_l = nullptr,
+                  const double* acor = nullptr, double* zsave = nullptr);
 // complete_step (+ zn[qmax] = acor when save) and, when norms, the order-
 // selection sums of the updated vectors
+// (store false: only the norms of the completed values, nothing written)
 int fused_complete(llg_ctx* c, int q, int qmax, const double* l, const double* acor, double* const* zn, bool save,
-                   bool norms, double cquot, const double* w, int slot);
+                   bool norms, double cquot, const double* w, int slot, bool store = true);
 // GMRES correction (stored only when del is non-null) + Newton update + both norms
 int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
                          double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks = nullptr);

@@ -253,9 +253,10 @@ int  llg_get_stats(llg_ctx* ctx, llg_stats* st);
  * a fresh run (set after llg_integrator_init, before its first
  * llg_integrate) take exactly that sequence: step n uses order q_n and size
  * h_n, the local error test is evaluated but does not reject (the steps it
- * would have rejected are counted), and a Newton failure retries the same
- * step with a fresh preconditioner setup, at most twice, then returns
- * LLG_CV_CONV_FAILURE.  A run that needs more steps than were recorded
+ * would have rejected are counted), the Newton iteration may take up to 10
+ * iterations without CVODE's divergence test (the step size cannot shrink),
+ * and a Newton failure retries the same step with a fresh preconditioner
+ * setup, at most twice, then returns LLG_CV_CONV_FAILURE.  A run that needs more steps than were recorded
  * returns LLG_ERR_STATE.  Host-driven integrator only (the device-resident
  * form is bypassed while recording or replaying).                          */
 int  llg_integrator_record_steps(llg_ctx* ctx, int32_t cap);
