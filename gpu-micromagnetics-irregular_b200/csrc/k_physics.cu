@@ -498,6 +498,7 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
 // LLG_JV_FULL_DEMAG (the same arithmetic as the operator's staging)
 __global__ void k_arnoldi_input(const double* __restrict__ in, const double* __restrict__ s, const double* in_a,
                                 double* __restrict__ vt, long long n3) {
+  pdl_entry();
   const double ain = kscale_of(in_a);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
     vt[i] = 1.0 * ((ain * in[i]) / s[i]);

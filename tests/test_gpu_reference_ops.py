@@ -86,7 +86,9 @@ def test_operators_match_reference_kernels(gpu, ng, ny, strength):
     assert strength == 0 or demag
     n0 = (C.c_double * 3)()
     if demag:
-        lib.Demag_GetSelfCoupling(demag, C.byref(n0, 0), C.byref(n0, 8), C.byref(n0, 16))
+        nx0, ny0, nz0 = C.c_double(), C.c_double(), C.c_double()
+        lib.Demag_GetSelfCoupling(demag, C.byref(nx0), C.byref(ny0), C.byref(nz0))
+        n0[:] = (nx0.value, ny0.value, nz0.value)
     ymsk = dev(act3)
     # reference: f (normalise, demag, RHS), JtvProduct, PrecondSetup / PrecondSolve
     ry, rydot, rhd = dev(y), zeros(), zeros()
