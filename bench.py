@@ -508,7 +508,12 @@ def run_ours(args, world, rank, local):
     if form != "plain" and not args.no_accuracy:
         try:
             accuracy = replay_accuracy(form, rank)
-            summary.update(max_dm_replayed=dict(zip([str(t) for t in accuracy["t"]], accuracy["max_dm_replayed"])),
+            ts = [str(t) for t in accuracy["t"]]
+            summary.update(max_dm_replayed=dict(zip(ts, accuracy["max_dm_replayed"])),
+                           max_dm_control_fp64_strength_1e9_replayed=dict(
+                               zip(ts, accuracy["max_dm_control_fp64_strength_1e-9_replayed"])),
+                           max_dm_fp64_rtol1e6_vs_rtol1e8=dict(zip([str(t) for t in accuracy["t_floor"]],
+                                                                   accuracy["max_dm_fp64_rtol1e-6_vs_rtol1e-8"])),
                            accuracy_bound=1e-4, accuracy_holds_at_t=accuracy["holds_at_t"])
         except llg.LLGError as e:   # reported, not hidden: the line says the check did not complete
             accuracy = {"error": str(e)}
