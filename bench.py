@@ -196,6 +196,12 @@ FORMS = {
     "mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=False, name="mixed-precision demag",
                   desc="mixed-precision demag (FP32 row FFTs, tcgen05 FP16 hi+lo column DFT stages with FP32 "
                        "accumulation), block-Jacobi; FP64 state, norms, Newton update, Gram-Schmidt"),
+    "mixed32": dict(demag_precision=llg.DEMAG_MIXED, learned=False, krylov=llg.KRYLOV_FP32,
+                    name="mixed-precision demag + FP32 Krylov basis",
+                    desc="mixed-precision demag (FP32 row FFTs, tcgen05 FP16 hi+lo column DFT stages with FP32 "
+                         "accumulation) and the SPGMR Krylov basis stored in FP32 (Arnoldi operator, Gram-Schmidt "
+                         "dots and update, correction read it; every product and sum in FP64), block-Jacobi; FP64 "
+                         "state, norms, Newton update, Gram-Schmidt dots"),
     "learned+mixed": dict(demag_precision=llg.DEMAG_MIXED, learned=True,
                           name="learned preconditioner + mixed-precision demag",
                           desc="learned preconditioner (3-layer 3x3 conv, 16 channels, BF16 weights, FP32 "
@@ -240,6 +246,7 @@ def train_weights(rank):
 
 def form_params(form, seed, gs=None):
     p, g, o = workload(seed=seed, gs=gs)
+    o.krylov_precision = FORMS[form].get("krylov", llg.KRYLOV_FP64)
     p.demag_precision = FORMS[form]["demag_precision"]
     p.precond_kind = llg.PREC_LEARNED if FORMS[form]["learned"] else llg.PREC_BLOCK_JACOBI
     return p, g, o
@@ -492,11 +499,14 @@ def run_ours(args, world, rank, local):
                    "plain_gmres_iters_per_newton": plain["counters"]["nli"] / max(plain["counters"]["nni"], 1),
                    "bdf_steps": main["counters"]["nst"], "plain_bdf_steps": plain["counters"]["nst"],
                    "plain_counters": plain["counters"]}
-        if FORMS[form]["learned"]:
-            mixed = timed_run(args, "mixed", world, rank, local, lib, clocks=False)
-            mixed["ctx"].close()
-            compare["mixed_only_value"] = mixed["value"]
-            compare["mixed_only_gmres_iters_per_newton"] = mixed["counters"]["nli"] / max(mixed["counters"]["nni"], 1)
+        for other in ("mixed", "mixed32", "learned+mixed"):
+            if other == form:
+                continue
+            r_ = timed_run(args, other, world, rank, local, lib, clocks=False)
+            r_["ctx"].close()
+            compare[f"{other}_value"] = r_["value"]
+            compare[f"{other}_gmres_iters_per_newton"] = r_["counters"]["nli"] / max(r_["counters"]["nni"], 1)
+            compare[f"{other}_bdf_steps"] = r_["counters"]["nst"]
         if not args.no_reference_gs:
             mgs = timed_run(args, "plain", world, rank, local, lib, clocks=False, gs=llg.GS_AUTO)
             mgs["ctx"].close()

@@ -43,6 +43,10 @@ struct Integrator {
   llg_ctx* c = nullptr;
   long long neq = 0;
   int qmax = 5, maxl = 5, classical_gs = 1, mxstep = 500;
+  // LLG_KRYLOV_FP32: the basis V[0..maxl] holds floats (the same allocations);
+  // the read-back-light SPGMR then calls the float variants of its kernels
+  bool kf32 = false;
+  float* Vf(int i) const { return reinterpret_cast<float*>(V[i]); }
   double rtol = 1e-4, atol = 1e-6;
   double* zn[QMAXL + 1] = {};
   double *ewt = nullptr, *acor = nullptr, *y = nullptr, *tempv = nullptr, *delta = nullptr;
@@ -131,7 +135,7 @@ struct Integrator {
   // learned preconditioner and training-pair harvesting stay on the host path
   bool device_applies() {
     return device_resident && started && classical_gs && maxl <= MAXLL - 1 && !learned_active(c) &&
-           !learned_harvest_wanted(c) && !replay && rec_cap == 0 && !c->dp.src_on && !c->d_hv;
+           !learned_harvest_wanted(c) && !replay && rec_cap == 0 && !c->dp.src_on && !c->d_hv && !kf32;
   }
   int integrate_device(double tout, double* yout, double* tret) {
     materialise();
@@ -313,12 +317,21 @@ struct Integrator {
   }
   void enqueue_iter(int l) {
     const int k = l + 1;
-    ok(launch_arnoldi_op(c, V[l], ewt, V[k], y, gamma, 1, nullptr, ka[l]));
-    const double* Y[MAXLL + 1];
-    for (int i = 0; i <= k; i++) Y[i] = V[i];
     const KScale ys = basis_scales(0, k, 0);   // V[k] itself: the fresh operator output, unscaled
-    ok(vdot_multi_dev(c, k + 1, V[k], Y, slot_it(l), &ys));
-    ok(vgs_update_dev(c, k, V, slot_it(l), slot_ss(l), &ys, slot_sc(l)));
+    if (kf32) {
+      ok(launch_arnoldi_op_f(c, Vf(l), ewt, Vf(k), y, gamma, ka[l]));
+      const float* Y[MAXLL + 1];
+      float* W[MAXLL + 1];
+      for (int i = 0; i <= k; i++) { Y[i] = Vf(i); W[i] = Vf(i); }
+      ok(vdot_multi_dev_f(c, k + 1, Vf(k), Y, slot_it(l), &ys));
+      ok(vgs_update_dev_f(c, k, W, slot_it(l), slot_ss(l), &ys, slot_sc(l)));
+    } else {
+      ok(launch_arnoldi_op(c, V[l], ewt, V[k], y, gamma, 1, nullptr, ka[l]));
+      const double* Y[MAXLL + 1];
+      for (int i = 0; i <= k; i++) Y[i] = V[i];
+      ok(vdot_multi_dev(c, k + 1, V[k], Y, slot_it(l), &ys));
+      ok(vgs_update_dev(c, k, V, slot_it(l), slot_ss(l), &ys, slot_sc(l)));
+    }
     ka[k] = c->d_scal + slot_sc(l);
   }
   int spgmr_spec(double* rhs, double delta_tol, bool harvest, double* zb) {
@@ -326,7 +339,9 @@ struct Integrator {
     int nl = 0, krydim = 0, converged = 0;
     nps++;
     if (harvest) ok(launch_psolve(c, rhs, zb));   // u = P_BJ^-1 r, kept with the solution
-    if (!ok(fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A, nullptr, SLOT_V0SC))) return LS_CONV_FAIL;
+    if (!ok(kf32 ? fused_psolve_scale_dot_f(c, rhs, ewt, Vf(0), SLOT_A, SLOT_V0SC)
+                 : fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A, nullptr, SLOT_V0SC)))
+      return LS_CONV_FAIL;
     ka[0] = c->d_scal + SLOT_V0SC;
     int queued = (lmax >= 2) ? 2 : 1;
     for (int l = 0; l < queued; l++) enqueue_iter(l);
@@ -362,16 +377,30 @@ struct Integrator {
         // so later queued iterations are void and are enqueued again
         second = true;
         queued = k;
-        const double* Y[MAXLL + 1];
-        for (int i = 0; i < k; i++) Y[i] = V[i];
         double dots[MAXLL + 1], cf[MAXLL + 1], ss = 0.0;
-        const double* X[MAXLL + 1];
         const KScale ys = basis_scales(0, k, 0), xs = basis_scales(0, k, 1);
-        if (ok(vdot_multi_dev(c, k, V[k], Y, SLOT_DOTS, &ys))) ok(fetch_scalars(c, SLOT_DOTS, k, dots));
+        if (kf32) {
+          const float* Y[MAXLL + 1];
+          for (int i = 0; i < k; i++) Y[i] = Vf(i);
+          if (ok(vdot_multi_dev_f(c, k, Vf(k), Y, SLOT_DOTS, &ys))) ok(fetch_scalars(c, SLOT_DOTS, k, dots));
+        } else {
+          const double* Y[MAXLL + 1];
+          for (int i = 0; i < k; i++) Y[i] = V[i];
+          if (ok(vdot_multi_dev(c, k, V[k], Y, SLOT_DOTS, &ys))) ok(fetch_scalars(c, SLOT_DOTS, k, dots));
+        }
         cf[0] = 1.0;
-        X[0] = V[k];
-        for (int i = 0; i < k; i++) { Hes[i][l] += dots[i]; cf[i + 1] = -dots[i]; X[i + 1] = V[i]; }
-        if (ok(fused_lincomb_norm(c, k + 1, cf, X, V[k], SLOT_DOTS, &xs))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
+        for (int i = 0; i < k; i++) { Hes[i][l] += dots[i]; cf[i + 1] = -dots[i]; }
+        if (kf32) {
+          const float* X[MAXLL + 1];
+          X[0] = Vf(k);
+          for (int i = 0; i < k; i++) X[i + 1] = Vf(i);
+          if (ok(fused_lincomb_norm_f(c, k + 1, cf, X, Vf(k), SLOT_DOTS, &xs))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
+        } else {
+          const double* X[MAXLL + 1];
+          X[0] = V[k];
+          for (int i = 0; i < k; i++) X[i + 1] = V[i];
+          if (ok(fused_lincomb_norm(c, k + 1, cf, X, V[k], SLOT_DOTS, &xs))) ok(fetch_scalars(c, SLOT_DOTS, 1, &ss));
+        }
         nrm = sqrt(ss);
       }
       Hes[k][l] = nrm;
@@ -379,7 +408,7 @@ struct Integrator {
       rot *= givens[2 * l + 1];
       rho = fabs(rot * rnorm);
       if (rho <= delta_tol) { converged = 1; break; }
-      if (second) ok(vscale(c, 1.0 / Hes[k][l], V[k], V[k]));
+      if (second) ok(kf32 ? vscale_f(c, 1.0 / Hes[k][l], Vf(k), Vf(k)) : vscale(c, 1.0 / Hes[k][l], V[k], V[k]));
     }
     nli += nl;
     yg[0] = rnorm;
@@ -387,15 +416,18 @@ struct Integrator {
     if (qr_sol(krydim, yg) != 0) return LS_QRSOL_FAIL;
     if (converged || rho < beta) {
       const double* X[MAXLL + 1];
-      for (int k = 0; k < krydim; k++) X[k] = V[k];
+      const float* Xf[MAXLL + 1];
+      for (int k = 0; k < krydim; k++) { X[k] = V[k]; Xf[k] = Vf(k); }
       const KScale xs = basis_scales(0, krydim, 0);
       const bool taken = converged || ls_curiter == 0;
       if (taken && fuse_update) {
-        ok(fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A, &xs));
+        ok(kf32 ? fused_lincomb_update_f(c, krydim, yg, Xf, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A, &xs)
+                : fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A, &xs));
         ok(fetch_scalars(c, SLOT_A, 2, upd_s));
         update_done = true;
       } else {
-        ok(fused_lincomb_div(c, krydim, yg, X, ewt, rhs, &xs));
+        ok(kf32 ? fused_lincomb_div_f(c, krydim, yg, Xf, ewt, rhs, &xs)
+                : fused_lincomb_div(c, krydim, yg, X, ewt, rhs, &xs));
       }
       if (converged && harvest) ok(learned_harvest(c, zb, rhs, ewt, c->gamma_setup));
       return converged ? LS_SUCCESS : LS_RES_REDUCED;
@@ -410,6 +442,7 @@ struct Integrator {
     double* zb = (learned || harvest) ? learned_zbuf(c) : nullptr;
     if ((learned || harvest) && !zb) return LS_CONV_FAIL;
     if (!learned && classical_gs) return spgmr_spec(rhs, delta_tol, harvest, zb);
+    if (kf32) { llg_set_error("FP32 Krylov basis: the learned / modified Gram-Schmidt solver keeps FP64"); err = LLG_ERR_NOTSUP; return LS_CONV_FAIL; }
     nps++;
     double ss = 0.0;
     if (harvest) ok(launch_psolve(c, rhs, zb));   // u = P_BJ^-1 r, kept with the solution
@@ -1158,6 +1191,17 @@ int integrator_create(llg_ctx* c, double t0, const double* y0, const llg_solver_
   b->rtol = o->rtol;
   b->atol = o->atol;
   b->device_resident = o->device_resident ? 1 : 0;
+  b->kf32 = (o->krylov_precision == LLG_KRYLOV_FP32);
+  if (o->krylov_precision != LLG_KRYLOV_FP64 && o->krylov_precision != LLG_KRYLOV_FP32) {
+    delete b;
+    llg_set_error("krylov_precision must be LLG_KRYLOV_FP64 or LLG_KRYLOV_FP32");
+    return LLG_ERR_ARG;
+  }
+  if (b->kf32 && (!b->classical_gs || c->p.precond_kind == LLG_PREC_LEARNED)) {
+    delete b;
+    llg_set_error("FP32 Krylov basis needs classical Gram-Schmidt and the block-Jacobi preconditioner");
+    return LLG_ERR_NOTSUP;
+  }
   const size_t vb = sizeof(double) * (size_t)b->neq;
   auto alloc = [&](double** p) -> int {
     LLG_CUDA_TRY(cudaMalloc(p, vb));
@@ -1213,7 +1257,10 @@ int integrator_time_kernel(llg_ctx* c, int kid, int iters, double* avg_ms) {
     switch (kid) {
       case KID_RHS: return launch_rhs(c, b->y, c->d_hd, b->tempv);
       case KID_JTV: return launch_jtv(c, b->V[0], b->tempv, b->y);
-      case KID_ARNOLDI: return c->have_setup ? launch_arnoldi_op(c, b->V[0], b->ewt, b->tempv, b->y, b->gamma) : LLG_ERR_STATE;
+      case KID_ARNOLDI:
+        if (!c->have_setup) return LLG_ERR_STATE;
+        return b->kf32 ? launch_arnoldi_op_f(c, b->Vf(0), b->ewt, b->Vf(1), b->y, b->gamma, nullptr)
+                       : launch_arnoldi_op(c, b->V[0], b->ewt, b->tempv, b->y, b->gamma);
       case KID_PSETUP: return launch_psetup(c, b->y, c->gamma_setup);
       case KID_PSOLVE: return c->have_setup ? launch_psolve(c, b->V[0], b->tempv) : LLG_ERR_STATE;
       case KID_NORM: return launch_normalize(c, b->tempv);
@@ -1419,6 +1466,7 @@ int integrator_checkpoint_save(llg_ctx* c, void* buf, uint64_t cap, uint64_t* wr
   hd.version = CKPT_VERSION;
   hd.header_bytes = sizeof(llg_ckpt_info);
   hd.scalar_bytes = sizeof(CkptScalars);
+  hd.krylov_precision = b->kf32 ? LLG_KRYLOV_FP32 : LLG_KRYLOV_FP64;
   hd.ng = c->p.ng;
   hd.ny = c->p.ny;
   hd.neq = b->neq;
@@ -1491,6 +1539,7 @@ int integrator_checkpoint_load(llg_ctx* c, const void* buf, uint64_t n) {
   o.gs_type = hd.classical_gs ? LLG_GS_CLASSICAL : LLG_GS_MODIFIED;
   o.mxstep = hd.mxstep;
   o.device_resident = hd.device_resident;
+  o.krylov_precision = (int32_t)hd.krylov_precision;
   rc = integrator_create(c, hd.tn, nullptr, &o);
   if (rc) return rc;
   Integrator* b = c->integ;

@@ -36,6 +36,11 @@ struct CPack {
 struct XPack {
   const double* p[FV];
 };
+// Krylov basis vectors stored as VT (double, or float for the FP32-basis solver)
+template <typename T>
+struct XPackT {
+  const T* p[FV];
+};
 struct ZPack {
   double* p[8];
 };
@@ -168,10 +173,11 @@ __global__ void k_rhs_resid_compact(DevProblem P, const double* __restrict__ y, 
 
 // (streams at HBM speed, so it rebuilds the block from the frozen (m, h),
 // 48 B/cell, rather than reading the 72 B/cell inverse that psetup stores)
+template <typename VT = double>
 __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const double* __restrict__ pm,
                                                          const double* __restrict__ ph,
                                                          const double* __restrict__ r,
-                                                         const double* __restrict__ ewt, double* __restrict__ v0,
+                                                         const double* __restrict__ ewt, VT* __restrict__ v0,
                                                          double gamma, double* partials, unsigned int* counter,
                                                          double* out, const DevArgs* da, double* aout) {
   pdl_entry();
@@ -193,11 +199,11 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
     const double z0 = g * (Pi[0] * rr[0] + Pi[1] * rr[1] + Pi[2] * rr[2]);
     const double z1 = g * (Pi[3] * rr[0] + Pi[4] * rr[1] + Pi[5] * rr[2]);
     const double z2 = g * (Pi[6] * rr[0] + Pi[7] * rr[1] + Pi[8] * rr[2]);
-    const double a0 = ewt[k] * z0, a1 = ewt[n + k] * z1, a2 = ewt[2 * n + k] * z2;
+    const VT a0 = (VT)(ewt[k] * z0), a1 = (VT)(ewt[n + k] * z1), a2 = (VT)(ewt[2 * n + k] * z2);
     v0[k] = a0; v0[n + k] = a1; v0[2 * n + k] = a2;
-    acc[0] += a0 * a0;
-    acc[0] += a1 * a1;
-    acc[0] += a2 * a2;
+    acc[0] += (double)a0 * (double)a0;
+    acc[0] += (double)a1 * (double)a1;
+    acc[0] += (double)a2 * (double)a2;
   }
   block_sum<1>(acc, sm);
   const bool last = finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
@@ -205,7 +211,8 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
 }
 
 // z = c0 X0; z = c_k X_k + z (z may alias X0), and sum z^2
-__global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, double* z, long long n,
+template <typename VT = double>
+__global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPackT<VT> X, VT* z, long long n,
                                                      double* partials, unsigned int* counter, double* out,
                                                      KScale ks) {
   pdl_entry();
@@ -215,24 +222,26 @@ __global__ void __launch_bounds__(RT) k_lincomb_norm(int nv, CPack c, XPack X, d
   __syncthreads();
   double acc[1] = {0.0};
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT) {
-    double s = c.c[0] * (xs[0] * X.p[0][i]);
-    for (int k = 1; k < nv; k++) s = c.c[k] * (xs[k] * X.p[k][i]) + s;
-    z[i] = s;
-    acc[0] += s * s;
+    double s = c.c[0] * (xs[0] * (double)X.p[0][i]);
+    for (int k = 1; k < nv; k++) s = c.c[k] * (xs[k] * (double)X.p[k][i]) + s;
+    const VT sv = (VT)s;
+    z[i] = sv;
+    acc[0] += (double)sv * (double)sv;
   }
   block_sum<1>(acc, sm);
   finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
 }
 
-__global__ void k_lincomb_div(int nv, CPack c, XPack X, const double* __restrict__ w, double* __restrict__ z,
+template <typename VT = double>
+__global__ void k_lincomb_div(int nv, CPack c, XPackT<VT> X, const double* __restrict__ w, double* __restrict__ z,
                               long long n, KScale ks) {
   pdl_entry();
   __shared__ double xs[FV];   // scales of the X vectors, staged once (see k_lincomb_update)
   if (threadIdx.x < nv) xs[threadIdx.x] = kscale_of(ks.a[threadIdx.x]);
   __syncthreads();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    double s = c.c[0] * (xs[0] * X.p[0][i]);
-    for (int k = 1; k < nv; k++) s = c.c[k] * (xs[k] * X.p[k][i]) + s;
+    double s = c.c[0] * (xs[0] * (double)X.p[0][i]);
+    for (int k = 1; k < nv; k++) s = c.c[k] * (xs[k] * (double)X.p[k][i]) + s;
     z[i] = s / w[i];
   }
 }
@@ -266,7 +275,8 @@ __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, doub
 // (ycor_in null: zero), and the sums (d*w)^2, (ycor*w)^2 — per element the
 // arithmetic of k_lincomb_div followed by k_update_wrms2, with the latter's
 // reduction partition
-__global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X, const double* __restrict__ w,
+template <typename VT = double>
+__global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPackT<VT> X, const double* __restrict__ w,
                                                        double* del, const double* ycor_in, double* ycor, long long n,
                                                        double* partials, unsigned int* counter, double* out,
                                                        KScale ks) {
@@ -286,7 +296,7 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X,
     for (int u = 0; u < UB; u++) {
       const long long i = i0 + u * st;
       const bool in = i < n;
-      s[u] = in ? c.c[0] * (xa0 * X.p[0][i]) : 0.0;
+      s[u] = in ? c.c[0] * (xa0 * (double)X.p[0][i]) : 0.0;
       wv[u] = in ? w[i] : 1.0;
       yv[u] = (in && ycor_in) ? ycor_in[i] : 0.0;
     }
@@ -294,7 +304,7 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPack X,
       const double xa = xs[k];
       double xv[UB];
 #pragma unroll
-      for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * X.p[k][i0 + u * st] : 0.0;
+      for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * (double)X.p[k][i0 + u * st] : 0.0;
 #pragma unroll
       for (int u = 0; u < UB; u++) s[u] = c.c[k] * xv[u] + s[u];
     }
@@ -521,42 +531,68 @@ int fused_resid(llg_ctx* c, const double* y, const double* zn1, const double* yc
   return 0;
 }
 
-int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot, const DevArgs* da,
-                           int slot_aout) {
+template <typename VT>
+static int psolve_scale_dot_impl(llg_ctx* c, const double* r, const double* ewt, VT* v0, int slot, const DevArgs* da,
+                                 int slot_aout) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
-  klaunch(k_psolve_scale_dot, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, ewt, v0,
+  klaunch(k_psolve_scale_dot<VT>, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, ewt, v0,
           c->gamma_setup, c->d_red, c->d_counter, c->d_scal + slot, da,
           slot_aout >= 0 ? c->d_scal + slot_aout : nullptr);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
+int fused_psolve_scale_dot(llg_ctx* c, const double* r, const double* ewt, double* v0, int slot, const DevArgs* da,
+                           int slot_aout) {
+  return psolve_scale_dot_impl<double>(c, r, ewt, v0, slot, da, slot_aout);
+}
+int fused_psolve_scale_dot_f(llg_ctx* c, const double* r, const double* ewt, float* v0, int slot, int slot_aout) {
+  return psolve_scale_dot_impl<float>(c, r, ewt, v0, slot, nullptr, slot_aout);
+}
 
-int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot,
-                       const KScale* ks) {
+template <typename VT>
+static int lincomb_norm_impl(llg_ctx* c, int nv, const double* coef, const VT* const* X, VT* z, int slot,
+                             const KScale* ks) {
   if (nv < 1 || nv > FV) { llg_set_error("lincomb_norm: bad nvec"); return LLG_ERR_ARG; }
   CPack cp{};
-  XPack xp{};
+  XPackT<VT> xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
   const KScale kz{};
   LLG_COUNT(KID_REDUCE);
-  klaunch(k_lincomb_norm, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, z, c->neq, c->d_red, c->d_counter,
+  klaunch(k_lincomb_norm<VT>, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, z, c->neq, c->d_red, c->d_counter,
           c->d_scal + slot, ks ? *ks : kz);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
+int fused_lincomb_norm(llg_ctx* c, int nv, const double* coef, const double* const* X, double* z, int slot,
+                       const KScale* ks) {
+  return lincomb_norm_impl<double>(c, nv, coef, X, z, slot, ks);
+}
+int fused_lincomb_norm_f(llg_ctx* c, int nv, const double* coef, const float* const* X, float* z, int slot,
+                         const KScale* ks) {
+  return lincomb_norm_impl<float>(c, nv, coef, X, z, slot, ks);
+}
 
-int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z,
-                      const KScale* ks) {
+template <typename VT>
+static int lincomb_div_impl(llg_ctx* c, int nv, const double* coef, const VT* const* X, const double* w, double* z,
+                            const KScale* ks) {
   if (nv < 1 || nv > FV) { llg_set_error("lincomb_div: bad nvec"); return LLG_ERR_ARG; }
   CPack cp{};
-  XPack xp{};
+  XPackT<VT> xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
   const KScale kz{};
   LLG_COUNT(KID_ELEMWISE);
-  klaunch(k_lincomb_div, ew_blocks(c, c->neq), 256, 0, c->stream, nv, cp, xp, w, z, c->neq, ks ? *ks : kz);
+  klaunch(k_lincomb_div<VT>, ew_blocks(c, c->neq), 256, 0, c->stream, nv, cp, xp, w, z, c->neq, ks ? *ks : kz);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
+}
+int fused_lincomb_div(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w, double* z,
+                      const KScale* ks) {
+  return lincomb_div_impl<double>(c, nv, coef, X, w, z, ks);
+}
+int fused_lincomb_div_f(llg_ctx* c, int nv, const double* coef, const float* const* X, const double* w, double* z,
+                        const KScale* ks) {
+  return lincomb_div_impl<float>(c, nv, coef, X, w, z, ks);
 }
 
 int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot,
@@ -577,18 +613,27 @@ int fused_wrms2(llg_ctx* c, const double* x1, double a, const double* x2, double
   return 0;
 }
 
-int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
-                         double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks) {
+template <typename VT>
+static int lincomb_update_impl(llg_ctx* c, int nv, const double* coef, const VT* const* X, const double* w,
+                               double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks) {
   if (nv < 1 || nv > FV) { llg_set_error("lincomb_update: bad nvec"); return LLG_ERR_ARG; }
   CPack cp{};
-  XPack xp{};
+  XPackT<VT> xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
   const KScale kz{};
   LLG_COUNT(KID_REDUCE);
-  klaunch(k_lincomb_update, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, w, del, ycor_zero ? nullptr : ycor, ycor,
-          c->neq, c->d_red, c->d_counter, c->d_scal + slot, ks ? *ks : kz);
+  klaunch(k_lincomb_update<VT>, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, w, del, ycor_zero ? nullptr : ycor,
+          ycor, c->neq, c->d_red, c->d_counter, c->d_scal + slot, ks ? *ks : kz);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
+}
+int fused_lincomb_update(llg_ctx* c, int nv, const double* coef, const double* const* X, const double* w,
+                         double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks) {
+  return lincomb_update_impl<double>(c, nv, coef, X, w, del, ycor_zero, ycor, slot, ks);
+}
+int fused_lincomb_update_f(llg_ctx* c, int nv, const double* coef, const float* const* X, const double* w,
+                           double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks) {
+  return lincomb_update_impl<float>(c, nv, coef, X, w, del, ycor_zero, ycor, slot, ks);
 }
 
 int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pend, bool do_ewt, double rtol,

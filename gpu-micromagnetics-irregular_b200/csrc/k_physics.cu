@@ -235,18 +235,21 @@ __global__ void k_psolve(DevProblem P, const double* __restrict__ pm, const doub
 // Fused Arnoldi operator of left-preconditioned, ewt-scaled GMRES:
 //   vt = in / s ;  u = vt − γ J(y) vt ;  out = s ⊙ P^-1 u
 // One pass: reads in (stencil), s (stencil), y (stencil), pm/ph, writes out.
-__global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const double* __restrict__ in,
+template <typename VT = double>
+__global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const VT* __restrict__ in,
                                                           const double* __restrict__ s,
-                                                          double* __restrict__ out, const double* __restrict__ y,
+                                                          VT* __restrict__ out, const double* __restrict__ y,
                                                           const double* __restrict__ hd,
                                                           const double* __restrict__ pinv, double gamma,
                                                           int scale_out, const DevArgs* da, const double* in_a) {
   pdl_entry();
   __shared__ Tile<2> T;
-  if (da) {
-    in = da->arn_in;
-    out = da->arn_out;
-    gamma = da->gamma;
+  if constexpr (sizeof(VT) == sizeof(double)) {
+    if (da) {
+      in = da->arn_in;
+      out = da->arn_out;
+      gamma = da->gamma;
+    }
   }
   const double ain = kscale_of(in_a);   // the input is read as ain * in
   // stage y and vt = in/s (windowed: w·) with halo
@@ -267,7 +270,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
 #pragma unroll
       for (int a = 0; a < 3; a++) {
         T.v[0][a][sy][sx] = ok ? ww * y[a * n + cell] : 0.0;
-        T.v[1][a][sy][sx] = ok ? ww * ((ain * in[a * n + cell]) / s[a * n + cell]) : 0.0;
+        T.v[1][a][sy][sx] = ok ? ww * ((ain * (double)in[a * n + cell]) / s[a * n + cell]) : 0.0;
       }
     }
     __syncthreads();
@@ -288,7 +291,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       m[a] = y[a * n + cell];
-      vv[a] = (ain * in[a * n + cell]) / ss[a];
+      vv[a] = (ain * (double)in[a * n + cell]) / ss[a];
     }
   }
   double msk[3], nsk[3];
@@ -324,13 +327,13 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
   const double z1 = gz * (Pi[3] * u[0] + Pi[4] * u[1] + Pi[5] * u[2]);
   const double z2 = gz * (Pi[6] * u[0] + Pi[7] * u[1] + Pi[8] * u[2]);
   if (scale_out) {
-    out[cell] = ss[0] * z0;
-    out[n + cell] = ss[1] * z1;
-    out[2 * n + cell] = ss[2] * z2;
+    out[cell] = (VT)(ss[0] * z0);
+    out[n + cell] = (VT)(ss[1] * z1);
+    out[2 * n + cell] = (VT)(ss[2] * z2);
   } else {  // block-Jacobi output for a further preconditioning stage
-    out[cell] = z0;
-    out[n + cell] = z1;
-    out[2 * n + cell] = z2;
+    out[cell] = (VT)z0;
+    out[n + cell] = (VT)z1;
+    out[2 * n + cell] = (VT)z2;
   }
 }
 
@@ -348,14 +351,20 @@ constexpr int AP_SLOTS = (TY + 2) * TX + (TY + 2) * 2;   // staged stencil slots
 constexpr int AP_PLANE = (TY + 2) * (TX + 2);            // doubles per stencil component
 constexpr int AP_CELLS = TX * TY;
 constexpr int AP_NT = TX * TY;
-__host__ __device__ constexpr int ap_buf_doubles(int jv_full) {
-  return 9 * AP_PLANE + (jv_full ? 3 : 0) * AP_CELLS;
+__host__ __device__ constexpr int ap_buf_doubles(int jv_full, int f32 = 0) {
+  // (an FP32 basis stages its input in a float plane after the doubles)
+  return 9 * AP_PLANE + (jv_full ? 3 : 0) * AP_CELLS + (f32 ? (3 * AP_PLANE + 1) / 2 : 0);
 }
 
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool ok) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
   const int sz = ok ? 8 : 0;   // 0: zero-fill, nothing read
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool ok) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  const int sz = ok ? 4 : 0;   // 0: zero-fill, nothing read
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(sz) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
@@ -365,25 +374,31 @@ __device__ __forceinline__ void ap_slot(int q, int& sx, int& sy) {
   else { const int r2 = q - (TY + 2) * TX; sy = r2 >> 1; sx = (r2 & 1) ? (TX + 1) : 0; }
 }
 
-__global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const double* __restrict__ in,
+template <typename VT = double>
+__global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const VT* __restrict__ in,
                                                            const double* __restrict__ s,
-                                                           double* __restrict__ out, const double* __restrict__ y,
+                                                           VT* __restrict__ out, const double* __restrict__ y,
                                                            const double* __restrict__ hd,
                                                            const double* __restrict__ pinv, double gamma,
                                                            int scale_out, const DevArgs* da, const double* in_a) {
   pdl_entry();
   extern __shared__ __align__(16) double apsm[];
-  if (da) {
-    in = da->arn_in;
-    out = da->arn_out;
-    gamma = da->gamma;
+  constexpr bool F32 = sizeof(VT) != sizeof(double);
+  if constexpr (!F32) {
+    if (da) {
+      in = da->arn_in;
+      out = da->arn_out;
+      gamma = da->gamma;
+    }
   }
   const double ain = kscale_of(in_a);   // the input is read as ain * in
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int n = P.ncell, ng = P.ng, ny = P.ny;
   const int gx = (ng + TX - 1) / TX, ntiles = gx * ((ny + TY - 1) / TY);
-  const int bufd = ap_buf_doubles(P.jv_full);
+  const int bufd = ap_buf_doubles(P.jv_full, F32 ? 1 : 0);
+  const int foff = ap_buf_doubles(P.jv_full);   // the float staging plane (FP32 basis)
   typedef double Plane[TY + 2][TX + 2];
+  typedef float FPlane[TY + 2][TX + 2];
 
   auto issue = [&](int t, double* B) {
     const int x0 = (t % gx) * TX, y0 = (t / gx) * TY;
@@ -399,7 +414,12 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
 #pragma unroll
       for (int a = 0; a < 3; a++) {
         cp_async8(&Y[a][sy][sx], y + a * (long long)n + cell, ok);
-        cp_async8(&V[a][sy][sx], in + a * (long long)n + cell, ok);
+        if constexpr (F32) {
+          FPlane* Fv = reinterpret_cast<FPlane*>(B + foff);
+          cp_async4(&Fv[a][sy][sx], in + a * (long long)n + cell, ok);
+        } else {
+          cp_async8(&V[a][sy][sx], in + a * (long long)n + cell, ok);
+        }
         cp_async8(&S[a][sy][sx], s + a * (long long)n + cell, ok);
       }
     }
@@ -437,8 +457,15 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
       ap_slot(q, sx, sy);
       int ii = x0 - 1 + sx, jj = y0 - 1 + sy;
       const bool ok = map_nb(ii, jj, ng, ny, P.bc);
+      if constexpr (F32) {
+        const FPlane* Fv = reinterpret_cast<const FPlane*>(B + foff);
 #pragma unroll
-      for (int a = 0; a < 3; a++) V[a][sy][sx] = ok ? 1.0 * ((ain * V[a][sy][sx]) / S[a][sy][sx]) : 0.0;
+        for (int a = 0; a < 3; a++)
+          V[a][sy][sx] = ok ? 1.0 * ((ain * (double)Fv[a][sy][sx]) / S[a][sy][sx]) : 0.0;
+      } else {
+#pragma unroll
+        for (int a = 0; a < 3; a++) V[a][sy][sx] = ok ? 1.0 * ((ain * V[a][sy][sx]) / S[a][sy][sx]) : 0.0;
+      }
     }
     __syncthreads();
     if (cok) {
@@ -480,13 +507,13 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
       const double z1 = g * (Pi[3] * u[0] + Pi[4] * u[1] + Pi[5] * u[2]);
       const double z2 = g * (Pi[6] * u[0] + Pi[7] * u[1] + Pi[8] * u[2]);
       if (scale_out) {
-        out[cell] = ss[0] * z0;
-        out[n + cell] = ss[1] * z1;
-        out[2 * n + cell] = ss[2] * z2;
+        out[cell] = (VT)(ss[0] * z0);
+        out[n + cell] = (VT)(ss[1] * z1);
+        out[2 * n + cell] = (VT)(ss[2] * z2);
       } else {
-        out[cell] = z0;
-        out[n + cell] = z1;
-        out[2 * n + cell] = z2;
+        out[cell] = (VT)z0;
+        out[n + cell] = (VT)z1;
+        out[2 * n + cell] = (VT)z2;
       }
     }
     __syncthreads();   // buffer b is refilled by the next iteration's issue
@@ -496,12 +523,13 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const d
 
 // the Arnoldi operator's input vt = (a in) / s, for the demag derivative of
 // LLG_JV_FULL_DEMAG (the same arithmetic as the operator's staging)
-__global__ void k_arnoldi_input(const double* __restrict__ in, const double* __restrict__ s, const double* in_a,
+template <typename VT = double>
+__global__ void k_arnoldi_input(const VT* __restrict__ in, const double* __restrict__ s, const double* in_a,
                                 double* __restrict__ vt, long long n3) {
   pdl_entry();
   const double ain = kscale_of(in_a);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
-    vt[i] = 1.0 * ((ain * in[i]) / s[i]);
+    vt[i] = 1.0 * ((ain * (double)in[i]) / s[i]);
 }
 
 int grid_1d(const llg_ctx* c, long long work, int block) {
@@ -578,51 +606,71 @@ int launch_psolve(llg_ctx* c, const double* r, double* z, const DevArgs* da) {
 
 int arnoldi_setup(llg_ctx* c) {
   const size_t smax = 2 * sizeof(double) * ap_buf_doubles(1);
-  if (cudaFuncSetAttribute((const void*)k_arnoldi_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax) !=
-      cudaSuccess) {
+  const size_t smaxf = 2 * sizeof(double) * ap_buf_doubles(1, 1);
+  if (cudaFuncSetAttribute((const void*)k_arnoldi_pipe<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smax) != cudaSuccess ||
+      cudaFuncSetAttribute((const void*)k_arnoldi_pipe<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smaxf) != cudaSuccess) {
     llg_set_error("arnoldi operator: shared-memory opt-in failed");
     return LLG_ERR_CUDA;
   }
   const long long ntiles = (long long)((c->p.ng + TX - 1) / TX) * ((c->p.ny + TY - 1) / TY);
   for (int jf = 0; jf < 2; jf++) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_pipe, AP_NT,
+    int per_sm = 0, per_sm_f = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi_pipe<double>, AP_NT,
                                                       2 * sizeof(double) * ap_buf_doubles(jf)) != cudaSuccess ||
-        per_sm < 1) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_arnoldi_pipe<float>, AP_NT,
+                                                      2 * sizeof(double) * ap_buf_doubles(jf, 1)) != cudaSuccess ||
+        per_sm < 1 || per_sm_f < 1) {
       llg_set_error("arnoldi operator: occupancy query failed");
       return LLG_ERR_CUDA;
     }
     c->arn_grid[jf] = (int)std::min<long long>(ntiles, (long long)per_sm * c->num_sms);
+    c->arn_grid_f[jf] = (int)std::min<long long>(ntiles, (long long)per_sm_f * c->num_sms);
   }
   return 0;
 }
 
-int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out, const double* y,
-                      double gamma, int scale_out, const DevArgs* da, const double* in_a) {
+template <typename VT>
+static int arnoldi_op_impl(llg_ctx* c, const VT* in, const double* ewt, VT* out, const double* y, double gamma,
+                           int scale_out, const DevArgs* da, const double* in_a) {
   if (!c->have_setup && !da) { llg_set_error("arnoldi operator before psetup"); return LLG_ERR_STATE; }
   DevProblem P = c->dp;
   if (c->d_hv) {   // LLG_JV_FULL_DEMAG: demag field of the operator's input vt = (a in) / s
     if (da) { llg_set_error("the demag-derivative Jacobian runs on the host-driven integrator"); return LLG_ERR_NOTSUP; }
     LLG_COUNT(KID_ELEMWISE);
-    klaunch(k_arnoldi_input, grid_1d(c, c->neq, 256), 256, 0, c->stream, in, ewt, in_a, c->d_vt, (long long)c->neq);
+    klaunch(k_arnoldi_input<VT>, grid_1d(c, c->neq, 256), 256, 0, c->stream, in, ewt, in_a, c->d_vt,
+            (long long)c->neq);
     LLG_CUDA_TRY(cudaPeekAtLastError());
     const int rc = demag_apply(c, c->d_vt, c->d_hv);
     if (rc) return rc;
     P.jv_hv = c->d_hv;
   }
+  constexpr int f32 = sizeof(VT) != sizeof(double) ? 1 : 0;
   LLG_COUNT(KID_ARNOLDI);
   ktimer_mark(c, KID_ARNOLDI, true);
   if (c->dp.windowed) {
-    klaunch(k_arnoldi_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, P, in, ewt, out, y, c->d_hd, c->d_pinv,
+    klaunch(k_arnoldi_tile<VT>, tile_grid(c), dim3(TX, TY), 0, c->stream, P, in, ewt, out, y, c->d_hd, c->d_pinv,
             gamma, scale_out, da, in_a);
   } else {
     const int jf = c->dp.jv_full ? 1 : 0;
-    klaunch(k_arnoldi_pipe, c->arn_grid[jf], AP_NT, 2 * sizeof(double) * ap_buf_doubles(jf), c->stream, P, in,
-            ewt, out, y, c->d_hd, c->d_pinv, gamma, scale_out, da, in_a);
+    klaunch(k_arnoldi_pipe<VT>, f32 ? c->arn_grid_f[jf] : c->arn_grid[jf], AP_NT,
+            2 * sizeof(double) * ap_buf_doubles(jf, f32), c->stream, P, in, ewt, out, y, c->d_hd, c->d_pinv, gamma,
+            scale_out, da, in_a);
   }
   ktimer_mark(c, KID_ARNOLDI, false);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
+}
+
+int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out, const double* y,
+                      double gamma, int scale_out, const DevArgs* da, const double* in_a) {
+  return arnoldi_op_impl<double>(c, in, ewt, out, y, gamma, scale_out, da, in_a);
+}
+
+int launch_arnoldi_op_f(llg_ctx* c, const float* in, const double* ewt, float* out, const double* y, double gamma,
+                        const double* in_a) {
+  return arnoldi_op_impl<float>(c, in, ewt, out, y, gamma, 1, nullptr, in_a);
 }
 
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot) {

@@ -40,8 +40,15 @@ struct CoefPack {
   double c[MAXV];
 };
 
-template <int K>
-__global__ void __launch_bounds__(RT) k_dot_multi(const double* __restrict__ x, PtrPack Y, long long n,
+// Krylov basis vectors stored as VT (double, or float for the FP32-basis
+// Krylov solver); arithmetic and accumulation stay FP64
+template <typename T>
+struct VPack {
+  const T* p[MAXV];
+};
+
+template <int K, typename VT = double>
+__global__ void __launch_bounds__(RT) k_dot_multi(const VT* __restrict__ x, VPack<VT> Y, long long n,
                                                   double* partials, unsigned int* counter, double* out,
                                                   KScale ks) {
   pdl_entry();
@@ -58,9 +65,9 @@ __global__ void __launch_bounds__(RT) k_dot_multi(const double* __restrict__ x, 
 #pragma unroll
     for (int u = 0; u < UB; u++) {
       const long long i = i0 + u * st;
-      xv[u] = (i < n) ? x[i] : 0.0;
+      xv[u] = (i < n) ? (double)x[i] : 0.0;
 #pragma unroll
-      for (int k = 0; k < K; k++) yv[u][k] = (i < n) ? ya[k] * Y.p[k][i] : 0.0;
+      for (int k = 0; k < K; k++) yv[u][k] = (i < n) ? ya[k] * (double)Y.p[k][i] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < UB; u++)
@@ -154,10 +161,11 @@ __global__ void k_lin(double a, const double* __restrict__ x, double b, const do
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     z[i] = a * x[i] + b * y[i];
 }
-__global__ void k_scale(double a, const double* __restrict__ x, double* __restrict__ z, long long n) {
+template <typename VT = double>
+__global__ void k_scale(double a, const VT* __restrict__ x, VT* __restrict__ z, long long n) {
   pdl_entry();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    z[i] = a * x[i];
+    z[i] = (VT)(a * (double)x[i]);
 }
 __global__ void k_const(double a, double* __restrict__ z, long long n) {
   pdl_entry();
@@ -225,7 +233,9 @@ __global__ void k_scale_cols(int q, CoefPack f, MPtrPack zn, long long n) {
 // classical Gram-Schmidt update with the dots read on the device:
 // z = 1 z + sum_{i<k} (-dots_i) X_i, and sum z^2 (the arithmetic of
 // k_lincomb_norm with coefficients {1, -dots_0, ..., -dots_{k-1}})
-__global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double* __restrict__ dots, double* z,
+// (VT float: the stored, rounded values are what the norm sums)
+template <typename VT = double>
+__global__ void __launch_bounds__(RT) k_gs_update(int k, VPack<VT> X, const double* __restrict__ dots, VT* z,
                                                   long long n, double* partials, unsigned int* counter,
                                                   double* out, KScale ks, double* aout) {
   pdl_entry();
@@ -243,22 +253,23 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, PtrPack X, const double
   for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
     double s[UB];
 #pragma unroll
-    for (int u = 0; u < UB; u++) s[u] = (i0 + u * st < n) ? 1.0 * z[i0 + u * st] : 0.0;
+    for (int u = 0; u < UB; u++) s[u] = (i0 + u * st < n) ? 1.0 * (double)z[i0 + u * st] : 0.0;
 #pragma unroll
     for (int j = 0; j < MAXV - 1; j++)
       if (j < k) {
         double xv[UB];
         const double xa = xs[j];   // the scale of X_j (1 when stored normalised)
 #pragma unroll
-        for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * X.p[j][i0 + u * st] : 0.0;
+        for (int u = 0; u < UB; u++) xv[u] = (i0 + u * st < n) ? xa * (double)X.p[j][i0 + u * st] : 0.0;
 #pragma unroll
         for (int u = 0; u < UB; u++) s[u] = cf[j] * xv[u] + s[u];
       }
 #pragma unroll
     for (int u = 0; u < UB; u++)
       if (i0 + u * st < n) {
-        z[i0 + u * st] = s[u];
-        acc[0] += s[u] * s[u];
+        const VT sv = (VT)s[u];
+        z[i0 + u * st] = sv;
+        acc[0] += (double)sv * (double)sv;
       }
   }
   block_sum<1>(acc, sm);
@@ -319,25 +330,33 @@ void reductions_free(llg_ctx* c) {
   c->h_mail = c->d_mail = nullptr;
 }
 
-int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot, const KScale* ks) {
+template <typename VT>
+static int vdot_multi_impl(llg_ctx* c, int nvec, const VT* x, const VT* const* Y, int slot, const KScale* ks) {
   const KScale kz{};
   const KScale& kk = ks ? *ks : kz;
   if (nvec <= 0) return 0;
   if (nvec > 16) { llg_set_error("dot_multi: nvec > 16"); return LLG_ERR_ARG; }
-  PtrPack pk{};
+  VPack<VT> pk{};
   for (int k = 0; k < nvec; k++) pk.p[k] = Y[k];
   const long long n = c->neq;
   const int nb = red_blocks(n);
   double* out = c->d_scal + slot;
   switch (nvec) {
 #define DOTK(K) \
-  case K: LLG_COUNT(KID_REDUCE); klaunch(k_dot_multi<K>, nb, RT, 0, c->stream, x, pk, n, c->d_red, c->d_counter, out, kk); break;
+  case K: LLG_COUNT(KID_REDUCE); klaunch(k_dot_multi<K, VT>, nb, RT, 0, c->stream, x, pk, n, c->d_red, c->d_counter, out, kk); break;
     DOTK(1) DOTK(2) DOTK(3) DOTK(4) DOTK(5) DOTK(6) DOTK(7) DOTK(8)
     DOTK(9) DOTK(10) DOTK(11) DOTK(12) DOTK(13) DOTK(14) DOTK(15) DOTK(16)
 #undef DOTK
   }
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
+}
+
+int vdot_multi_dev(llg_ctx* c, int nvec, const double* x, const double* const* Y, int slot, const KScale* ks) {
+  return vdot_multi_impl<double>(c, nvec, x, Y, slot, ks);
+}
+int vdot_multi_dev_f(llg_ctx* c, int nvec, const float* x, const float* const* Y, int slot, const KScale* ks) {
+  return vdot_multi_impl<float>(c, nvec, x, Y, slot, ks);
 }
 
 int vwrms_dev(llg_ctx* c, const double* x, const double* w, int slot) {
@@ -387,17 +406,26 @@ int fetch_range(llg_ctx* c, int lo, int hi) {
   return 0;
 }
 
-int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss, const KScale* ks,
-                   int slot_aout) {
+template <typename VT>
+static int vgs_update_impl(llg_ctx* c, int k, VT* const* V, int slot_dots, int slot_ss, const KScale* ks,
+                           int slot_aout) {
   if (k < 1 || k > MAXV - 1) { llg_set_error("gs_update: bad k"); return LLG_ERR_ARG; }
-  PtrPack pk{};
+  VPack<VT> pk{};
   for (int j = 0; j < k; j++) pk.p[j] = V[j];
   const KScale kz{};
   LLG_COUNT(KID_REDUCE);
-  klaunch(k_gs_update, red_blocks(c->neq), RT, 0, c->stream, k, pk, c->d_scal + slot_dots, V[k], c->neq, c->d_red,
+  klaunch(k_gs_update<VT>, red_blocks(c->neq), RT, 0, c->stream, k, pk, c->d_scal + slot_dots, V[k], c->neq, c->d_red,
           c->d_counter, c->d_scal + slot_ss, ks ? *ks : kz, slot_aout >= 0 ? c->d_scal + slot_aout : nullptr);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
+}
+int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss, const KScale* ks,
+                   int slot_aout) {
+  return vgs_update_impl<double>(c, k, V, slot_dots, slot_ss, ks, slot_aout);
+}
+int vgs_update_dev_f(llg_ctx* c, int k, float* const* V, int slot_dots, int slot_ss, const KScale* ks,
+                     int slot_aout) {
+  return vgs_update_impl<float>(c, k, V, slot_dots, slot_ss, ks, slot_aout);
 }
 
 int fetch_scalars(llg_ctx* c, int slot, int n, double* out) {
@@ -413,9 +441,15 @@ int vlin(llg_ctx* c, double a, const double* x, double b, const double* y, doubl
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
+int vscale_f(llg_ctx* c, double a, const float* x, float* z) {
+  LLG_COUNT(KID_ELEMWISE);
+  klaunch(k_scale<float>, ew_grid(c, c->neq), 256, 0, c->stream, a, x, z, c->neq);
+  LLG_CUDA_TRY(cudaPeekAtLastError());
+  return 0;
+}
 int vscale(llg_ctx* c, double a, const double* x, double* z) {
   LLG_COUNT(KID_ELEMWISE);
-  klaunch(k_scale, ew_grid(c, c->neq), 256, 0, c->stream, a, x, z, c->neq);
+  klaunch(k_scale<double>, ew_grid(c, c->neq), 256, 0, c->stream, a, x, z, c->neq);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

@@ -92,6 +92,7 @@ struct llg_ctx {
   int device = 0;
   int num_sms = 148;
   int arn_grid[2] = {0, 0};   // persistent Arnoldi operator: CTAs (without / with the demag field staged)
+  int arn_grid_f[2] = {0, 0}; // the same for an FP32 Krylov basis
 
   // geometry
   uint8_t* d_act = nullptr;
@@ -159,6 +160,9 @@ int arnoldi_setup(llg_ctx* c);   // shared-memory opt-in and grid of the persist
 int launch_arnoldi_op(llg_ctx* c, const double* in, const double* ewt, double* out,
                       const double* y, double gamma, int scale_out = 1, const DevArgs* da = nullptr,
                       const double* in_a = nullptr);
+// the same operator on an FP32 Krylov basis (host-driven integrator only)
+int launch_arnoldi_op_f(llg_ctx* c, const float* in, const double* ewt, float* out, const double* y, double gamma,
+                        const double* in_a);
 int rhs_full(llg_ctx* c, double t, double* y, double* ydot);
 // value of the soft source at t into c->dp.src_h (the field the next RHS,
 // residual and setup launches add at the source column)
@@ -237,6 +241,20 @@ int fetch_range(llg_ctx* c, int lo, int hi);
 // the vector's pre-update sum of squares at d_scal[slot_dots + k])
 int vgs_update_dev(llg_ctx* c, int k, double* const* V, int slot_dots, int slot_ss, const KScale* ks = nullptr,
                    int slot_aout = -1);
+// FP32 Krylov basis (LLG_KRYLOV_FP32): the basis is stored as float, every
+// product and sum is formed in FP64
+int vdot_multi_dev_f(llg_ctx* c, int nvec, const float* x, const float* const* Y, int slot,
+                     const KScale* ks = nullptr);
+int vgs_update_dev_f(llg_ctx* c, int k, float* const* V, int slot_dots, int slot_ss, const KScale* ks = nullptr,
+                     int slot_aout = -1);
+int vscale_f(llg_ctx* c, double a, const float* x, float* z);
+int fused_psolve_scale_dot_f(llg_ctx* c, const double* r, const double* ewt, float* v0, int slot, int slot_aout);
+int fused_lincomb_norm_f(llg_ctx* c, int nv, const double* coef, const float* const* X, float* z, int slot,
+                         const KScale* ks = nullptr);
+int fused_lincomb_div_f(llg_ctx* c, int nv, const double* coef, const float* const* X, const double* w, double* z,
+                        const KScale* ks = nullptr);
+int fused_lincomb_update_f(llg_ctx* c, int nv, const double* coef, const float* const* X, const double* w,
+                           double* del, bool ycor_zero, double* ycor, int slot, const KScale* ks = nullptr);
 double vmaxnorm_host(llg_ctx* c, const double* x);
 int vlin(llg_ctx* c, double a, const double* x, double b, const double* y, double* z);
 int vscale(llg_ctx* c, double a, const double* x, double* z);

@@ -33,6 +33,7 @@ DEMAG_OFF, DEMAG_PERIODIC, DEMAG_OPEN = 0, 1, 2
 DEMAG_FP64, DEMAG_MIXED = 0, 1
 JV_REFERENCE, JV_FULL_FIELD, JV_FULL_DEMAG = 0, 1, 2
 GS_AUTO, GS_CLASSICAL, GS_MODIFIED = 0, 1, 2
+KRYLOV_FP64, KRYLOV_FP32 = 0, 1
 PREC_BLOCK_JACOBI, PREC_LEARNED = 0, 1
 GEOM_BULK, GEOM_HOLE_SQUARE, GEOM_RING, GEOM_POLYCRYSTAL, GEOM_CUSTOM, GEOM_ELLIPSE, GEOM_ANNULUS, GEOM_SLIT = range(8)
 IC_UNIFORM, IC_HEAD_ON_STRIPES, IC_TWO_DOMAIN, IC_GRAIN_BUMPS, IC_CUSTOM, IC_TWO_DOMAIN_X, IC_VORTEX, IC_NEEL = range(8)
@@ -63,7 +64,7 @@ class SolverOpts(C.Structure):
     _fields_ = [
         ("rtol", C.c_double), ("atol", C.c_double), ("maxl", C.c_int32), ("maxord", C.c_int32),
         ("gs_type", C.c_int32), ("mxstep", C.c_int32), ("device_resident", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("krylov_precision", C.c_int32),
     ]
 
 
@@ -91,7 +92,7 @@ class Stats(C.Structure):
 class CkptInfo(C.Structure):
     _fields_ = [
         ("magic", C.c_char * 8), ("version", C.c_uint32), ("header_bytes", C.c_uint32),
-        ("scalar_bytes", C.c_uint32), ("reserved0", C.c_uint32), ("ng", C.c_int32), ("ny", C.c_int32),
+        ("scalar_bytes", C.c_uint32), ("krylov_precision", C.c_uint32), ("ng", C.c_int32), ("ny", C.c_int32),
         ("neq", C.c_int64), ("qmax", C.c_int32), ("maxl", C.c_int32), ("classical_gs", C.c_int32),
         ("mxstep", C.c_int32), ("device_resident", C.c_int32), ("have_setup", C.c_int32),
         ("rtol", C.c_double), ("atol", C.c_double), ("gamma_setup", C.c_double), ("tn", C.c_double),

@@ -143,8 +143,17 @@ typedef struct llg_solver_opts {
   int32_t gs_type;         /* LLG_GS_*                                            */
   int32_t mxstep;          /* max internal steps per llg_integrate call (500)     */
   int32_t device_resident; /* 1: whole step loop on the device (CUDA graph)       */
-  int32_t reserved0;
+  int32_t krylov_precision;/* LLG_KRYLOV_FP64 (0) | LLG_KRYLOV_FP32 (1)           */
 } llg_solver_opts;
+/* Storage of the SPGMR Krylov basis.  FP32 halves the basis traffic of the
+ * Arnoldi operator, the Gram-Schmidt dots and update and the final
+ * correction; every product, dot and sum is still formed in FP64, and the
+ * state, the norms and the Newton update stay FP64.  Host-driven integrator
+ * with classical Gram-Schmidt and block-Jacobi only (LLG_ERR_NOTSUP
+ * otherwise; the device-resident form is not used with it).  No reference
+ * counterpart (SUNDIALS keeps the basis in the state's precision).         */
+#define LLG_KRYLOV_FP64       0
+#define LLG_KRYLOV_FP32       1
 
 /* counters, same meaning as PrintFinalStats (2d_i2/2d_fft.cu:414-435) */
 typedef struct llg_stats {
@@ -295,7 +304,7 @@ int  llg_set_control_op_limit(llg_ctx* ctx, int64_t limit);
  * save its weights with llg_learned_get_weights).                         */
 typedef struct llg_ckpt_info {
   char     magic[8];             /* "LLGCKPT1"                               */
-  uint32_t version, header_bytes, scalar_bytes, reserved0;
+  uint32_t version, header_bytes, scalar_bytes, krylov_precision;
   int32_t  ng, ny;
   int64_t  neq;
   int32_t  qmax, maxl, classical_gs, mxstep, device_resident, have_setup;

@@ -228,3 +228,41 @@ def test_replayed_mixed_form_within_1e4_of_fp64(gpu):
         dm = float(np.abs(x - y).max())
         print(f"replayed mixed vs FP64, t={t}: max|dm| = {dm:.3e}")
         assert dm <= 1e-4
+
+
+def test_fp32_krylov_basis_tracks_fp64_basis(gpu):
+    """LLG_KRYLOV_FP32 stores the SPGMR basis in FP32 (products and sums in
+    FP64).  On the stable hole + open-demag film, replaying the FP64-basis
+    run's steps, the final states agree to far below the integration
+    tolerance and GMRES needs about as many iterations per Newton
+    iteration.  Unsupported combinations are refused."""
+    import torch
+    p, geo = _hole(alpha=0.2, prec=llg.DEMAG_MIXED)
+    y0 = torch.from_numpy(geo["y0"]).cuda()
+    a = _ctx(p, geo)
+    a.integrator_init(0.0, y0, llg.default_solver_opts())
+    a.record_steps(100000)
+    ya = _run(torch, a, 1, 20, torch.zeros_like(y0))
+    h, q = a.recorded_steps()
+    b = _ctx(p, geo)
+    b.integrator_init(0.0, y0, llg.default_solver_opts(krylov_precision=llg.KRYLOV_FP32))
+    b.replay_steps(h, q)
+    yb = _run(torch, b, 1, 20, torch.zeros_like(y0))
+    sa, sb = a.stats(), b.stats()
+    dm = float(np.abs(ya - yb).max())
+    ia, ib = sa["nli"] / sa["nni"], sb["nli"] / sb["nni"]
+    print(f"FP32 vs FP64 Krylov basis: max|dm| {dm:.2e}, GMRES/Newton {ia:.3f} vs {ib:.3f}")
+    assert dm <= 1e-6
+    assert abs(ib - ia) <= 0.05 * ia + 0.05
+    # its own step selection also works
+    c = _ctx(p, geo)
+    c.integrator_init(0.0, y0, llg.default_solver_opts(krylov_precision=llg.KRYLOV_FP32))
+    yc = _run(torch, c, 1, 20, torch.zeros_like(y0))
+    assert np.isfinite(yc).all() and float(np.abs(yc - ya).max()) <= 1e-3
+    with pytest.raises(llg.LLGError, match="LLG_ERR_NOTSUP|failed with status -105"):
+        _ctx(p, geo).integrator_init(0.0, y0, llg.default_solver_opts(krylov_precision=llg.KRYLOV_FP32,
+                                                                      gs_type=llg.GS_MODIFIED))
+    pl = llg.default_params(p.ng, p.ny, demag_mode=llg.DEMAG_OPEN, demag_strength=4.0, alpha=0.2,
+                            norm_kind=llg.NORM_REG, precond_kind=llg.PREC_LEARNED)
+    with pytest.raises(llg.LLGError):
+        _ctx(pl, geo).integrator_init(0.0, y0, llg.default_solver_opts(krylov_precision=llg.KRYLOV_FP32))
