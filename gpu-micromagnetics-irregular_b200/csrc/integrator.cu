@@ -1595,7 +1595,7 @@ int integrator_batch_prepare(llg_ctx* c, DevInteg** d_out, DState* hs_out) {
   if (!ok_dev) {
     llg_set_error("batch graph: an instance uses a setting the device-resident step graph does not cover "
                   "(modified Gram-Schmidt, learned preconditioner, harvesting, replay/recording, a source "
-                  "term or the demag-derivative Jacobian)");
+                  "term, the demag-derivative Jacobian or an FP32 Krylov basis)");
     return LLG_ERR_NOTSUP;
   }
   if (!b->dev) {
