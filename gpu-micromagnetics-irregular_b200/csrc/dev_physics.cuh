@@ -146,6 +146,11 @@ __device__ __forceinline__ void block_inverse(const DevProblem& P, const double 
 }
 
 // the block inverse of one cell stored by psetup (9 planes of n doubles)
+// (the FP32-basis Krylov solver stores it in FP32)
+__device__ __forceinline__ void load_pinv(const float* __restrict__ pinv, int n, int cell, double Pi[9]) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) Pi[k] = (double)pinv[(long long)k * n + cell];
+}
 __device__ __forceinline__ void load_pinv(const double* __restrict__ pinv, int n, int cell, double Pi[9]) {
 #pragma unroll
   for (int k = 0; k < 9; k++) Pi[k] = pinv[(long long)k * n + cell];

@@ -1229,6 +1229,12 @@ int integrator_create(llg_ctx* c, double t0, const double* y0, const llg_solver_
   b->indx_acor = b->qmax;
   if (c->integ) { c->integ->free_all(); delete c->integ; }
   c->integ = b;
+  // the FP32-basis operator reads an FP32 block inverse: psetup stores that
+  // precision from now on (every step sequence starts with a setup)
+  if (c->pinv_f32 != (b->kf32 ? 1 : 0)) {
+    c->pinv_f32 = b->kf32 ? 1 : 0;
+    c->have_setup = 0;
+  }
   return 0;
 }
 

@@ -181,7 +181,7 @@ __global__ void k_jtv_compact(DevProblem P, const double* __restrict__ v, double
 __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const double* __restrict__ y,
                                                          const double* __restrict__ hd, double* __restrict__ pm,
                                                          double* __restrict__ ph, double* __restrict__ pinv,
-                                                         double gamma, const DevArgs* da) {
+                                                         double gamma, const DevArgs* da, int pinv_f32) {
   pdl_entry();
   if (da && !da->run_setup) return;
   if (da) gamma = da->gamma_setup;
@@ -205,8 +205,14 @@ __global__ void __launch_bounds__(TX * TY) k_psetup_tile(DevProblem P, const dou
   const double ws = P.windowed ? P.w[cell] : 1.0;
   double Pi[9];
   block_inverse(P, m, h, msk, ws, gamma, Pi);
+  if (pinv_f32) {
+    float* pf = reinterpret_cast<float*>(pinv);
 #pragma unroll
-  for (int k = 0; k < 9; k++) pinv[(long long)k * n + cell] = Pi[k];
+    for (int k = 0; k < 9; k++) pf[(long long)k * n + cell] = (float)Pi[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; k++) pinv[(long long)k * n + cell] = Pi[k];
+  }
 }
 
 
@@ -240,7 +246,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
                                                           const double* __restrict__ s,
                                                           VT* __restrict__ out, const double* __restrict__ y,
                                                           const double* __restrict__ hd,
-                                                          const double* __restrict__ pinv, double gamma,
+                                                          const VT* __restrict__ pinv, double gamma,
                                                           int scale_out, const DevArgs* da, const double* in_a) {
   pdl_entry();
   __shared__ Tile<2> T;
@@ -379,7 +385,7 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const V
                                                            const double* __restrict__ s,
                                                            VT* __restrict__ out, const double* __restrict__ y,
                                                            const double* __restrict__ hd,
-                                                           const double* __restrict__ pinv, double gamma,
+                                                           const VT* __restrict__ pinv, double gamma,
                                                            int scale_out, const DevArgs* da, const double* in_a) {
   pdl_entry();
   extern __shared__ __align__(16) double apsm[];
@@ -589,7 +595,7 @@ int launch_jtv(llg_ctx* c, const double* v, double* Jv, const double* y) {
 int launch_psetup(llg_ctx* c, const double* y, double gamma, const DevArgs* da) {
   LLG_COUNT(KID_PSETUP);
   klaunch(k_psetup_tile, tile_grid(c), dim3(TX, TY), 0, c->stream, c->dp, y, c->d_hd, c->d_pm, c->d_ph, c->d_pinv,
-          gamma, da);
+          gamma, da, c->pinv_f32);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   c->gamma_setup = gamma;
   c->have_setup = 1;
@@ -647,16 +653,20 @@ static int arnoldi_op_impl(llg_ctx* c, const VT* in, const double* ewt, VT* out,
     P.jv_hv = c->d_hv;
   }
   constexpr int f32 = sizeof(VT) != sizeof(double) ? 1 : 0;
+  if (f32 != c->pinv_f32) {
+    llg_set_error("arnoldi operator: block inverse stored in the other precision (psetup first)");
+    return LLG_ERR_STATE;
+  }
   LLG_COUNT(KID_ARNOLDI);
   ktimer_mark(c, KID_ARNOLDI, true);
   if (c->dp.windowed) {
-    klaunch(k_arnoldi_tile<VT>, tile_grid(c), dim3(TX, TY), 0, c->stream, P, in, ewt, out, y, c->d_hd, c->d_pinv,
-            gamma, scale_out, da, in_a);
+    klaunch(k_arnoldi_tile<VT>, tile_grid(c), dim3(TX, TY), 0, c->stream, P, in, ewt, out, y, c->d_hd,
+            reinterpret_cast<const VT*>(c->d_pinv), gamma, scale_out, da, in_a);
   } else {
     const int jf = c->dp.jv_full ? 1 : 0;
     klaunch(k_arnoldi_pipe<VT>, f32 ? c->arn_grid_f[jf] : c->arn_grid[jf], AP_NT,
-            2 * sizeof(double) * ap_buf_doubles(jf, f32), c->stream, P, in, ewt, out, y, c->d_hd, c->d_pinv, gamma,
-            scale_out, da, in_a);
+            2 * sizeof(double) * ap_buf_doubles(jf, f32), c->stream, P, in, ewt, out, y, c->d_hd,
+            reinterpret_cast<const VT*>(c->d_pinv), gamma, scale_out, da, in_a);
   }
   ktimer_mark(c, KID_ARNOLDI, false);
   LLG_CUDA_TRY(cudaPeekAtLastError());

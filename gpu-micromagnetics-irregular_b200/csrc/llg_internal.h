@@ -112,6 +112,7 @@ struct llg_ctx {
   double* d_vt = nullptr;    // LLG_JV_FULL_DEMAG: the Arnoldi operator's scaled input (3N)
   double gamma_setup = 0.0;
   int have_setup = 0;
+  int pinv_f32 = 0;          // d_pinv holds FP32 values (the FP32-basis Krylov solver's operator)
 
   // reductions
   double* d_red = nullptr;      // partial sums scratch (17 x 1024 doubles)
