@@ -81,9 +81,10 @@ def bench_config(args, world):
             "parallelism": f"replicas x{world}", "l2": "state > 126 MB L2 (>= 20 vectors x 18.9 MB); no flush"}
 
 
-def algorithmic_bytes(kid, ng, ny, dims, mixed=False):
+def algorithmic_bytes(kid, ng, ny, dims, mixed=False, kf32=False):
     """Compulsory HBM bytes of one launch of kernel family kid (FP64 state;
-    the mixed demag chain keeps its spectra and tensor spectra in FP32)."""
+    the mixed demag chain keeps its spectra and tensor spectra in FP32; an
+    FP32 Krylov basis halves V and the operator's block inverse)."""
     n = ng * ny
     px, py, hx, nrows = dims
     S = 3 * hx * nrows * (8 if mixed else 16)
@@ -91,7 +92,9 @@ def algorithmic_bytes(kid, ng, ny, dims, mixed=False):
         return 24 * n + 24 * n + n + 24 * n
     if kid == 1:   # jtv: y, v, mask in; Jv out
         return 24 * n + 24 * n + n + 24 * n
-    if kid == 2:   # arnoldi: V_l, ewt, y, stored block inverse (9 doubles), mask in; V_l+1 out
+    if kid == 2:   # arnoldi: V_l, ewt, y, stored block inverse (9 values), mask in; V_l+1 out
+        if kf32:
+            return 12 * n + 24 * n + 24 * n + 36 * n + n + 12 * n
         return 3 * 24 * n + 72 * n + n + 24 * n
     if kid == 3:   # psetup: y, hd, mask in; m, h, block inverse out
         return 24 * n + 24 * n + n + 48 * n + 72 * n
@@ -332,7 +335,7 @@ def timed_run(args, form, world, rank, local, lib, clocks=True, gs=None):
             "ran": ran}
 
 
-def roofline_for(lib, run, ng, ny, mixed):
+def roofline_for(lib, run, ng, ny, mixed, kf32=False):
     """Roofline of the kernel with the largest live device-time share in the
     timed region: algorithmic bytes per launch / its live average launch time
     (CUDA events around each launch on the integrator's stream)."""
@@ -354,13 +357,13 @@ def roofline_for(lib, run, ng, ny, mixed):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
-    abytes = algorithmic_bytes(kid, ng, ny, dd, mixed)
+    abytes = algorithmic_bytes(kid, ng, ny, dd, mixed, kf32)
     avg_ms = live[dom]["total_ms"] / live[dom]["launches"]
     achieved = abytes / (avg_ms * 1e-3) / 1e9
     traffic = None
     try:
         with open(os.path.join(REPO, "profiles", "traffic_per_launch.json")) as f:
-            traffic = json.load(f).get(("mixed:" if mixed else "") + dom)
+            traffic = json.load(f).get(("mixed32:" if kf32 else "mixed:" if mixed else "") + dom)
     except Exception:
         pass
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -485,7 +488,8 @@ def run_ours(args, world, rank, local):
     form = args.form or BEST_FORM
     ng, ny = 1536, 512
     main = timed_run(args, form, world, rank, local, lib)
-    roof = roofline_for(lib, main, ng, ny, FORMS[form]["demag_precision"] == llg.DEMAG_MIXED)
+    roof = roofline_for(lib, main, ng, ny, FORMS[form]["demag_precision"] == llg.DEMAG_MIXED,
+                        FORMS[form].get("krylov", llg.KRYLOV_FP64) == llg.KRYLOV_FP32)
     clk = main["clocks"].summary()
     main["ctx"].close()
     summary = {"form_ran": main["ran"], "value": main["value"]}
