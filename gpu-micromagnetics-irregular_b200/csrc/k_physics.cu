@@ -29,6 +29,10 @@
 
 #include <algorithm>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "llg_internal.h"
 #include "launch.h"
 #include "dev_physics.cuh"
@@ -637,6 +641,61 @@ int arnoldi_setup(llg_ctx* c) {
   return 0;
 }
 
+// Autotune of the persistent operator's grid: the first launch of a (grid
+// size, staged field, basis precision) shape times the kernel at 1, 2, ...
+// CTAs per SM up to the occupancy limit on the live buffers (each candidate
+// twice, the second timing kept) and keeps the fastest, process-wide.  The
+// grid does not change any cell's arithmetic; the candidates' outputs are
+// overwritten by the launch that follows.
+static std::mutex g_arn_mu;
+static std::map<std::tuple<int, int, int, int>, int> g_arn_tuned;
+
+template <typename VT>
+static int arnoldi_tune(llg_ctx* c, const DevProblem& P, int jf, const VT* in, const double* ewt, VT* out,
+                        const double* y, double gamma, int scale_out, const double* in_a, int* grid) {
+  constexpr int f32 = sizeof(VT) != sizeof(double) ? 1 : 0;
+  const auto key = std::make_tuple(c->p.ng, c->p.ny, jf, f32);
+  {
+    std::lock_guard<std::mutex> g(g_arn_mu);
+    auto it = g_arn_tuned.find(key);
+    if (it != g_arn_tuned.end()) { *grid = it->second; return 0; }
+  }
+  const long long ntiles = (long long)((c->p.ng + TX - 1) / TX) * ((c->p.ny + TY - 1) / TY);
+  const int gmax = *grid;
+  const size_t smem = 2 * sizeof(double) * ap_buf_doubles(jf, f32);
+  cudaEvent_t e0, e1;
+  LLG_CUDA_TRY(cudaEventCreate(&e0));
+  LLG_CUDA_TRY(cudaEventCreate(&e1));
+  int best = gmax;
+  float best_ms = 1e30f;
+  for (int per = 1; per * c->num_sms <= gmax + c->num_sms - 1; per++) {
+    const int gsz = (int)std::min<long long>({ntiles, (long long)per * c->num_sms, (long long)gmax});
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; rep++) {
+      cudaEventRecord(e0, c->stream);
+      k_arnoldi_pipe<VT><<<gsz, AP_NT, smem, c->stream>>>(P, in, ewt, out, y, c->d_hd,
+                                                          reinterpret_cast<const VT*>(c->d_pinv), gamma, scale_out,
+                                                          nullptr, in_a);
+      cudaEventRecord(e1, c->stream);
+    }
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      LLG_CUDA_TRY(cudaGetLastError());
+      return LLG_ERR_CUDA;
+    }
+    if (ms < best_ms) { best_ms = ms; best = gsz; }
+    if (gsz >= gmax) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  pdl_break();
+  *grid = best;
+  std::lock_guard<std::mutex> g(g_arn_mu);
+  g_arn_tuned[key] = best;
+  return 0;
+}
+
 template <typename VT>
 static int arnoldi_op_impl(llg_ctx* c, const VT* in, const double* ewt, VT* out, const double* y, double gamma,
                            int scale_out, const DevArgs* da, const double* in_a) {
@@ -664,7 +723,13 @@ static int arnoldi_op_impl(llg_ctx* c, const VT* in, const double* ewt, VT* out,
             reinterpret_cast<const VT*>(c->d_pinv), gamma, scale_out, da, in_a);
   } else {
     const int jf = c->dp.jv_full ? 1 : 0;
-    klaunch(k_arnoldi_pipe<VT>, f32 ? c->arn_grid_f[jf] : c->arn_grid[jf], AP_NT,
+    int& grid = f32 ? c->arn_grid_f[jf] : c->arn_grid[jf];
+    if (!da && !c->capturing && !(f32 ? c->arn_tuned_f[jf] : c->arn_tuned[jf])) {
+      const int rc = arnoldi_tune<VT>(c, P, jf, in, ewt, out, y, gamma, scale_out, in_a, &grid);
+      if (rc) return rc;
+      (f32 ? c->arn_tuned_f[jf] : c->arn_tuned[jf]) = 1;
+    }
+    klaunch(k_arnoldi_pipe<VT>, grid, AP_NT,
             2 * sizeof(double) * ap_buf_doubles(jf, f32), c->stream, P, in, ewt, out, y, c->d_hd,
             reinterpret_cast<const VT*>(c->d_pinv), gamma, scale_out, da, in_a);
   }

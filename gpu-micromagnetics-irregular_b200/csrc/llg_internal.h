@@ -93,6 +93,7 @@ struct llg_ctx {
   int num_sms = 148;
   int arn_grid[2] = {0, 0};   // persistent Arnoldi operator: CTAs (without / with the demag field staged)
   int arn_grid_f[2] = {0, 0}; // the same for an FP32 Krylov basis
+  int arn_tuned[2] = {0, 0}, arn_tuned_f[2] = {0, 0};   // grid autotuned (first host-path launch)
 
   // geometry
   uint8_t* d_act = nullptr;
