@@ -17,8 +17,8 @@
 // code cannot pass the array's name to a kernel (in host code the name is a
 // host-side stand-in, not a device address), so the first call on each
 // device looks up the device address with cudaGetSymbolAddress, with that
-// device current, and caches it per device ordinal; that first call should
-// come before any stream capture.  The cached address belongs to the CUDA
+// device current, and caches it per device ordinal; that first call makes
+// this one synchronous runtime call, later calls make none.  The cached address belongs to the CUDA
 // runtime's primary context of the device: callers that make another
 // driver-API context current on the same device must not use this entry
 // point from it.  All calls share the array and it keeps the last call's

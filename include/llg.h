@@ -235,8 +235,8 @@ int  llg_wrms_norm(llg_ctx* ctx, const double* d_x, const double* d_w, double* h
  * nvec > LLG_NOALLOC_MAX_VECS is rejected (LLG_ERR_ARG).  The first call on
  * a device looks up the array's device address (cudaGetSymbolAddress) in
  * the CUDA runtime's primary context of that device and caches it: use the
- * entry point from that context only, and make the first call on a device
- * before any stream capture.  Calls share the array: calls that overlap on
+ * entry point from that context only; later calls on the device make no
+ * such runtime call.  Calls share the array: calls that overlap on
  * the GPU race.  Same result, bit for bit, as llg_dot_multi for the same
  * vectors (same block partition, per-thread order and reduction tree).      */
 #define LLG_NOALLOC_MAX_VECS   16
