@@ -2,8 +2,8 @@
 // (double for the FP64 demag chain, float for the mixed-precision chain).
 //
 // Natural order in and out, no reordering tables: each pass stages the
-// thread's radix-R butterflies (R = 8/4/2/3/5; any other prime through a
-// generic path) in registers, synchronises, applies twiddles and the
+// thread's radix-R butterflies (R = 16/8/4/2, 12/6, 3, 5; any other prime
+// through a generic path) in registers, synchronises, applies twiddles and the
 // in-register DFT, and scatters to (j / Ns)·Ns·R + j % Ns + r·Ns.
 #pragma once
 #include <cuda_runtime.h>
@@ -17,8 +17,10 @@ template <> struct Cx<double> { using T = double2; };
 template <> struct Cx<float> { using T = float2; };
 template <typename R> using cx_t = typename Cx<R>::T;
 
+#define FFT_HD __host__ __device__ __forceinline__
+
 template <typename R>
-__device__ __forceinline__ cx_t<R> mk(R a, R b) {
+FFT_HD cx_t<R> mk(R a, R b) {
   cx_t<R> v;
   v.x = a;
   v.y = b;
@@ -47,16 +49,16 @@ template <typename R>
 __host__ __device__ constexpr int padded_len(int n) { return n + (n >> (sizeof(R) == 8 ? 3 : 4)) + 1; }
 
 template <typename R>
-__device__ __forceinline__ cx_t<R> cmul(cx_t<R> a, cx_t<R> b) {
+FFT_HD cx_t<R> cmul(cx_t<R> a, cx_t<R> b) {
   return mk<R>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 template <typename R>
-__device__ __forceinline__ cx_t<R> cadd(cx_t<R> a, cx_t<R> b) { return mk<R>(a.x + b.x, a.y + b.y); }
+FFT_HD cx_t<R> cadd(cx_t<R> a, cx_t<R> b) { return mk<R>(a.x + b.x, a.y + b.y); }
 template <typename R>
-__device__ __forceinline__ cx_t<R> csub(cx_t<R> a, cx_t<R> b) { return mk<R>(a.x - b.x, a.y - b.y); }
+FFT_HD cx_t<R> csub(cx_t<R> a, cx_t<R> b) { return mk<R>(a.x - b.x, a.y - b.y); }
 // v * (SIGN < 0 ? -i : +i)
 template <typename R, int SIGN>
-__device__ __forceinline__ cx_t<R> rot90(cx_t<R> v) {
+FFT_HD cx_t<R> rot90(cx_t<R> v) {
   return (SIGN < 0) ? mk<R>(v.y, -v.x) : mk<R>(-v.y, v.x);
 }
 
@@ -69,13 +71,13 @@ __device__ __forceinline__ cx_t<R> twid(const FftPlanT<R>& pl, int idx) {
 
 // in-register DFTs, out[q] = sum_r v[r] exp(SIGN 2 pi i r q / R)
 template <typename R, int SIGN>
-__device__ __forceinline__ void dft2(cx_t<R>* v) {
+FFT_HD void dft2(cx_t<R>* v) {
   const cx_t<R> a = v[0], b = v[1];
   v[0] = cadd<R>(a, b);
   v[1] = csub<R>(a, b);
 }
 template <typename R, int SIGN>
-__device__ __forceinline__ void dft4(cx_t<R>* v) {
+FFT_HD void dft4(cx_t<R>* v) {
   const cx_t<R> a0 = cadd<R>(v[0], v[2]), a1 = csub<R>(v[0], v[2]);
   const cx_t<R> b0 = cadd<R>(v[1], v[3]), b1 = rot90<R, SIGN>(csub<R>(v[1], v[3]));
   v[0] = cadd<R>(a0, b0);
@@ -84,7 +86,7 @@ __device__ __forceinline__ void dft4(cx_t<R>* v) {
   v[3] = csub<R>(a1, b1);
 }
 template <typename R, int SIGN>
-__device__ __forceinline__ void dft3(cx_t<R>* v) {
+FFT_HD void dft3(cx_t<R>* v) {
   const R c = R(-0.5), s = R(SIGN) * R(0.86602540378443864676);  // sin(2pi/3)
   const cx_t<R> t1 = cadd<R>(v[1], v[2]), t2 = csub<R>(v[1], v[2]);
   const cx_t<R> a = mk<R>(v[0].x + c * t1.x, v[0].y + c * t1.y);
@@ -94,7 +96,7 @@ __device__ __forceinline__ void dft3(cx_t<R>* v) {
   v[2] = csub<R>(a, b);
 }
 template <typename R, int SIGN>
-__device__ __forceinline__ void dft5(cx_t<R>* v) {
+FFT_HD void dft5(cx_t<R>* v) {
   const R c1 = R(0.30901699437494742410), c2 = R(-0.80901699437494742410);
   const R s1 = R(SIGN) * R(0.95105651629515357212), s2 = R(SIGN) * R(0.58778525229247312917);
   const cx_t<R> t1 = cadd<R>(v[1], v[4]), t2 = cadd<R>(v[2], v[3]);
@@ -110,7 +112,7 @@ __device__ __forceinline__ void dft5(cx_t<R>* v) {
   v[3] = mk<R>(a2.x + b2.y, a2.y - b2.x);
 }
 template <typename R, int SIGN>
-__device__ __forceinline__ void dft8(cx_t<R>* v) {
+FFT_HD void dft8(cx_t<R>* v) {
   const R h = R(0.70710678118654752440);
   cx_t<R> e[4] = {v[0], v[2], v[4], v[6]};
   cx_t<R> o[4] = {v[1], v[3], v[5], v[7]};
@@ -128,13 +130,131 @@ __device__ __forceinline__ void dft8(cx_t<R>* v) {
   v[3] = cadd<R>(e[3], o3);
   v[7] = csub<R>(e[3], o3);
 }
+// v * (c + SIGN i s), a constant rotation
+template <typename R, int SIGN>
+FFT_HD cx_t<R> crot(cx_t<R> v, R c, R s) {
+  const R ss = R(SIGN) * s;
+  return mk<R>(v.x * c - v.y * ss, v.x * ss + v.y * c);
+}
+// Composite radices as two in-register stages (Cooley-Tukey, R = A x B):
+// index r = B n1 + n2, frequency q = k1 + A k2; the inner DFT_A runs over n1
+// for every n2, the products take the constant twiddles w_R^(n2 k1), the
+// outer DFT_B runs over n2 for every k1.
+template <typename R, int SIGN>
+FFT_HD void dft6(cx_t<R>* v) {   // 6 = 2 x 3
+  const R h = R(0.5), t = R(0.86602540378443864676);   // cos, sin of 2 pi / 6
+  cx_t<R> a[3][2];
+#pragma unroll
+  for (int n2 = 0; n2 < 3; n2++) {
+    a[n2][0] = v[n2];
+    a[n2][1] = v[3 + n2];
+    dft2<R, SIGN>(a[n2]);
+  }
+  a[1][1] = crot<R, SIGN>(a[1][1], h, t);      // w6^1
+  a[2][1] = crot<R, SIGN>(a[2][1], -h, t);     // w6^2
+#pragma unroll
+  for (int k1 = 0; k1 < 2; k1++) {
+    cx_t<R> b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+    dft3<R, SIGN>(b);
+#pragma unroll
+    for (int k2 = 0; k2 < 3; k2++) v[k1 + 2 * k2] = b[k2];
+  }
+}
+template <typename R, int SIGN>
+FFT_HD void dft12(cx_t<R>* v) {  // 12 = 4 x 3
+  const R h = R(0.5), t = R(0.86602540378443864676);   // cos, sin of 2 pi / 6
+  cx_t<R> a[3][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 3; n2++) {
+#pragma unroll
+    for (int n1 = 0; n1 < 4; n1++) a[n2][n1] = v[3 * n1 + n2];
+    dft4<R, SIGN>(a[n2]);
+  }
+  a[1][1] = crot<R, SIGN>(a[1][1], t, h);      // w12^1
+  a[1][2] = crot<R, SIGN>(a[1][2], h, t);      // w12^2
+  a[1][3] = rot90<R, SIGN>(a[1][3]);           // w12^3
+  a[2][1] = crot<R, SIGN>(a[2][1], h, t);      // w12^2
+  a[2][2] = crot<R, SIGN>(a[2][2], -h, t);     // w12^4
+  a[2][3] = mk<R>(-a[2][3].x, -a[2][3].y);     // w12^6
+#pragma unroll
+  for (int k1 = 0; k1 < 4; k1++) {
+    cx_t<R> b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+    dft3<R, SIGN>(b);
+#pragma unroll
+    for (int k2 = 0; k2 < 3; k2++) v[k1 + 4 * k2] = b[k2];
+  }
+}
+template <typename R, int SIGN>
+FFT_HD void dft16(cx_t<R>* v) {  // 16 = 4 x 4
+  const R c1 = R(0.92387953251128675613), s1 = R(0.38268343236508977173);   // cos, sin of pi / 8
+  const R h = R(0.70710678118654752440);
+  cx_t<R> a[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; n2++) {
+#pragma unroll
+    for (int n1 = 0; n1 < 4; n1++) a[n2][n1] = v[4 * n1 + n2];
+    dft4<R, SIGN>(a[n2]);
+  }
+  a[1][1] = crot<R, SIGN>(a[1][1], c1, s1);    // w16^1
+  a[1][2] = crot<R, SIGN>(a[1][2], h, h);      // w16^2
+  a[1][3] = crot<R, SIGN>(a[1][3], s1, c1);    // w16^3
+  a[2][1] = crot<R, SIGN>(a[2][1], h, h);      // w16^2
+  a[2][2] = rot90<R, SIGN>(a[2][2]);           // w16^4
+  a[2][3] = crot<R, SIGN>(a[2][3], -h, h);     // w16^6
+  a[3][1] = crot<R, SIGN>(a[3][1], s1, c1);    // w16^3
+  a[3][2] = crot<R, SIGN>(a[3][2], -h, h);     // w16^6
+  a[3][3] = crot<R, SIGN>(a[3][3], -c1, -s1);  // w16^9
+#pragma unroll
+  for (int k1 = 0; k1 < 4; k1++) {
+    cx_t<R> b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+    dft4<R, SIGN>(b);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = b[k2];
+  }
+}
 template <typename R, int RAD, int SIGN>
-__device__ __forceinline__ void dft_fixed(cx_t<R>* v) {
+FFT_HD void dft_fixed(cx_t<R>* v) {
   if constexpr (RAD == 2) dft2<R, SIGN>(v);
   else if constexpr (RAD == 3) dft3<R, SIGN>(v);
   else if constexpr (RAD == 4) dft4<R, SIGN>(v);
   else if constexpr (RAD == 5) dft5<R, SIGN>(v);
+  else if constexpr (RAD == 6) dft6<R, SIGN>(v);
   else if constexpr (RAD == 8) dft8<R, SIGN>(v);
+  else if constexpr (RAD == 12) dft12<R, SIGN>(v);
+  else if constexpr (RAD == 16) dft16<R, SIGN>(v);
+}
+
+// v[r] *= w^(r * jm * tstride), r = 1..RAD-1 (the twiddles of butterfly jm
+// of a pass with span Ns; jm * tstride < n / RAD)
+template <typename R, int RAD, int SIGN>
+__device__ __forceinline__ void apply_twiddles(cx_t<R>* v, const FftPlanT<R>& pl, int jm, int tstride) {
+  if constexpr (RAD <= 8) {
+    // one table load per butterfly; higher powers in registers
+    const cx_t<R> w1 = twid<R, SIGN>(pl, jm * tstride);
+    cx_t<R> wr = w1;
+#pragma unroll
+    for (int r = 1; r < RAD; r++) {
+      v[r] = cmul<R>(v[r], wr);
+      if (r + 1 < RAD) wr = cmul<R>(wr, w1);
+    }
+  } else {
+    // w^1, w^2, w^4, w^8 from the table (r * jm * tstride < n for r < RAD);
+    // every other power is a product of at most three of them, so no power
+    // carries a long chain of roundings
+    const int b = jm * tstride;
+    const cx_t<R> w1 = twid<R, SIGN>(pl, b), w2 = twid<R, SIGN>(pl, 2 * b);
+    const cx_t<R> w4 = twid<R, SIGN>(pl, 4 * b), w8 = twid<R, SIGN>(pl, 8 * b);
+#pragma unroll
+    for (int r = 1; r < RAD; r++) {
+      cx_t<R> wr;
+      bool have = false;
+      if (r & 1) { wr = w1; have = true; }
+      if (r & 2) { wr = have ? cmul<R>(wr, w2) : w2; have = true; }
+      if (r & 4) { wr = have ? cmul<R>(wr, w4) : w4; have = true; }
+      if (r & 8) { wr = have ? cmul<R>(wr, w8) : w8; }
+      v[r] = cmul<R>(v[r], wr);
+    }
+  }
 }
 
 // One Stockham pass of one transform held in buf[0..n).  All threads of the
@@ -164,16 +284,7 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
       int q, jm;
       if (lg >= 0) { q = j >> lg; jm = j & (Ns - 1); }
       else { q = j / Ns; jm = j - q * Ns; }
-      if (Ns > 1 && jm != 0) {
-        // one table load per butterfly; higher powers in registers
-        const cx_t<R> w1 = twid<R, SIGN>(pl, jm * tstride);
-        cx_t<R> wr = w1;
-#pragma unroll
-        for (int r = 1; r < RAD; r++) {
-          v[u][r] = cmul<R>(v[u][r], wr);
-          if (r + 1 < RAD) wr = cmul<R>(wr, w1);
-        }
-      }
+      if (Ns > 1 && jm != 0) apply_twiddles<R, RAD, SIGN>(v[u], pl, jm, tstride);
       dft_fixed<R, RAD, SIGN>(v[u]);
       const int ob = q * Ns * RAD + jm;
 #pragma unroll
@@ -181,6 +292,57 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
     }
   }
   __syncthreads();
+}
+
+// The first pass (span 1: no twiddles, butterfly j writes j·R .. j·R + R-1)
+// with its inputs taken from ld(i) instead of from buf, so the input never
+// makes a round trip through shared memory.  HALF: the inputs i >= n/2 are
+// known to be zero (an open-boundary row, zero-padded to twice its length)
+// and the butterflies' upper halves are not loaded or computed.
+template <typename R, int RAD, int SIGN, int EPT, bool PAD, bool HALF, typename LD>
+__device__ __forceinline__ void stockham_first_pass_ld(cx_t<R>* buf, const FftPlanT<R>& pl, LD&& ld) {
+  constexpr int MB = (EPT + RAD - 1) / RAD;
+  static_assert(!HALF || RAD % 2 == 0, "HALF needs an even radix");
+  const int nb = pl.n / RAD;
+#pragma unroll
+  for (int u = 0; u < MB; u++) {
+    const int j = threadIdx.x + u * blockDim.x;
+    if (j < nb) {
+      cx_t<R> v[RAD];
+#pragma unroll
+      for (int r = 0; r < RAD; r++) v[r] = (HALF && 2 * r >= RAD) ? mk<R>(R(0), R(0)) : ld(j + r * nb);
+      dft_fixed<R, RAD, SIGN>(v);
+#pragma unroll
+      for (int r = 0; r < RAD; r++) buf[fpad<R, PAD>(j * RAD + r)] = v[r];
+    }
+  }
+  __syncthreads();
+}
+
+// The last pass (span n/R: butterfly j = jm writes jm + r·n/R) with its
+// outputs handed to st(i, value) instead of written back to buf.  HALF: only
+// the outputs i < n/2 are wanted (the kept half of an open-boundary row), so
+// the upper half of every butterfly is neither stored nor, where the
+// compiler can drop it, computed.  buf is only read: no barrier follows.
+template <typename R, int RAD, int SIGN, int EPT, bool PAD, bool HALF, typename ST>
+__device__ __forceinline__ void stockham_last_pass_st(const cx_t<R>* buf, const FftPlanT<R>& pl, int4 ps, ST&& st) {
+  constexpr int MB = (EPT + RAD - 1) / RAD;
+  static_assert(!HALF || RAD % 2 == 0, "HALF needs an even radix");
+  const int nb = pl.n / RAD, Ns = ps.y;   // Ns = nb here
+#pragma unroll
+  for (int u = 0; u < MB; u++) {
+    const int j = threadIdx.x + u * blockDim.x;
+    if (j < nb) {
+      cx_t<R> v[RAD];
+#pragma unroll
+      for (int r = 0; r < RAD; r++) v[r] = buf[fpad<R, PAD>(j + r * nb)];
+      if (Ns > 1 && j != 0) apply_twiddles<R, RAD, SIGN>(v, pl, j, 1);
+      dft_fixed<R, RAD, SIGN>(v);
+#pragma unroll
+      for (int r = 0; r < RAD; r++)
+        if (!HALF || 2 * r < RAD) st(j + r * Ns, v[r]);
+    }
+  }
 }
 
 // Any other radix (small primes, test sizes only): one butterfly per thread
@@ -211,18 +373,23 @@ __device__ void stockham_pass_generic(cx_t<R>* buf, const FftPlanT<R>& pl, int4 
 
 // Natural-order in, natural-order out, in place in buf (this row's transform).
 // Every thread of the block must call it (it synchronises).  The passes run
-// as straight-line regions in factorisation order (8s, one 4, one 2, 3s, 5s,
-// other primes): a runtime switch over radices inside one loop makes the
-// register allocator keep every variant's state live at once.
+// as straight-line regions in factorisation order (16s, one 8, one 4, one 2,
+// one 12 or 6, 3s, 5s, other primes): a runtime switch over radices inside
+// one loop makes the register allocator keep every variant's state live at
+// once.
+// Passes [p, pe) of the plan (default: all of them).
 template <typename R, int SIGN, int EPT, bool PAD = false>
-__device__ void fft_stockham(cx_t<R>* buf, const FftPlanT<R>& pl) {
-  int p = 0;
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<R, 8, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
-  if (p < pl.nr && __ldg(&pl.pass[p].x) == 4) { stockham_pass<R, 4, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  if (p < pl.nr && __ldg(&pl.pass[p].x) == 2) { stockham_pass<R, 2, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<R, 3, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<R, 5, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pl.nr; p++) stockham_pass_generic<R, SIGN, PAD>(buf, pl, __ldg(&pl.pass[p]));
+__device__ void fft_stockham(cx_t<R>* buf, const FftPlanT<R>& pl, int p = 0, int pe = -1) {
+  if (pe < 0) pe = pl.nr;
+  for (; p < pe && __ldg(&pl.pass[p].x) == 16; p++) stockham_pass<R, 16, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pe && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<R, 8, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  if (p < pe && __ldg(&pl.pass[p].x) == 4) { stockham_pass<R, 4, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  if (p < pe && __ldg(&pl.pass[p].x) == 2) { stockham_pass<R, 2, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  if (p < pe && __ldg(&pl.pass[p].x) == 12) { stockham_pass<R, 12, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  if (p < pe && __ldg(&pl.pass[p].x) == 6) { stockham_pass<R, 6, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  for (; p < pe && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<R, 3, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pe && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<R, 5, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pe; p++) stockham_pass_generic<R, SIGN, PAD>(buf, pl, __ldg(&pl.pass[p]));
 }
 
 }  // namespace

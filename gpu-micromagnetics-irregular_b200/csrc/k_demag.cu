@@ -73,7 +73,8 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
   cx_t<R>* buf = sm + b * np;
   const double* src = in + (long long)c * comp_stride;
   const int ya = y0 + 2 * b, yb = ya + 1;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  // packed input element i: rows ya (real part) and yb (imaginary part)
+  auto load_in = [&](int i) -> cx_t<R> {
     double va = 0.0, vb = 0.0;
     if (i < row_len) {
       if (ya < nrows) {
@@ -85,10 +86,25 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
         vb = src[q] * (w ? w[q] : 1.0);
       }
     }
-    buf[fpad<R, true>(i)] = mk<R>((R)va, (R)vb);
+    return mk<R>((R)va, (R)vb);
+  };
+  // The first pass reads its inputs from HBM directly; an open-boundary row
+  // (row_len <= n/2) skips the zero-padded upper half of every butterfly.
+  const int r0 = __ldg(&pl.pass[0].x);
+  const bool half = 2 * row_len <= n;
+  int p0 = 1;
+  if (r0 == 16) {
+    if (half) stockham_first_pass_ld<R, 16, -1, EPT, true, true>(buf, pl, load_in);
+    else stockham_first_pass_ld<R, 16, -1, EPT, true, false>(buf, pl, load_in);
+  } else if (r0 == 8) {
+    if (half) stockham_first_pass_ld<R, 8, -1, EPT, true, true>(buf, pl, load_in);
+    else stockham_first_pass_ld<R, 8, -1, EPT, true, false>(buf, pl, load_in);
+  } else {
+    p0 = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) buf[fpad<R, true>(i)] = load_in(i);
+    __syncthreads();
   }
-  __syncthreads();
-  fft_stockham<R, -1, EPT, true>(buf, pl);
+  fft_stockham<R, -1, EPT, true>(buf, pl, p0);
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int e = tid; e < Hx * 2 * NB; e += T) {
     const int kx = e / (2 * NB), r = e - kx * (2 * NB);
@@ -227,8 +243,36 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
   }
   __syncthreads();
   C* buf = sm + b * np;
-  fft_stockham<R, +1, EPT, true>(buf, pl);
   double* dst = h + (long long)c * comp_stride;
+  // The last pass writes the kept outputs i < ng of rows ya (real part) and
+  // yb (imaginary part) to HBM directly; an open-boundary row (ng <= n/2)
+  // forms only the lower half of every butterfly.
+  const int ya = y0 + 2 * b, yb = ya + 1;
+  auto st = [&](int i, C z) {
+    if (i < ng) {
+      if (ya < nrows) dst[(long long)ya * ng + i] = (double)z.x;
+      if (yb < nrows) dst[(long long)yb * ng + i] = (double)z.y;
+    }
+  };
+  const int nr = pl.nr;
+  const int4 pz = __ldg(&pl.pass[nr - 1]);
+  const bool half = 2 * ng <= n;
+#define LAST_PASS(RAD)                                                        \
+  do {                                                                        \
+    fft_stockham<R, +1, EPT, true>(buf, pl, 0, nr - 1);                        \
+    if (half) stockham_last_pass_st<R, RAD, +1, EPT, true, true>(buf, pl, pz, st); \
+    else stockham_last_pass_st<R, RAD, +1, EPT, true, false>(buf, pl, pz, st);     \
+  } while (0)
+  switch (pz.x) {
+    case 16: LAST_PASS(16); return;
+    case 12: LAST_PASS(12); return;
+    case 8: LAST_PASS(8); return;
+    case 6: LAST_PASS(6); return;
+    case 4: LAST_PASS(4); return;
+    default: break;
+  }
+#undef LAST_PASS
+  fft_stockham<R, +1, EPT, true>(buf, pl);
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
 #pragma unroll
   for (int r = 0; r < NB * 2; r++) {
@@ -388,6 +432,12 @@ __global__ void k_tensor_finish(const double2* __restrict__ Sxx, const double2* 
 // ── host side ───────────────────────────────────────────────────────────
 static constexpr int kRowsNB = 1;  // packed transforms per row-CTA at init (tensor spectra)
 
+// radices with an in-register DFT (stockham_pass); any other prime takes
+// the generic pass, one thread per butterfly
+static bool fixed_radix(int r) {
+  return r == 2 || r == 3 || r == 4 || r == 5 || r == 6 || r == 8 || r == 12 || r == 16;
+}
+
 struct HostFft {
   int n = 0, tx = 32, ept = 8;
   std::vector<int> radix;
@@ -399,7 +449,7 @@ struct HostFft {
   int tx_for(int e) const {
     int need = (n + e - 1) / e;
     for (int r : radix)
-      if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) need = std::max(need, n / r);
+      if (!fixed_radix(r)) need = std::max(need, n / r);
     return ((std::max(need, 32) + 31) / 32) * 32;
   }
   template <typename R>
@@ -451,9 +501,18 @@ struct DemagPlan {
 static int factorize(int n, std::vector<int>& rad) {
   rad.clear();
   int m = n;
-  while (m % 8 == 0) { rad.push_back(8); m /= 8; }
-  while (m % 4 == 0) { rad.push_back(4); m /= 4; }
-  while (m % 2 == 0) { rad.push_back(2); m /= 2; }
+  // the order fft_stockham runs the passes in: 16s, the rest of the power
+  // of two as one 8, 4 or 2 — or, with a factor 3, one 12 or 6 — then 3s,
+  // 5s and other primes (3072 = 16.16.12: three shared-memory passes)
+  while (m % 16 == 0) { rad.push_back(16); m /= 16; }
+  int p2 = 1;
+  while (m % 2 == 0) { p2 *= 2; m /= 2; }
+  if ((p2 == 2 || p2 == 4) && m % 3 == 0) {
+    rad.push_back(3 * p2);
+    m /= 3;
+  } else if (p2 > 1) {
+    rad.push_back(p2);
+  }
   while (m % 3 == 0) { rad.push_back(3); m /= 3; }
   while (m % 5 == 0) { rad.push_back(5); m /= 5; }
   for (int p = 7; m > 1; p += 2) {
@@ -483,7 +542,7 @@ static int fft_init(HostFft& f, int n, int batch) {
   f.ept = (((n + 7) / 8 + 31) / 32 * 32 * batch <= 1024) ? 8 : 16;
   int need = (n + f.ept - 1) / f.ept;
   for (int r : f.radix)
-    if (r != 2 && r != 3 && r != 4 && r != 5 && r != 8) need = std::max(need, n / r);
+    if (!fixed_radix(r)) need = std::max(need, n / r);
   f.tx = ((std::max(need, 32) + 31) / 32) * 32;
   std::vector<double2> tw(n);
   std::vector<float2> twf(n);
