@@ -326,6 +326,65 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPackT<V
   finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
 }
 
+// k_lincomb_update with the vector count NV fixed at compile time: the loads
+// of all NV vectors (and of w, ycor) for the UB slice elements are issued
+// before any of them is used.  Per element the same operations in the same
+// order, so the result is bitwise that of k_lincomb_update.
+template <int NV, typename VT>
+__global__ void __launch_bounds__(RT) k_lincomb_update_k(CPack c, XPackT<VT> X, const double* __restrict__ w,
+                                                         double* del, const double* ycor_in, double* ycor,
+                                                         long long n, double* partials, unsigned int* counter,
+                                                         double* out, KScale ks) {
+  pdl_entry();
+  __shared__ double sm[2 * (RT / 32)];
+  __shared__ double xs[NV];
+  if (threadIdx.x < NV) xs[threadIdx.x] = kscale_of(ks.a[threadIdx.x]);
+  __syncthreads();
+  double cf[NV], xa[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    cf[k] = c.c[k];
+    xa[k] = xs[k];
+  }
+  double acc[2] = {0.0, 0.0};
+  const long long st = (long long)gridDim.x * RT;
+  for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
+    VT xr[NV][UB];
+    double wv[UB], yv[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const long long i = i0 + u * st;
+      const bool in = i < n;
+#pragma unroll
+      for (int k = 0; k < NV; k++) xr[k][u] = in ? X.p[k][i] : VT(0);
+      wv[u] = in ? w[i] : 1.0;
+      yv[u] = (in && ycor_in) ? ycor_in[i] : 0.0;
+    }
+    double s[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) s[u] = cf[0] * (xa[0] * (double)xr[0][u]);
+#pragma unroll
+    for (int k = 1; k < NV; k++)
+#pragma unroll
+      for (int u = 0; u < UB; u++) s[u] = cf[k] * (xa[k] * (double)xr[k][u]) + s[u];
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const long long i = i0 + u * st;
+      if (i >= n) continue;
+      const double wi = wv[u];
+      const double d = s[u] / wi;
+      if (del) del[i] = d;
+      const double yc = 1.0 * yv[u] + 1.0 * d;
+      ycor[i] = yc;
+      const double p = d * wi, q = yc * wi;
+      acc[0] += p * p;
+      acc[1] += q * q;
+    }
+  }
+  block_sum<2>(acc, sm);
+  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+}
+
 // sums (x1*w)^2 and ((a x2 + b x3)*w)^2
 __global__ void __launch_bounds__(RT) k_wrms2(const double* __restrict__ x1, double a, const double* __restrict__ x2,
                                               double b, const double* __restrict__ x3, const double* __restrict__ w,
@@ -621,9 +680,27 @@ static int lincomb_update_impl(llg_ctx* c, int nv, const double* coef, const VT*
   XPackT<VT> xp{};
   for (int k = 0; k < nv; k++) { cp.c[k] = coef[k]; xp.p[k] = X[k]; }
   const KScale kz{};
+  const KScale kk = ks ? *ks : kz;
   LLG_COUNT(KID_REDUCE);
-  klaunch(k_lincomb_update<VT>, red_blocks(c->neq), RT, 0, c->stream, nv, cp, xp, w, del, ycor_zero ? nullptr : ycor,
-          ycor, c->neq, c->d_red, c->d_counter, c->d_scal + slot, ks ? *ks : kz);
+  const int nb = red_blocks(c->neq);
+  const double* yin = ycor_zero ? nullptr : ycor;
+  double* out = c->d_scal + slot;
+#define LU_K(NV) klaunch(k_lincomb_update_k<NV, VT>, nb, RT, 0, c->stream, cp, xp, w, del, yin, ycor, c->neq, c->d_red, \
+                         c->d_counter, out, kk)
+  switch (nv) {
+    case 1: LU_K(1); break;
+    case 2: LU_K(2); break;
+    case 3: LU_K(3); break;
+    case 4: LU_K(4); break;
+    case 5: LU_K(5); break;
+    case 6: LU_K(6); break;
+    case 7: LU_K(7); break;
+    case 8: LU_K(8); break;
+    default:
+      klaunch(k_lincomb_update<VT>, nb, RT, 0, c->stream, nv, cp, xp, w, del, yin, ycor, c->neq, c->d_red,
+              c->d_counter, out, kk);
+  }
+#undef LU_K
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }

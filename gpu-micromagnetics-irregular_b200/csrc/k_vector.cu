@@ -278,6 +278,58 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, VPack<VT> X, const doub
   if (last && aout && threadIdx.x == 0) *aout = gs_scale_of(out[0], dots + k);
 }
 
+// k_gs_update with the vector count K fixed at compile time: the loads of
+// all K basis vectors (and of z) for the UB slice elements are issued before
+// any of them is used, where the runtime-k loop waits on one vector at a
+// time.  Per element the same operations in the same order, so the result is
+// bitwise that of k_gs_update.
+template <int K, typename VT>
+__global__ void __launch_bounds__(RT) k_gs_update_k(VPack<VT> X, const double* __restrict__ dots, VT* z, long long n,
+                                                    double* partials, unsigned int* counter, double* out, KScale ks,
+                                                    double* aout) {
+  pdl_entry();
+  __shared__ double sm[RT / 32];
+  __shared__ double xs[K];
+  if (threadIdx.x < K) xs[threadIdx.x] = kscale_of(ks.a[threadIdx.x]);
+  __syncthreads();
+  double cf[K], xa[K];
+#pragma unroll
+  for (int j = 0; j < K; j++) {
+    cf[j] = -dots[j];
+    xa[j] = xs[j];
+  }
+  double acc[1] = {0.0};
+  const long long st = (long long)gridDim.x * RT;
+  for (long long i0 = blockIdx.x * (long long)RT + threadIdx.x; i0 < n; i0 += UB * st) {
+    VT zr[UB], xr[K][UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const long long i = i0 + u * st;
+      const bool in = i < n;
+      zr[u] = in ? z[i] : VT(0);
+#pragma unroll
+      for (int j = 0; j < K; j++) xr[j][u] = in ? X.p[j][i] : VT(0);
+    }
+    double s[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) s[u] = 1.0 * (double)zr[u];
+#pragma unroll
+    for (int j = 0; j < K; j++)
+#pragma unroll
+      for (int u = 0; u < UB; u++) s[u] = cf[j] * (xa[j] * (double)xr[j][u]) + s[u];
+#pragma unroll
+    for (int u = 0; u < UB; u++)
+      if (i0 + u * st < n) {
+        const VT sv = (VT)s[u];
+        z[i0 + u * st] = sv;
+        acc[0] += (double)sv * (double)sv;
+      }
+  }
+  block_sum<1>(acc, sm);
+  const bool last = finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  if (last && aout && threadIdx.x == 0) *aout = gs_scale_of(out[0], dots + K);
+}
+
 // one warp copies d_scal[lo, hi) into the mapped host mailbox, makes the
 // copies visible to the host, then writes the sequence word last
 __global__ void k_publish(const double* __restrict__ src, int lo, int hi, double* mail,
@@ -414,8 +466,25 @@ static int vgs_update_impl(llg_ctx* c, int k, VT* const* V, int slot_dots, int s
   for (int j = 0; j < k; j++) pk.p[j] = V[j];
   const KScale kz{};
   LLG_COUNT(KID_REDUCE);
-  klaunch(k_gs_update<VT>, red_blocks(c->neq), RT, 0, c->stream, k, pk, c->d_scal + slot_dots, V[k], c->neq, c->d_red,
-          c->d_counter, c->d_scal + slot_ss, ks ? *ks : kz, slot_aout >= 0 ? c->d_scal + slot_aout : nullptr);
+  const int nb = red_blocks(c->neq);
+  const double* dots = c->d_scal + slot_dots;
+  double* ss = c->d_scal + slot_ss;
+  double* aout = slot_aout >= 0 ? c->d_scal + slot_aout : nullptr;
+  const KScale kk = ks ? *ks : kz;
+#define GS_K(K) klaunch(k_gs_update_k<K, VT>, nb, RT, 0, c->stream, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout)
+  switch (k) {
+    case 1: GS_K(1); break;
+    case 2: GS_K(2); break;
+    case 3: GS_K(3); break;
+    case 4: GS_K(4); break;
+    case 5: GS_K(5); break;
+    case 6: GS_K(6); break;
+    case 7: GS_K(7); break;
+    case 8: GS_K(8); break;
+    default:
+      klaunch(k_gs_update<VT>, nb, RT, 0, c->stream, k, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout);
+  }
+#undef GS_K
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
