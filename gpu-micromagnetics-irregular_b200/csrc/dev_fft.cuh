@@ -4,7 +4,10 @@
 // Natural order in and out, no reordering tables: each pass stages the
 // thread's radix-R butterflies (R = 16/8/4/2, 12/6, 3, 5; any other prime
 // through a generic path) in registers, synchronises, applies twiddles and the
-// in-register DFT, and scatters to (j / Ns)·Ns·R + j % Ns + r·Ns.
+// in-register DFT, and scatters to (j / Ns)·Ns·R + j % Ns + r·Ns.  A length
+// runs either a runtime plan (pass table in device memory) or, for the
+// lengths of kFixedLengths, a compile-time plan whose passes, spans and
+// shifts are constants of its kernel.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -27,9 +30,10 @@ FFT_HD cx_t<R> mk(R a, R b) {
   return v;
 }
 
-// Stockham plan for one transform length n.  Radices in pass order
-// (8/4/2 first so every power-of-two pass sees a power-of-two span Ns, then
-// 3, 5 and any other prime).  tx = threads per transform.
+// Stockham plan for one transform length n: the runtime pass table
+// (runtime_radices: 8/4/2 first so every power-of-two pass sees a
+// power-of-two span Ns, then 3, 5 and any other prime) and the twiddles, which
+// a compile-time plan uses too.  tx = threads per transform.
 template <typename R>
 struct FftPlanT {
   int n, nr, tx;
@@ -225,7 +229,7 @@ FFT_HD void dft_fixed(cx_t<R>* v) {
 }
 
 // v[r] *= w^(r * jm * tstride), r = 1..RAD-1 (the twiddles of butterfly jm
-// of a pass with span Ns; jm * tstride < n / RAD)
+// of a pass with span Ns; r * jm * tstride < n for r < RAD)
 template <typename R, int RAD, int SIGN>
 __device__ __forceinline__ void apply_twiddles(cx_t<R>* v, const FftPlanT<R>& pl, int jm, int tstride) {
   if constexpr (RAD <= 8) {
@@ -238,9 +242,8 @@ __device__ __forceinline__ void apply_twiddles(cx_t<R>* v, const FftPlanT<R>& pl
       if (r + 1 < RAD) wr = cmul<R>(wr, w1);
     }
   } else {
-    // w^1, w^2, w^4, w^8 from the table (r * jm * tstride < n for r < RAD);
-    // every other power is a product of at most three of them, so no power
-    // carries a long chain of roundings
+    // w^1, w^2, w^4, w^8 from the table; every other power is a product of
+    // at most three of them, so no power carries a long chain of roundings
     const int b = jm * tstride;
     const cx_t<R> w1 = twid<R, SIGN>(pl, b), w2 = twid<R, SIGN>(pl, 2 * b);
     const cx_t<R> w4 = twid<R, SIGN>(pl, 4 * b), w8 = twid<R, SIGN>(pl, 8 * b);
@@ -257,15 +260,16 @@ __device__ __forceinline__ void apply_twiddles(cx_t<R>* v, const FftPlanT<R>& pl
   }
 }
 
-// One Stockham pass of one transform held in buf[0..n).  All threads of the
-// row stage their butterflies in registers, the block synchronises, then
-// twiddle + DFT_R + scatter to (j / Ns)·Ns·R + j % Ns + r·Ns.
-// A row of tx threads covers n/R butterflies with at most MB each
-// (tx >= n/EPT is guaranteed by the plan).
+// One Stockham pass of one transform of length n held in buf[0..n), span Ns
+// (lg = log2 Ns, or -1).  All threads of the row stage their butterflies in
+// registers, the block synchronises, then twiddle + DFT_R + scatter to
+// (j / Ns)·Ns·R + j % Ns + r·Ns.  A row of tx threads covers n/R butterflies
+// with at most MB each (tx >= n/EPT is guaranteed by the plan).  n, Ns and
+// lg are arguments so that a compile-time plan (fft_fixed) folds them.
 template <typename R, int RAD, int SIGN, int EPT, bool PAD>
-__device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& pl, int4 ps) {
+__device__ __forceinline__ void stockham_pass_n(cx_t<R>* buf, const FftPlanT<R>& pl, int n, int Ns, int lg) {
   constexpr int MB = (EPT + RAD - 1) / RAD;
-  const int n = pl.n, nb = n / RAD, Ns = ps.y, lg = ps.z;
+  const int nb = n / RAD;
   const int tstride = n / (Ns * RAD);
   cx_t<R> v[MB][RAD];
 #pragma unroll
@@ -293,6 +297,10 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
   }
   __syncthreads();
 }
+template <typename R, int RAD, int SIGN, int EPT, bool PAD>
+__device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& pl, int4 ps) {
+  stockham_pass_n<R, RAD, SIGN, EPT, PAD>(buf, pl, pl.n, ps.y, ps.z);
+}
 
 // The first pass (span 1: no twiddles, butterfly j writes j·R .. j·R + R-1)
 // with its inputs taken from ld(i) instead of from buf, so the input never
@@ -300,10 +308,10 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
 // known to be zero (an open-boundary row, zero-padded to twice its length)
 // and the butterflies' upper halves are not loaded or computed.
 template <typename R, int RAD, int SIGN, int EPT, bool PAD, bool HALF, typename LD>
-__device__ __forceinline__ void stockham_first_pass_ld(cx_t<R>* buf, const FftPlanT<R>& pl, LD&& ld) {
+__device__ __forceinline__ void stockham_first_pass_ld(cx_t<R>* buf, int n, LD&& ld) {
   constexpr int MB = (EPT + RAD - 1) / RAD;
   static_assert(!HALF || RAD % 2 == 0, "HALF needs an even radix");
-  const int nb = pl.n / RAD;
+  const int nb = n / RAD;
 #pragma unroll
   for (int u = 0; u < MB; u++) {
     const int j = threadIdx.x + u * blockDim.x;
@@ -322,13 +330,13 @@ __device__ __forceinline__ void stockham_first_pass_ld(cx_t<R>* buf, const FftPl
 // The last pass (span n/R: butterfly j = jm writes jm + r·n/R) with its
 // outputs handed to st(i, value) instead of written back to buf.  HALF: only
 // the outputs i < n/2 are wanted (the kept half of an open-boundary row), so
-// the upper half of every butterfly is neither stored nor, where the
-// compiler can drop it, computed.  buf is only read: no barrier follows.
+// the upper half of every butterfly is not stored.  buf is only read: no
+// barrier follows.
 template <typename R, int RAD, int SIGN, int EPT, bool PAD, bool HALF, typename ST>
-__device__ __forceinline__ void stockham_last_pass_st(const cx_t<R>* buf, const FftPlanT<R>& pl, int4 ps, ST&& st) {
+__device__ __forceinline__ void stockham_last_pass_st(const cx_t<R>* buf, const FftPlanT<R>& pl, int n, ST&& st) {
   constexpr int MB = (EPT + RAD - 1) / RAD;
   static_assert(!HALF || RAD % 2 == 0, "HALF needs an even radix");
-  const int nb = pl.n / RAD, Ns = ps.y;   // Ns = nb here
+  const int nb = n / RAD;   // = the span of the last pass
 #pragma unroll
   for (int u = 0; u < MB; u++) {
     const int j = threadIdx.x + u * blockDim.x;
@@ -336,11 +344,11 @@ __device__ __forceinline__ void stockham_last_pass_st(const cx_t<R>* buf, const 
       cx_t<R> v[RAD];
 #pragma unroll
       for (int r = 0; r < RAD; r++) v[r] = buf[fpad<R, PAD>(j + r * nb)];
-      if (Ns > 1 && j != 0) apply_twiddles<R, RAD, SIGN>(v, pl, j, 1);
+      if (nb > 1 && j != 0) apply_twiddles<R, RAD, SIGN>(v, pl, j, 1);
       dft_fixed<R, RAD, SIGN>(v);
 #pragma unroll
       for (int r = 0; r < RAD; r++)
-        if (!HALF || 2 * r < RAD) st(j + r * Ns, v[r]);
+        if (!HALF || 2 * r < RAD) st(j + r * nb, v[r]);
     }
   }
 }
@@ -371,25 +379,100 @@ __device__ void stockham_pass_generic(cx_t<R>* buf, const FftPlanT<R>& pl, int4 
   __syncthreads();
 }
 
-// Natural-order in, natural-order out, in place in buf (this row's transform).
-// Every thread of the block must call it (it synchronises).  The passes run
-// as straight-line regions in factorisation order (16s, one 8, one 4, one 2,
-// one 12 or 6, 3s, 5s, other primes): a runtime switch over radices inside
-// one loop makes the register allocator keep every variant's state live at
-// once.
-// Passes [p, pe) of the plan (default: all of them).
-template <typename R, int SIGN, int EPT, bool PAD = false>
-__device__ void fft_stockham(cx_t<R>* buf, const FftPlanT<R>& pl, int p = 0, int pe = -1) {
-  if (pe < 0) pe = pl.nr;
-  for (; p < pe && __ldg(&pl.pass[p].x) == 16; p++) stockham_pass<R, 16, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pe && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<R, 8, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
-  if (p < pe && __ldg(&pl.pass[p].x) == 4) { stockham_pass<R, 4, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  if (p < pe && __ldg(&pl.pass[p].x) == 2) { stockham_pass<R, 2, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  if (p < pe && __ldg(&pl.pass[p].x) == 12) { stockham_pass<R, 12, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  if (p < pe && __ldg(&pl.pass[p].x) == 6) { stockham_pass<R, 6, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
-  for (; p < pe && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<R, 3, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pe && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<R, 5, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
-  for (; p < pe; p++) stockham_pass_generic<R, SIGN, PAD>(buf, pl, __ldg(&pl.pass[p]));
+// ── the two factorisations ──────────────────────────────────────────────
+// A runtime plan (any length; its pass table lives in device memory) runs 8s,
+// one 4, one 2, 3s, 5s and any other prime <= 64 (fft_stockham).  A
+// compile-time plan (fft_fixed, the lengths of kFixedLengths) runs 16s, the
+// rest of the power of two as one 8, 4 or 2 — or, with a factor 3, one 12
+// or 6 — then 3s and 5s: 3072 = 16.16.12 is three shared-memory passes.
+// Each length has exactly one plan, so results never depend on launch shape.
+struct RadixList {
+  int r[MAXR];
+  int nr;   // -1: not factorable (a prime factor > 64, or too many passes)
+};
+__host__ __device__ constexpr RadixList runtime_radices(int n) {
+  RadixList L{};
+  int m = n, k = 0;
+  // (after the 8s at most one 4 and one 2 remain)
+  const int small[5] = {8, 4, 2, 3, 5};
+  for (int s = 0; s < 5; s++) {
+    const int r = small[s];
+    while (m % r == 0) {
+      if (k >= MAXR) { L.nr = -1; return L; }
+      L.r[k++] = r;
+      m /= r;
+    }
+  }
+  for (int p = 7; m > 1; p += 2) {
+    while (m % p == 0) {
+      if (p > 64 || k >= MAXR) { L.nr = -1; return L; }
+      L.r[k++] = p;
+      m /= p;
+    }
+    if (p * p > m && m > 1) {
+      if (m > 64 || k >= MAXR) { L.nr = -1; return L; }
+      L.r[k++] = m;
+      m = 1;
+    }
+  }
+  L.nr = k;
+  return L;
 }
+__host__ __device__ constexpr RadixList fixed_radices(int n) {
+  RadixList L{};
+  int m = n, k = 0;
+  while (m % 16 == 0) { L.r[k++] = 16; m /= 16; }
+  int p2 = 1;
+  while (m % 2 == 0) { p2 *= 2; m /= 2; }
+  if ((p2 == 2 || p2 == 4) && m % 3 == 0) {
+    L.r[k++] = 3 * p2;
+    m /= 3;
+  } else if (p2 > 1) {
+    L.r[k++] = p2;
+  }
+  while (m % 3 == 0) { L.r[k++] = 3; m /= 3; }
+  while (m % 5 == 0) { L.r[k++] = 5; m /= 5; }
+  L.nr = (m == 1) ? k : -1;
+  return L;
+}
+__host__ __device__ constexpr int ilog2_or_neg(int x) {
+  if (x <= 0 || (x & (x - 1))) return -1;
+  int l = 0;
+  while ((1 << l) < x) l++;
+  return l;
+}
+
+// Natural-order in, natural-order out, in place in buf (this row's transform),
+// runtime plan.  Every thread of the block must call it (it synchronises).
+// The passes run as straight-line regions in factorisation order: a runtime
+// switch over radices inside one loop makes the register allocator keep every
+// variant's state live at once.
+template <typename R, int SIGN, int EPT, bool PAD = false>
+__device__ void fft_stockham(cx_t<R>* buf, const FftPlanT<R>& pl) {
+  int p = 0;
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 8; p++) stockham_pass<R, 8, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  if (p < pl.nr && __ldg(&pl.pass[p].x) == 4) { stockham_pass<R, 4, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  if (p < pl.nr && __ldg(&pl.pass[p].x) == 2) { stockham_pass<R, 2, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p])); p++; }
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 3; p++) stockham_pass<R, 3, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pl.nr && __ldg(&pl.pass[p].x) == 5; p++) stockham_pass<R, 5, SIGN, EPT, PAD>(buf, pl, __ldg(&pl.pass[p]));
+  for (; p < pl.nr; p++) stockham_pass_generic<R, SIGN, PAD>(buf, pl, __ldg(&pl.pass[p]));
+}
+
+// Compile-time plan of length N (fixed_radices): passes [P, PE) with span NS
+// at pass P, every size, span and shift folded into the code.  pl supplies
+// the twiddle table only.
+template <typename R, int SIGN, int EPT, bool PAD, int N, int P, int PE, int NS>
+__device__ __forceinline__ void fft_fixed(cx_t<R>* buf, const FftPlanT<R>& pl) {
+  if constexpr (P < PE) {
+    constexpr RadixList L = fixed_radices(N);
+    constexpr int RAD = L.r[P];
+    stockham_pass_n<R, RAD, SIGN, EPT, PAD>(buf, pl, N, NS, ilog2_or_neg(NS));
+    fft_fixed<R, SIGN, EPT, PAD, N, P + 1, PE, NS * RAD>(buf, pl);
+  }
+}
+
+// the lengths with a compile-time plan (their kernels are instantiated per
+// length); every other length takes the runtime plan
+constexpr int kFixedLengths[] = {1024, 2048, 3072, 4096};
 
 }  // namespace

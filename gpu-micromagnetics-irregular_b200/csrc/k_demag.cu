@@ -58,8 +58,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // ── K1: forward real transform of data rows along x ─────────────────────
 // CTA = (component c, 2*NB rows); threadIdx.y = packed transform (rows ya, ya+1).
-// The FP64 input is rounded to R on load (R = float: mixed chain).
-template <typename R, int NB, int EPT>
+// The FP64 input is rounded to R on load (R = float: mixed chain).  FIX > 0:
+// the compile-time plan of that length, whose first pass reads its inputs
+// from HBM directly and, for an open-boundary row (row_len <= n/2), skips the
+// zero-padded upper half of every butterfly; FIX = 0: the runtime plan.
+template <typename R, int NB, int EPT, int FIX>
 __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long long comp_stride, int row_len,
                            int nrows, const double* __restrict__ w, cx_t<R>* __restrict__ S, int ld, int Hx) {
   pdl_entry();
@@ -67,7 +70,7 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
   cx_t<R>* sm = reinterpret_cast<cx_t<R>*>(smraw);
   const int c = blockIdx.y;
   const int y0 = blockIdx.x * (2 * NB);
-  const int n = pl.n;
+  const int n = FIX > 0 ? FIX : pl.n;
   const int b = threadIdx.y;
   const int np = padded_len<R>(n);
   cx_t<R>* buf = sm + b * np;
@@ -88,23 +91,21 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
     }
     return mk<R>((R)va, (R)vb);
   };
-  // The first pass reads its inputs from HBM directly; an open-boundary row
-  // (row_len <= n/2) skips the zero-padded upper half of every butterfly.
-  const int r0 = __ldg(&pl.pass[0].x);
-  const bool half = 2 * row_len <= n;
-  int p0 = 1;
-  if (r0 == 16) {
-    if (half) stockham_first_pass_ld<R, 16, -1, EPT, true, true>(buf, pl, load_in);
-    else stockham_first_pass_ld<R, 16, -1, EPT, true, false>(buf, pl, load_in);
-  } else if (r0 == 8) {
-    if (half) stockham_first_pass_ld<R, 8, -1, EPT, true, true>(buf, pl, load_in);
-    else stockham_first_pass_ld<R, 8, -1, EPT, true, false>(buf, pl, load_in);
+  if constexpr (FIX > 0) {
+    constexpr RadixList L = fixed_radices(FIX);
+    constexpr int R0 = L.r[0];
+    if constexpr (R0 % 2 == 0) {
+      if (2 * row_len <= FIX) stockham_first_pass_ld<R, R0, -1, EPT, true, true>(buf, FIX, load_in);
+      else stockham_first_pass_ld<R, R0, -1, EPT, true, false>(buf, FIX, load_in);
+    } else {
+      stockham_first_pass_ld<R, R0, -1, EPT, true, false>(buf, FIX, load_in);
+    }
+    fft_fixed<R, -1, EPT, true, FIX, 1, L.nr, R0>(buf, pl);
   } else {
-    p0 = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) buf[fpad<R, true>(i)] = load_in(i);
     __syncthreads();
+    fft_stockham<R, -1, EPT, true>(buf, pl);
   }
-  fft_stockham<R, -1, EPT, true>(buf, pl, p0);
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int e = tid; e < Hx * 2 * NB; e += T) {
     const int kx = e / (2 * NB), r = e - kx * (2 * NB);
@@ -120,12 +121,19 @@ __global__ void k_rows_fwd(FftPlanT<R> pl, const double* __restrict__ in, long l
   }
 }
 
+// the column transform of one CTA row (a runtime or a compile-time plan)
+template <typename R, int SIGN, int EPT, int FIX>
+__device__ __forceinline__ void col_fft(cx_t<R>* buf, const FftPlanT<R>& pl) {
+  if constexpr (FIX > 0) fft_fixed<R, SIGN, EPT, false, FIX, 0, fixed_radices(FIX).nr, 1>(buf, pl);
+  else fft_stockham<R, SIGN, EPT>(buf, pl);
+}
+
 // ── K2: column transform + tensor multiply + inverse column transform ─────
 // CTA = one x-frequency column; threadIdx.y = component.  The three spectrum
 // columns and (STAGE) this column's tensor spectra are fetched with
 // asynchronous copies (cp.async) at entry, so the tensor read overlaps the
 // forward transform instead of stalling the multiply.
-template <typename R, int EPT, bool STAGE>
+template <typename R, int EPT, bool STAGE, int FIX>
 __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
                             const R* __restrict__ txx, const R* __restrict__ tyy, const R* __restrict__ tzz,
                             const cx_t<R>* __restrict__ txy) {
@@ -134,7 +142,7 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int kx = blockIdx.x;
-  const int n = pl.n;
+  const int n = FIX > 0 ? FIX : pl.n;
   const int c = threadIdx.y;
   C* buf = sm + c * n;
   C* col = S + ((long long)c * Hx + kx) * ld;
@@ -162,7 +170,7 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
   cp_async_commit();
   cp_async_wait<1>();
   __syncthreads();
-  fft_stockham<R, -1, EPT>(buf, pl);
+  col_fft<R, -1, EPT, FIX>(buf, pl);
   cp_async_wait<0>();
   __syncthreads();
   for (int ky = tid; ky < n; ky += T) {
@@ -177,27 +185,30 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
     sm[2 * n + ky] = mk<R>(d * mz.x, d * mz.y);
   }
   __syncthreads();
-  fft_stockham<R, +1, EPT>(buf, pl);
+  col_fft<R, +1, EPT, FIX>(buf, pl);
   for (int yy = threadIdx.x; yy < nrows; yy += blockDim.x) col[yy] = buf[yy];
 }
 
 // forward column transform only (tensor spectra at init, FP64)
-template <int EPT>
+template <int EPT, int FIX>
 __global__ void k_cols_fwd(FftPlan pl, double2* __restrict__ S, int ld, int nrows, int Hx) {
   pdl_entry();
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* sm = reinterpret_cast<double2*>(smraw);
   const int kx = blockIdx.x;
-  const int n = pl.n;
+  const int n = FIX > 0 ? FIX : pl.n;
   double2* col = S + (long long)kx * ld;
   for (int yy = threadIdx.x; yy < n; yy += blockDim.x) sm[yy] = (yy < nrows) ? col[yy] : make_double2(0.0, 0.0);
   __syncthreads();
-  fft_stockham<double, -1, EPT>(sm, pl);
+  col_fft<double, -1, EPT, FIX>(sm, pl);
   for (int yy = threadIdx.x; yy < n; yy += blockDim.x) col[yy] = sm[yy];
 }
 
 // ── K3: inverse real transform along x, scatter to SoA h (FP64) ──────────
-template <typename R, int NB, int EPT>
+// FIX > 0: the compile-time plan of that length, whose last pass writes the
+// kept outputs i < ng to HBM directly (an open-boundary row, ng <= n/2,
+// forms only the lower half of every butterfly); FIX = 0: the runtime plan.
+template <typename R, int NB, int EPT, int FIX>
 __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
                            double* __restrict__ h, long long comp_stride, int ng) {
   pdl_entry();
@@ -206,7 +217,7 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
   C* sm = reinterpret_cast<C*>(smraw);
   const int c = blockIdx.y;
   const int y0 = blockIdx.x * (2 * NB);
-  const int n = pl.n;
+  const int n = FIX > 0 ? FIX : pl.n;
   const int b = threadIdx.y;
   const bool even = (n % 2) == 0;
   const int np = padded_len<R>(n);
@@ -244,43 +255,35 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
   __syncthreads();
   C* buf = sm + b * np;
   double* dst = h + (long long)c * comp_stride;
-  // The last pass writes the kept outputs i < ng of rows ya (real part) and
-  // yb (imaginary part) to HBM directly; an open-boundary row (ng <= n/2)
-  // forms only the lower half of every butterfly.
-  const int ya = y0 + 2 * b, yb = ya + 1;
-  auto st = [&](int i, C z) {
-    if (i < ng) {
-      if (ya < nrows) dst[(long long)ya * ng + i] = (double)z.x;
-      if (yb < nrows) dst[(long long)yb * ng + i] = (double)z.y;
+  if constexpr (FIX > 0) {
+    // rows ya (real part) and yb (imaginary part), kept outputs i < ng
+    const int ya = y0 + 2 * b, yb = ya + 1;
+    auto st = [&](int i, C z) {
+      if (i < ng) {
+        if (ya < nrows) dst[(long long)ya * ng + i] = (double)z.x;
+        if (yb < nrows) dst[(long long)yb * ng + i] = (double)z.y;
+      }
+    };
+    constexpr RadixList L = fixed_radices(FIX);
+    constexpr int RL = L.r[L.nr - 1];
+    fft_fixed<R, +1, EPT, true, FIX, 0, L.nr - 1, 1>(buf, pl);
+    if constexpr (RL % 2 == 0) {
+      if (2 * ng <= FIX) stockham_last_pass_st<R, RL, +1, EPT, true, true>(buf, pl, FIX, st);
+      else stockham_last_pass_st<R, RL, +1, EPT, true, false>(buf, pl, FIX, st);
+    } else {
+      stockham_last_pass_st<R, RL, +1, EPT, true, false>(buf, pl, FIX, st);
     }
-  };
-  const int nr = pl.nr;
-  const int4 pz = __ldg(&pl.pass[nr - 1]);
-  const bool half = 2 * ng <= n;
-#define LAST_PASS(RAD)                                                        \
-  do {                                                                        \
-    fft_stockham<R, +1, EPT, true>(buf, pl, 0, nr - 1);                        \
-    if (half) stockham_last_pass_st<R, RAD, +1, EPT, true, true>(buf, pl, pz, st); \
-    else stockham_last_pass_st<R, RAD, +1, EPT, true, false>(buf, pl, pz, st);     \
-  } while (0)
-  switch (pz.x) {
-    case 16: LAST_PASS(16); return;
-    case 12: LAST_PASS(12); return;
-    case 8: LAST_PASS(8); return;
-    case 6: LAST_PASS(6); return;
-    case 4: LAST_PASS(4); return;
-    default: break;
-  }
-#undef LAST_PASS
-  fft_stockham<R, +1, EPT, true>(buf, pl);
-  const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+  } else {
+    fft_stockham<R, +1, EPT, true>(buf, pl);
+    const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
 #pragma unroll
-  for (int r = 0; r < NB * 2; r++) {
-    const int y = y0 + r;
-    if (y >= nrows) break;
-    for (int i = tid; i < ng; i += T) {
-      const C z = sm[(r >> 1) * np + fpad<R, true>(i)];
-      dst[(long long)y * ng + i] = (double)((r & 1) ? z.y : z.x);
+    for (int r = 0; r < NB * 2; r++) {
+      const int y = y0 + r;
+      if (y >= nrows) break;
+      for (int i = tid; i < ng; i += T) {
+        const C z = sm[(r >> 1) * np + fpad<R, true>(i)];
+        dst[(long long)y * ng + i] = (double)((r & 1) ? z.y : z.x);
+      }
     }
   }
 }
@@ -440,6 +443,7 @@ static bool fixed_radix(int r) {
 
 struct HostFft {
   int n = 0, tx = 32, ept = 8;
+  int fix = 0;   // n when the compile-time plan runs (fixed_length), else 0
   std::vector<int> radix;
   double2* d_tw = nullptr;
   float2* d_twf = nullptr;   // FP32 twiddles (mixed chain)
@@ -448,8 +452,9 @@ struct HostFft {
   // fixed radices; a generic radix R needs one thread per butterfly (n/R)
   int tx_for(int e) const {
     int need = (n + e - 1) / e;
-    for (int r : radix)
-      if (!fixed_radix(r)) need = std::max(need, n / r);
+    if (!fix)
+      for (int r : radix)
+        if (!fixed_radix(r)) need = std::max(need, n / r);
     return ((std::max(need, 32) + 31) / 32) * 32;
   }
   template <typename R>
@@ -498,41 +503,25 @@ struct DemagPlan {
   const void* gkey[3] = {nullptr, nullptr, nullptr};
 };
 
+// the runtime pass table of length n (runtime_radices), or -1
 static int factorize(int n, std::vector<int>& rad) {
   rad.clear();
-  int m = n;
-  // the order fft_stockham runs the passes in: 16s, the rest of the power
-  // of two as one 8, 4 or 2 — or, with a factor 3, one 12 or 6 — then 3s,
-  // 5s and other primes (3072 = 16.16.12: three shared-memory passes)
-  while (m % 16 == 0) { rad.push_back(16); m /= 16; }
-  int p2 = 1;
-  while (m % 2 == 0) { p2 *= 2; m /= 2; }
-  if ((p2 == 2 || p2 == 4) && m % 3 == 0) {
-    rad.push_back(3 * p2);
-    m /= 3;
-  } else if (p2 > 1) {
-    rad.push_back(p2);
-  }
-  while (m % 3 == 0) { rad.push_back(3); m /= 3; }
-  while (m % 5 == 0) { rad.push_back(5); m /= 5; }
-  for (int p = 7; m > 1; p += 2) {
-    while (m % p == 0) {
-      if (p > 64) return -1;
-      rad.push_back(p);
-      m /= p;
-    }
-    if (p * p > m && m > 1) {
-      if (m > 64) return -1;
-      rad.push_back(m);
-      m = 1;
-    }
-  }
-  if ((int)rad.size() > MAXR) return -1;
+  const RadixList L = runtime_radices(n);
+  if (L.nr < 0) return -1;
+  for (int i = 0; i < L.nr; i++) rad.push_back(L.r[i]);
+  return 0;
+}
+
+// n if length n has a compile-time plan (kFixedLengths), else 0
+static int fixed_length(int n) {
+  for (int f : kFixedLengths)
+    if (f == n && fixed_radices(n).nr > 0) return n;
   return 0;
 }
 
 static int fft_init(HostFft& f, int n, int batch) {
   f.n = n;
+  f.fix = fixed_length(n);
   if (factorize(n, f.radix) != 0) {
     llg_set_error("FFT length " + std::to_string(n) + " has a prime factor > 64");
     return LLG_ERR_NOTSUP;
@@ -606,16 +595,84 @@ static int set_smem(const void* fn, size_t bytes) {
 template <typename R>
 static constexpr int kp() { return sizeof(R) == 8 ? 0 : 1; }
 
+// Kernel of each launch shape: nb packed transforms per CTA, ept elements
+// per thread, and the compile-time plan of the transform length when it has
+// one (HostFft::fix).
+template <typename R>
+using RowsFwdFn = void (*)(FftPlanT<R>, const double*, long long, int, int, const double*, cx_t<R>*, int, int);
+template <typename R>
+using RowsInvFn = void (*)(FftPlanT<R>, const cx_t<R>*, int, int, int, double*, long long, int);
+template <typename R>
+using ColsFn = void (*)(FftPlanT<R>, cx_t<R>*, int, int, int, const R*, const R*, const R*, const cx_t<R>*);
+using ColsFwdFn = void (*)(FftPlan, double2*, int, int, int);
+
+#define LLG_FIX_SWITCH(fix, EXPR_OF)                                          \
+  switch (fix) {                                                              \
+    case 1024: return EXPR_OF(1024);                                          \
+    case 2048: return EXPR_OF(2048);                                          \
+    case 3072: return EXPR_OF(3072);                                          \
+    case 4096: return EXPR_OF(4096);                                          \
+    default: return EXPR_OF(0);                                               \
+  }
+template <typename R, int NB, int EPT>
+static RowsFwdFn<R> rows_fwd_fn_t(int fix) {
+#define K_OF(F) k_rows_fwd<R, NB, EPT, F>
+  LLG_FIX_SWITCH(fix, K_OF)
+#undef K_OF
+}
+template <typename R, int NB, int EPT>
+static RowsInvFn<R> rows_inv_fn_t(int fix) {
+#define K_OF(F) k_rows_inv<R, NB, EPT, F>
+  LLG_FIX_SWITCH(fix, K_OF)
+#undef K_OF
+}
+template <typename R, int EPT, bool ST>
+static ColsFn<R> cols_fn_t(int fix) {
+#define K_OF(F) k_cols_conv<R, EPT, ST, F>
+  LLG_FIX_SWITCH(fix, K_OF)
+#undef K_OF
+}
+template <int EPT>
+static ColsFwdFn cols_fwd_fn_t(int fix) {
+#define K_OF(F) k_cols_fwd<EPT, F>
+  LLG_FIX_SWITCH(fix, K_OF)
+#undef K_OF
+}
+#undef LLG_FIX_SWITCH
+template <typename R>
+static RowsFwdFn<R> rows_fwd_fn(int fix, int nb, int ept) {
+  if (nb == 1) return ept == 8 ? rows_fwd_fn_t<R, 1, 8>(fix) : rows_fwd_fn_t<R, 1, 16>(fix);
+  return ept == 8 ? rows_fwd_fn_t<R, 2, 8>(fix) : rows_fwd_fn_t<R, 2, 16>(fix);
+}
+template <typename R>
+static RowsInvFn<R> rows_inv_fn(int fix, int nb, int ept) {
+  if (nb == 1) return ept == 8 ? rows_inv_fn_t<R, 1, 8>(fix) : rows_inv_fn_t<R, 1, 16>(fix);
+  return ept == 8 ? rows_inv_fn_t<R, 2, 8>(fix) : rows_inv_fn_t<R, 2, 16>(fix);
+}
+template <typename R>
+static ColsFn<R> cols_fn(int fix, int ept, bool stage) {
+  if (ept == 8) return stage ? cols_fn_t<R, 8, true>(fix) : cols_fn_t<R, 8, false>(fix);
+  return stage ? cols_fn_t<R, 16, true>(fix) : cols_fn_t<R, 16, false>(fix);
+}
+static ColsFwdFn cols_fwd_fn(int fix, int ept) { return ept == 8 ? cols_fwd_fn_t<8>(fix) : cols_fwd_fn_t<16>(fix); }
+
+// threads per block a kernel can be launched with (its register use)
+static int max_threads(const void* fn) {
+  cudaFuncAttributes at{};
+  if (cudaFuncGetAttributes(&at, fn) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return at.maxThreadsPerBlock;
+}
+
 template <typename R>
 static int launch_rows_fwd(const DemagPlan* d, cudaStream_t s, const double* in, long long cs, int row_len,
                            int nrows, const double* w, cx_t<R>* S, int ld, int ncomp, const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fx.dev<R>();
   const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((nrows + 2 * k.nb - 1) / (2 * k.nb), ncomp), b(d->fx.tx_for(k.ept), k.nb);
-#define ROWS_FWD(NB, E) klaunch(k_rows_fwd<R, NB, E>, g, b, sm, s, pl, in, cs, row_len, nrows, w, S, ld, d->hx)
-  if (k.nb == 1) { if (k.ept == 8) ROWS_FWD(1, 8); else ROWS_FWD(1, 16); }
-  else { if (k.ept == 8) ROWS_FWD(2, 8); else ROWS_FWD(2, 16); }
-#undef ROWS_FWD
+  klaunch(rows_fwd_fn<R>(d->fx.fix, k.nb, k.ept), g, b, sm, s, pl, in, cs, row_len, nrows, w, S, ld, d->hx);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -626,10 +683,7 @@ static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, const cx_t<R>* S,
   const FftPlanT<R> pl = d->fx.dev<R>();
   const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((d->ny + 2 * k.nb - 1) / (2 * k.nb), 3), b(d->fx.tx_for(k.ept), k.nb);
-#define ROWS_INV(NB, E) klaunch(k_rows_inv<R, NB, E>, g, b, sm, s, pl, S, d->ny, d->ny, d->hx, h, cs, d->ng)
-  if (k.nb == 1) { if (k.ept == 8) ROWS_INV(1, 8); else ROWS_INV(1, 16); }
-  else { if (k.ept == 8) ROWS_INV(2, 8); else ROWS_INV(2, 16); }
-#undef ROWS_INV
+  klaunch(rows_inv_fn<R>(d->fx.fix, k.nb, k.ept), g, b, sm, s, pl, S, d->ny, d->ny, d->hx, h, cs, d->ng);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -641,13 +695,7 @@ static int launch_cols_conv(const DemagPlan* d, cudaStream_t s, cx_t<R>* S, cons
   const dim3 b(d->fy.tx_for(k.ept), 3);
   const size_t base = sizeof(cx_t<R>) * 3 * (size_t)d->py;
   const size_t sm = k.stage ? base + (sizeof(R) * 3 + sizeof(cx_t<R>)) * (size_t)d->py : base;
-#define COLS_LAUNCH(E, ST) klaunch(k_cols_conv<R, E, ST>, d->hx, b, sm, s, pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy)
-  if (k.ept == 8) {
-    if (k.stage) COLS_LAUNCH(8, true); else COLS_LAUNCH(8, false);
-  } else {
-    if (k.stage) COLS_LAUNCH(16, true); else COLS_LAUNCH(16, false);
-  }
-#undef COLS_LAUNCH
+  klaunch(cols_fn<R>(d->fy.fix, k.ept, k.stage), d->hx, b, sm, s, pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -655,17 +703,18 @@ static int launch_cols_conv(const DemagPlan* d, cudaStream_t s, cx_t<R>* S, cons
 static int launch_cols_fwd(const DemagPlan* d, cudaStream_t s, double2* S) {
   const FftPlan pl = d->fy.dev<double>();
   const size_t sm = sizeof(double2) * (size_t)d->py;
-  if (d->fy.ept == 8)
-    klaunch(k_cols_fwd<8>, d->hx, dim3(d->fy.tx, 1), sm, s, pl, S, d->py, d->py, d->hx);
-  else
-    klaunch(k_cols_fwd<16>, d->hx, dim3(d->fy.tx, 1), sm, s, pl, S, d->py, d->py, d->hx);
+  klaunch(cols_fwd_fn(d->fy.fix, d->fy.ept), d->hx, dim3(d->fy.tx_for(d->fy.ept), 1), sm, s, pl, S, d->py, d->py,
+          d->hx);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
 
 template <typename R>
 static bool rows_ok(const DemagPlan* d, int nb, int ept) {
-  return d->fx.tx_for(ept) * nb <= 1024 && sizeof(cx_t<R>) * (size_t)nb * padded_len<R>(d->px) <= 227 * 1024;
+  const int threads = d->fx.tx_for(ept) * nb;
+  return threads <= 1024 && sizeof(cx_t<R>) * (size_t)nb * padded_len<R>(d->px) <= 227 * 1024 &&
+         threads <= max_threads((const void*)rows_fwd_fn<R>(d->fx.fix, nb, ept)) &&
+         threads <= max_threads((const void*)rows_inv_fn<R>(d->fx.fix, nb, ept));
 }
 template <typename R>
 static size_t cols_smem(const DemagPlan* d, bool stage) {
@@ -674,7 +723,8 @@ static size_t cols_smem(const DemagPlan* d, bool stage) {
 }
 template <typename R>
 static bool cols_ok(const DemagPlan* d, int ept, bool stage) {
-  if (d->fy.tx_for(ept) * 3 > 1024) return false;
+  const int threads = d->fy.tx_for(ept) * 3;
+  if (threads > 1024 || threads > max_threads((const void*)cols_fn<R>(d->fy.fix, ept, stage))) return false;
   if (!stage) return cols_smem<R>(d, false) <= 227 * 1024;
   return d->py % (int)(16 / sizeof(R)) == 0 && cols_smem<R>(d, true) <= 200 * 1024;
 }
@@ -684,21 +734,21 @@ template <typename R>
 static int set_smem_all(DemagPlan* d) {
   int rc;
   const size_t r1 = sizeof(cx_t<R>) * (size_t)padded_len<R>(d->px), r2 = 2 * r1;
-  if ((rc = set_smem((const void*)k_rows_fwd<R, 1, 8>, r1)) || (rc = set_smem((const void*)k_rows_fwd<R, 1, 16>, r1)) ||
-      (rc = set_smem((const void*)k_rows_inv<R, 1, 8>, r1)) || (rc = set_smem((const void*)k_rows_inv<R, 1, 16>, r1)))
-    return rc;
-  if (r2 <= 227 * 1024 &&
-      ((rc = set_smem((const void*)k_rows_fwd<R, 2, 8>, r2)) || (rc = set_smem((const void*)k_rows_fwd<R, 2, 16>, r2)) ||
-       (rc = set_smem((const void*)k_rows_inv<R, 2, 8>, r2)) || (rc = set_smem((const void*)k_rows_inv<R, 2, 16>, r2))))
-    return rc;
+  for (int nb = 1; nb <= 2; nb++)
+    for (int ept = 8; ept <= 16; ept *= 2) {
+      const size_t r = nb == 1 ? r1 : r2;
+      if (r > 227 * 1024) continue;
+      if ((rc = set_smem((const void*)rows_fwd_fn<R>(d->fx.fix, nb, ept), r)) ||
+          (rc = set_smem((const void*)rows_inv_fn<R>(d->fx.fix, nb, ept), r)))
+        return rc;
+    }
   const size_t c0 = cols_smem<R>(d, false), c1 = cols_smem<R>(d, true);
-  if ((rc = set_smem((const void*)k_cols_conv<R, 8, false>, c0)) ||
-      (rc = set_smem((const void*)k_cols_conv<R, 16, false>, c0)))
-    return rc;
-  if (c1 <= 200 * 1024 && ((rc = set_smem((const void*)k_cols_conv<R, 8, true>, c1)) ||
-                           (rc = set_smem((const void*)k_cols_conv<R, 16, true>, c1))))
-    return rc;
-  // default shapes (before tuning): one transform per CTA, fewest elements per thread
+  for (int ept = 8; ept <= 16; ept *= 2) {
+    if ((rc = set_smem((const void*)cols_fn<R>(d->fy.fix, ept, false), c0))) return rc;
+    if (c1 <= 200 * 1024 && (rc = set_smem((const void*)cols_fn<R>(d->fy.fix, ept, true), c1))) return rc;
+  }
+  // default shapes (before tuning): one transform per CTA, fewest elements
+  // per thread that the kernel's registers allow
   LaunchCfg& rw = d->rows[kp<R>()];
   LaunchCfg& cl = d->cols[kp<R>()];
   rw.nb = 1;
@@ -825,8 +875,8 @@ int demag_create(llg_ctx* c) {
     return LLG_ERR_NOTSUP;
   }
   if ((rc = set_smem_all<double>(d)) || (d->mixed && (rc = set_smem_all<float>(d))) ||
-      (rc = set_smem((const void*)k_cols_fwd<8>, sizeof(double2) * (size_t)d->py)) ||
-      (rc = set_smem((const void*)k_cols_fwd<16>, sizeof(double2) * (size_t)d->py))) {
+      (rc = set_smem((const void*)cols_fwd_fn(d->fy.fix, 8), sizeof(double2) * (size_t)d->py)) ||
+      (rc = set_smem((const void*)cols_fwd_fn(d->fy.fix, 16), sizeof(double2) * (size_t)d->py))) {
     demag_destroy(d);
     return rc;
   }
@@ -855,9 +905,7 @@ int demag_create(llg_ctx* c) {
   double2* spec = nullptr;
   LLG_CUDA_TRY(cudaMalloc(&spec, sizeof(double2) * 9 * (size_t)nspec));
   for (int k = 0; k < 9; k++) {
-    LaunchCfg k1;
-    k1.nb = kRowsNB;
-    k1.ept = d->fx.ept;
+    LaunchCfg k1 = d->rows[kp<double>()];   // the default FP64 shape (one transform per CTA)
     if ((rc = launch_rows_fwd<double>(d, s, d->d_T + k * np, 0, d->px, d->py, nullptr, spec + k * nspec, d->py, 1,
                                       k1)) ||
         (rc = launch_cols_fwd(d, s, spec + k * nspec))) {

@@ -193,18 +193,20 @@ def test_device_resident_control_bound_returns_timeout(gpu):
 
 def test_replayed_mixed_form_within_1e4_of_fp64(gpu):
     """The mixed-precision form's own error on a hole + open-demag film
-    (256x128, strength 4, t 0 -> 5 at rtol 1e-4): both forms take plain
-    FP64's recorded steps, so max|dm| measures the reduced-precision demag
-    alone.  alpha = 0.2: the relaxation is stable, and the form stays
-    within 1e-4 of FP64 at every output.  (On the benchmark film, alpha =
-    0.02, the dynamics amplify any perturbation exponentially — a plain FP64
-    run with the demag strength changed by 1e-9 moves by 1e-2 within 20 time
-    units — and bench.py reports both distances side by side.)"""
+    (256x128, strength 1, alpha 0.2, t 0 -> 10 at rtol 1e-4): both forms take
+    plain FP64's recorded steps, so max|dm| measures the reduced-precision
+    demag alone, and an FP64 control with the demag strength changed by 1e-9
+    (same steps) measures how much the film amplifies a perturbation.  This
+    film relaxes without forming domains: the control stays below 1e-7 and
+    the form within 1e-4 of FP64 at every output.  (At strength 4 the film
+    breaks into domains near t = 4 and the 1e-9 control itself jumps to
+    1e-4 there, as does the form: there the distance is the film's, not the
+    form's.)"""
     import torch
-    t_out = [1.0, 2.0, 3.0, 4.0, 5.0]
+    t_out = [float(t) for t in range(1, 11)]
 
-    def run(prec, replay=None):
-        p, geo = _hole(256, 128, prec=prec, alpha=0.2)
+    def run(prec, replay=None, strength=1.0):
+        p, geo = _hole(256, 128, prec=prec, alpha=0.2, strength=strength)
         ctx = _ctx(p, geo)
         y0 = torch.from_numpy(geo["y0"]).cuda()
         ctx.integrator_init(0.0, y0, llg.default_solver_opts())
@@ -214,7 +216,7 @@ def test_replayed_mixed_form_within_1e4_of_fp64(gpu):
             ctx.replay_steps(*replay)
         yout = torch.zeros_like(y0)
         outs = []
-        for k in range(1, 51):
+        for k in range(1, 101):
             ctx.integrate(0.1 * k, yout)
             if k % 10 == 0:
                 torch.cuda.synchronize()
@@ -223,11 +225,14 @@ def test_replayed_mixed_form_within_1e4_of_fp64(gpu):
 
     a, steps = run(llg.DEMAG_FP64)
     b, st = run(llg.DEMAG_MIXED, replay=steps)
+    c, _ = run(llg.DEMAG_FP64, replay=steps, strength=1.0 * (1.0 + 1e-9))
     assert st["position"] == len(steps[0])
-    for t, x, y in zip(t_out, a, b):
-        dm = float(np.abs(x - y).max())
-        print(f"replayed mixed vs FP64, t={t}: max|dm| = {dm:.3e}")
-        assert dm <= 1e-4
+    dms = [float(np.abs(x - y).max()) for x, y in zip(a, b)]
+    dcs = [float(np.abs(x - y).max()) for x, y in zip(a, c)]
+    for t, dm, dc in zip(t_out, dms, dcs):
+        print(f"t={t}: replayed mixed vs FP64 max|dm| = {dm:.3e}, FP64 control {dc:.3e}")
+    assert max(dcs) <= 1e-7
+    assert max(dms) <= 1e-4
 
 
 def test_fp32_krylov_basis_tracks_fp64_basis(gpu):
