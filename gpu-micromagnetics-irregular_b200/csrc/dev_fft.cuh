@@ -267,14 +267,15 @@ __device__ __forceinline__ void apply_twiddles(cx_t<R>* v, const FftPlanT<R>& pl
 // with at most MB each (tx >= n/EPT is guaranteed by the plan).  n, Ns and
 // lg are arguments so that a compile-time plan (fft_fixed) folds them.
 template <typename R, int RAD, int SIGN, int EPT, bool PAD>
-__device__ __forceinline__ void stockham_pass_n(cx_t<R>* buf, const FftPlanT<R>& pl, int n, int Ns, int lg) {
+__device__ __forceinline__ void stockham_pass_n(cx_t<R>* buf, const FftPlanT<R>& pl, int n, int Ns, int lg,
+                                                int tx = threadIdx.x) {
   constexpr int MB = (EPT + RAD - 1) / RAD;
   const int nb = n / RAD;
   const int tstride = n / (Ns * RAD);
   cx_t<R> v[MB][RAD];
 #pragma unroll
   for (int u = 0; u < MB; u++) {
-    const int j = threadIdx.x + u * blockDim.x;
+    const int j = tx + u * blockDim.x;
     if (j < nb) {
 #pragma unroll
       for (int r = 0; r < RAD; r++) v[u][r] = buf[fpad<R, PAD>(j + r * nb)];
@@ -283,7 +284,7 @@ __device__ __forceinline__ void stockham_pass_n(cx_t<R>* buf, const FftPlanT<R>&
   __syncthreads();
 #pragma unroll
   for (int u = 0; u < MB; u++) {
-    const int j = threadIdx.x + u * blockDim.x;
+    const int j = tx + u * blockDim.x;
     if (j < nb) {
       int q, jm;
       if (lg >= 0) { q = j >> lg; jm = j & (Ns - 1); }
@@ -308,13 +309,13 @@ __device__ __forceinline__ void stockham_pass(cx_t<R>* buf, const FftPlanT<R>& p
 // known to be zero (an open-boundary row, zero-padded to twice its length)
 // and the butterflies' upper halves are not loaded or computed.
 template <typename R, int RAD, int SIGN, int EPT, bool PAD, bool HALF, typename LD>
-__device__ __forceinline__ void stockham_first_pass_ld(cx_t<R>* buf, int n, LD&& ld) {
+__device__ __forceinline__ void stockham_first_pass_ld(cx_t<R>* buf, int n, LD&& ld, int tx = threadIdx.x) {
   constexpr int MB = (EPT + RAD - 1) / RAD;
   static_assert(!HALF || RAD % 2 == 0, "HALF needs an even radix");
   const int nb = n / RAD;
 #pragma unroll
   for (int u = 0; u < MB; u++) {
-    const int j = threadIdx.x + u * blockDim.x;
+    const int j = tx + u * blockDim.x;
     if (j < nb) {
       cx_t<R> v[RAD];
 #pragma unroll
@@ -333,13 +334,14 @@ __device__ __forceinline__ void stockham_first_pass_ld(cx_t<R>* buf, int n, LD&&
 // the upper half of every butterfly is not stored.  buf is only read: no
 // barrier follows.
 template <typename R, int RAD, int SIGN, int EPT, bool PAD, bool HALF, typename ST>
-__device__ __forceinline__ void stockham_last_pass_st(const cx_t<R>* buf, const FftPlanT<R>& pl, int n, ST&& st) {
+__device__ __forceinline__ void stockham_last_pass_st(const cx_t<R>* buf, const FftPlanT<R>& pl, int n, ST&& st,
+                                                      int tx = threadIdx.x) {
   constexpr int MB = (EPT + RAD - 1) / RAD;
   static_assert(!HALF || RAD % 2 == 0, "HALF needs an even radix");
   const int nb = n / RAD;   // = the span of the last pass
 #pragma unroll
   for (int u = 0; u < MB; u++) {
-    const int j = threadIdx.x + u * blockDim.x;
+    const int j = tx + u * blockDim.x;
     if (j < nb) {
       cx_t<R> v[RAD];
 #pragma unroll
@@ -462,13 +464,23 @@ __device__ void fft_stockham(cx_t<R>* buf, const FftPlanT<R>& pl) {
 // at pass P, every size, span and shift folded into the code.  pl supplies
 // the twiddle table only.
 template <typename R, int SIGN, int EPT, bool PAD, int N, int P, int PE, int NS>
-__device__ __forceinline__ void fft_fixed(cx_t<R>* buf, const FftPlanT<R>& pl) {
+__device__ __forceinline__ void fft_fixed(cx_t<R>* buf, const FftPlanT<R>& pl, int tx = threadIdx.x) {
   if constexpr (P < PE) {
     constexpr RadixList L = fixed_radices(N);
     constexpr int RAD = L.r[P];
-    stockham_pass_n<R, RAD, SIGN, EPT, PAD>(buf, pl, N, NS, ilog2_or_neg(NS));
-    fft_fixed<R, SIGN, EPT, PAD, N, P + 1, PE, NS * RAD>(buf, pl);
+    stockham_pass_n<R, RAD, SIGN, EPT, PAD>(buf, pl, N, NS, ilog2_or_neg(NS), tx);
+    fft_fixed<R, SIGN, EPT, PAD, N, P + 1, PE, NS * RAD>(buf, pl, tx);
   }
+}
+
+// The thread index as a value the compiler cannot see through: a persistent
+// kernel reads it once per item, so the address arithmetic of its unrolled
+// passes is redone per item instead of being hoisted out of the item loop
+// and held in registers for the kernel's lifetime.
+__device__ __forceinline__ int opaque_tid() {
+  int t;
+  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
+  return t;
 }
 
 // the lengths with a compile-time plan (their kernels are instantiated per
