@@ -113,23 +113,36 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
   constexpr int BB = bbytes_for(D1);
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* Ab = sm + BB;
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar[2];    // per team: the MMA completion of its stage
   __shared__ uint32_t tmem_slot;
-  __shared__ int s_fail;
+  __shared__ int s_fail[2];
   __shared__ int s_e[3][NCOL];    // per (component, column) input exponent
   __shared__ int s_eo[3][NCOL];   // exponent carried by the tensor product
   __shared__ float2 s_tw[32][32]; // w1024^(k l) at [k][l]: lane l reads [k][l], no bank conflicts
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int c = warp >> 2, q = warp & 3;
+  // Two teams run the stage sequence independently: warps 0-7 the coupled x
+  // and y components, warps 8-11 the z component.  Each has its own named
+  // barrier, MMA-issuing thread and completion mbarrier, so one team's
+  // epilogue (CUDA cores, TMEM read-back) overlaps the other's MMAs and
+  // neither waits at the other's barriers.
+  const int team = (c < 2) ? 0 : 1;
+  const int team_lead = team ? 256 : 0, team_threads = team ? 128 : 256;
+  const int c_lo = team ? 2 : 0, c_hi = team ? 3 : 2;
+  auto team_sync = [&]() {
+    asm volatile("bar.sync %0, %1;\n" ::"r"(1 + team), "r"(team_threads) : "memory");
+  };
 
   for (int i = tid; i < BB / 16; i += NT) reinterpret_cast<uint4*>(sm)[i] = a.bmat[i];
   for (int i = tid; i < 32 * 32; i += NT) s_tw[i >> 5][i & 31] = a.tw[((i >> 5) * (i & 31)) & (P - 1)];
   if (warp == 0) tmem_alloc(&tmem_slot, TMEM_COLS);
   if (tid == 0) {
-    mbar_init(&mbar, 1);
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
     mbar_init_fence();
-    s_fail = 0;
+    s_fail[0] = 0;
+    s_fail[1] = 0;
   }
   fence_proxy_async_smem();
   tc_fence_before();
@@ -142,14 +155,15 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
   unsigned char* Al = Ah + AMAT;
   uint32_t phase = 0;
 
-  // barrier + one thread issues the stage's MMAs + everyone waits for them
+  // team barrier + the team's lead thread issues the stage's MMAs for the
+  // team's components + the team waits for them
   auto run_stage = [&](int st) -> bool {
     fence_proxy_async_smem();
     tc_fence_before();
-    __syncthreads();
-    if (tid == 0) {
+    team_sync();
+    if (tid == team_lead) {
       tc_fence_after();
-      for (int cc = 0; cc < 3; cc++) {
+      for (int cc = c_lo; cc < c_hi; cc++) {
         const uint32_t aH = sA + cc * ACOMP, aL = aH + AMAT;
         if (st == 0)
           issue3(tbase + 128 * cc, aH, aL, sB + oF1h, sB + oF1l, K1 / 16, 2 * LBO_K, LBO_K, K1 * 16, K1 * 16,
@@ -164,12 +178,12 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
           issue3(tbase + 128 * cc, aH, aL, sB + oG1h, sB + oG1l, 4, 2 * LBO_MN, LBO_MN, SBO_MN, 1024,
                  idesc_f16_f32(128, 2 * D1, 1, 0));
       }
-      tc_commit(&mbar);
+      tc_commit(&mbar[team]);
     }
-    const bool ok = mbar_wait(&mbar, phase, WAIT_LIMIT);
-    if (!ok) atomicExch(&s_fail, 1);
-    __syncthreads();
-    if (s_fail) return false;   // phase left pending for the bounded drain below
+    const bool ok = mbar_wait(&mbar[team], phase, WAIT_LIMIT);
+    if (!ok) atomicExch(&s_fail[team], 1);
+    team_sync();
+    if (s_fail[team]) return false;   // phase left pending for the bounded drain below
     phase ^= 1u;
     tc_fence_after();
     return true;
@@ -257,7 +271,8 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
     if (!(good = run_stage(1))) break;
     // ── F2 epilogue: tensor multiply, conj, 2^(e_t-6) -> G2 operand (K-major) ──
     {
-      const int ex = s_e[0][q], ey = s_e[1][q];
+      // (the z team reads only its own exponent: the x/y ones may already be the next group's)
+      const int ex = (c < 2) ? s_e[0][q] : 0, ey = (c < 2) ? s_e[1][q] : 0;
       const int em = (c == 2) ? s_e[2][q] : max(ex, ey);
       const float fx = ldexpf(1.f, ex - em), fy = ldexpf(1.f, ey - em);
       const long long tb = (long long)(colok ? kx : 0) * P + lane;
@@ -373,9 +388,9 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
     }
   }
   if (!good) {
-    if (tid == 0) atomicExch(a.err, 1);
-    // let MMAs still in flight finish (bounded) before tensor memory is freed
-    mbar_wait(&mbar, phase, WAIT_LIMIT);
+    if (tid == team_lead) atomicExch(a.err, 1);
+    // let the team's MMAs still in flight finish (bounded) before tensor memory is freed
+    mbar_wait(&mbar[team], phase, WAIT_LIMIT);
   }
   tc_fence_before();
   __syncthreads();
