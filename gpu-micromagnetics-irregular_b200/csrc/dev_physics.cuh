@@ -13,12 +13,23 @@ constexpr int TY = 8;
 
 // Logical slot -> grid cell.  Tile slots can lie up to a tile width past the
 // edge (grids narrower than a tile), so the periodic wrap is a full modulo.
+// Periodic wrap without integer division: the tile loaders ask for indices
+// one cell outside the grid (and, in a tile that overhangs a small grid,
+// further out, where only the remainder's range matters), so one add or
+// subtract covers the common case and the division is the rare fallback.
+__device__ __forceinline__ int wrap_idx(int i, int n) {
+  if (i < 0) i += n;
+  else if (i >= n) i -= n;
+  if ((unsigned)i >= (unsigned)n) {   // more than one period out
+    i %= n;
+    if (i < 0) i += n;
+  }
+  return i;
+}
 __device__ __forceinline__ bool map_nb(int& i, int& j, int ng, int ny, int bc) {
   if (bc == LLG_BC_FREE) return (i >= 0 && i < ng && j >= 0 && j < ny);
-  i %= ng;
-  if (i < 0) i += ng;
-  j %= ny;
-  if (j < 0) j += ny;
+  i = wrap_idx(i, ng);
+  j = wrap_idx(j, ny);
   return true;
 }
 

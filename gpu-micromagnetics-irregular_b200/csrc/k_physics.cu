@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const V
       tile_field(P, Y, sx, sy, m, msk, nsk, h);
       if (P.jv_full) {
 #pragma unroll
-        for (int a = 0; a < 3; a++) h[a] = h[a] + C[a * AP_CELLS + tid] + happ_at(P, a, P.src_on ? cell % P.ng : -1);
+        for (int a = 0; a < 3; a++) h[a] = h[a] + C[a * AP_CELLS + tid] + happ_at(P, a, P.src_on ? gi : -1);
       }
       double K[3][3];
       aniso_jac(P, m, msk, K);
