@@ -60,20 +60,6 @@ constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t WAIT_LIMIT = 1u << 22;
 
 __host__ __device__ constexpr int bbytes_for(int D1) { return 1024 * D1 + 16384; }
-// Tensor columns of a group staged in shared memory (D1 = 16 only; with
-// D1 = 32 the B operands leave no room): the x/y team's txx, tyy, txy and
-// the z team's tzz for the group's NCOL columns, filled by cp.async at the
-// group's start so the tensor multiply reads shared memory.
-constexpr int TST_XY = NCOL * P * (4 + 4 + 8), TST_Z = NCOL * P * 4;
-__host__ __device__ constexpr bool tstage_for(int D1) { return D1 == 16; }
-__host__ __device__ constexpr int tc_smem_for(int D1) {
-  return bbytes_for(D1) + 3 * ACOMP + (tstage_for(D1) ? TST_XY + TST_Z : 0);
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
 
 struct TcArgs {
   float2* S;
@@ -222,37 +208,9 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
     }
   };
   prefetch_group(blockIdx.x, false);
-  constexpr bool TSTAGE = tstage_for(D1);
-  // the team's staged tensor columns: [column q][frequency] per entry kind
-  float* tst = reinterpret_cast<float*>(Ab + 3 * ACOMP);
-  float* st_xx = tst;
-  float* st_yy = st_xx + NCOL * P;
-  float2* st_xy = reinterpret_cast<float2*>(st_yy + NCOL * P);
-  float* st_zz = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(tst) + TST_XY);
-  auto stage_tensor = [&](int gg) {
-    const int ttid = tid - team_lead;
-    for (int qq = 0; qq < NCOL; qq++) {
-      const int k2 = gg * NCOL + qq;
-      if (k2 >= a.hx) break;
-      const long long tb = (long long)k2 * P;
-      if (team == 0) {
-        for (int e = ttid; e < P / 4; e += team_threads) {
-          cp_async16(st_xx + qq * P + 4 * e, a.txx + tb + 4 * e);
-          cp_async16(st_yy + qq * P + 4 * e, a.tyy + tb + 4 * e);
-        }
-        for (int e = ttid; e < P / 2; e += team_threads) cp_async16(st_xy + qq * P + 2 * e, a.txy + tb + 2 * e);
-      } else {
-        for (int e = ttid; e < P / 4; e += team_threads) cp_async16(st_zz + qq * P + 4 * e, a.tzz + tb + 4 * e);
-      }
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  };
   bool good = true;
   for (int g = blockIdx.x; g < a.ngroups && good; g += gridDim.x) {
     prefetch_group(g + gridDim.x, true);
-    // (the previous group's tensor multiply read the staging area before the
-    // team's stage-2 barrier of that group)
-    if constexpr (TSTAGE) stage_tensor(g);
     const int kx = g * NCOL + q;
     const bool colok = kx < a.hx;
     // ── F1 operand: rows 32q + n2, K = (n1, re/im), this warp's own row ──
@@ -310,7 +268,6 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       *reinterpret_cast<uint4*>(Ah + oim) = hi.u;
       *reinterpret_cast<uint4*>(Al + oim) = li.u;
     }
-    if constexpr (TSTAGE) asm volatile("cp.async.wait_all;\n" ::: "memory");   // visible after the stage barrier
     if (!(good = run_stage(1))) break;
     // ── F2 epilogue: tensor multiply, conj, 2^(e_t-6) -> G2 operand (K-major) ──
     {
@@ -325,19 +282,12 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       // ahead so their latency overlaps the previous block's arithmetic
       float tn[8];
       float2 tq[8];
-      const float* sdiag = (c == 0) ? st_xx : ((c == 1) ? st_yy : st_zz);
       auto load_t = [&](int j, float(&n)[8], float2(&x)[8]) {
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-          if constexpr (TSTAGE) {
-            const int f = q * P + lane + 32 * (8 * j + i);
-            n[i] = colok ? sdiag[f] : 0.f;
-            x[i] = (colok && c < 2) ? st_xy[f] : make_float2(0.f, 0.f);
-          } else {
-            const long long e = tb + 32LL * (8 * j + i);
-            n[i] = colok ? __ldg(&tdiag[e]) : 0.f;
-            x[i] = (colok && c < 2) ? __ldg(&a.txy[e]) : make_float2(0.f, 0.f);
-          }
+          const long long e = tb + 32LL * (8 * j + i);
+          n[i] = colok ? __ldg(&tdiag[e]) : 0.f;
+          x[i] = (colok && c < 2) ? __ldg(&a.txy[e]) : make_float2(0.f, 0.f);
         }
       };
       load_t(0, tn, tq);
@@ -437,7 +387,6 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       }
     }
   }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy still in flight at exit
   if (!good) {
     if (tid == team_lead) atomicExch(a.err, 1);
     // let the team's MMAs still in flight finish (bounded) before tensor memory is freed
@@ -557,7 +506,7 @@ int demag_tc_create(llg_ctx* c, int px, int py, int hx, int ny, const float* txx
   t->grid = std::min(t->ngroups, c->num_sms);
   t->txx = txx; t->tyy = tyy; t->tzz = tzz; t->txy = txy;
   const int D1 = t->D1, K1 = 2 * D1, BB = bbytes_for(D1);
-  t->smem = (size_t)tc_smem_for(D1);
+  t->smem = (size_t)BB + 3 * (size_t)ACOMP;
   // B operands: F1 (64 x K1), F2 (64 x 64), G1 (2 D1 x 64), hi then lo each
   std::vector<unsigned char> b(BB, 0);
   const int oF1h = 0, oF1l = 128 * K1, oF2h = 256 * K1, oF2l = oF2h + 8192, oG1h = oF2h + 16384, oG1l = oG1h + 256 * D1;
