@@ -473,16 +473,6 @@ __device__ __forceinline__ void fft_fixed(cx_t<R>* buf, const FftPlanT<R>& pl, i
   }
 }
 
-// The thread index as a value the compiler cannot see through: a persistent
-// kernel reads it once per item, so the address arithmetic of its unrolled
-// passes is redone per item instead of being hoisted out of the item loop
-// and held in registers for the kernel's lifetime.
-__device__ __forceinline__ int opaque_tid() {
-  int t;
-  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
-  return t;
-}
-
 // the lengths with a compile-time plan (their kernels are instantiated per
 // length); every other length takes the runtime plan
 constexpr int kFixedLengths[] = {1024, 2048, 3072, 4096};

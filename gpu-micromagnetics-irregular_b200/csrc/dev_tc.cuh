@@ -141,20 +141,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint3
   return false;
 }
 
-// the arriving thread adds `bytes` to the phase's expected transaction count
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mbar)), "r"(bytes)
-               : "memory");
-}
-// bulk (non-tensor) copy global -> this CTA's shared memory, completing on
-// mbar; both addresses 16-byte aligned, bytes a multiple of 16; no multicast
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(mbar))
-               : "memory");
-}
-
 // FP32 -> FP16 hi + FP16 lo' with v ~ hi + 2^-11 lo' (to ~2^-22 relative).
 // The remainder is stored scaled up by 2^11 so it stays a normal FP16
 // number (an unscaled remainder of a value below ~0.1 would be subnormal).

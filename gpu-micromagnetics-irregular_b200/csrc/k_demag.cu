@@ -38,7 +38,6 @@
 #include <vector>
 
 #include "dev_fft.cuh"
-#include "dev_tc.cuh"
 #include "llg_internal.h"
 #include "launch.h"
 
@@ -289,218 +288,6 @@ __global__ void k_rows_inv(FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld
   }
 }
 
-// ── K1 / K3 persistent, double-buffered forms (compile-time plans) ───────
-// The same per-element arithmetic as k_rows_fwd / k_rows_inv with NB = 1.
-// Each CTA walks the (component, row pair) items blockIdx.x, blockIdx.x +
-// gridDim.x, ... and, while it transforms one item, the next item's input is
-// already on its way into the other staging buffer: two bulk asynchronous
-// copies per item (the FP64 rows, and the window rows when windowed) for the
-// forward transform, one 16- or 32-byte cp.async per spectrum column for the
-// inverse.  HBM latency then overlaps the previous item's shared-memory
-// passes instead of stalling every CTA at its start.  A wait that runs out
-// sets *err and the CTA stops after its copies have landed.
-constexpr uint32_t kRowsWaitLimit = 1u << 22;
-__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
-template <typename R>
-__host__ __device__ constexpr size_t fwd_pipe_smem(int n, int row_len, bool win) {
-  return align16(sizeof(cx_t<R>) * padded_len<R>(n)) + 2 * (size_t)(win ? 4 : 2) * row_len * sizeof(double);
-}
-template <typename R>
-__host__ __device__ constexpr size_t inv_pipe_smem(int n, int hx) {
-  return align16(sizeof(cx_t<R>) * padded_len<R>(n)) + 2 * (size_t)hx * 2 * sizeof(cx_t<R>);
-}
-
-// threads of a persistent row CTA, and the resident CTAs per SM its register
-// budget is sized for (FP32: three, so the loop's hoisted addresses do not
-// push it to one)
-template <int EPT, int FIX>
-__host__ __device__ constexpr int pipe_threads() { return ((FIX / EPT + 31) / 32) * 32; }
-template <typename R, int EPT, int FIX>
-__host__ __device__ constexpr int pipe_min_blocks() {
-  return (sizeof(R) == 4 && pipe_threads<EPT, FIX>() <= 256) ? 3 : 1;
-}
-
-template <typename R, int EPT, int FIX>
-__global__ void __launch_bounds__(pipe_threads<EPT, FIX>(), pipe_min_blocks<R, EPT, FIX>()) k_rows_fwd_pipe(FftPlanT<R> pl, const double* __restrict__ in, long long comp_stride, int row_len,
-                                int nrows, const double* __restrict__ w, cx_t<R>* __restrict__ S, int ld, int Hx,
-                                int ncomp, int* err) {
-  pdl_entry();
-  extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ uint64_t mbar[2];
-  constexpr int n = FIX;
-  constexpr int np = padded_len<R>(n);
-  cx_t<R>* buf = reinterpret_cast<cx_t<R>*>(smraw);
-  double* stg = reinterpret_cast<double*>(smraw + align16(sizeof(cx_t<R>) * np));
-  const int sdb = (w ? 4 : 2) * row_len;   // doubles per staging buffer
-  const int npairs = (nrows + 1) / 2, nitems = ncomp * npairs;
-  const uint32_t rbytes = (uint32_t)row_len * 8u;
-  auto issue = [&](int item, int sb) {     // thread 0
-    const int c = item / npairs, ya = 2 * (item - c * npairs), yb = ya + 1;
-    const bool two = yb < nrows;
-    double* dst = stg + sb * sdb;
-    const double* src = in + (long long)c * comp_stride;
-    fence_proxy_async_smem();   // the buffer's last generic reads come before the async writes
-    mbar_arrive_expect_tx(&mbar[sb], rbytes * (two ? 2u : 1u) * (w ? 2u : 1u));
-    bulk_g2s(dst, src + (long long)ya * row_len, rbytes, &mbar[sb]);
-    if (two) bulk_g2s(dst + row_len, src + (long long)yb * row_len, rbytes, &mbar[sb]);
-    if (w) {
-      bulk_g2s(dst + 2 * row_len, w + (long long)ya * row_len, rbytes, &mbar[sb]);
-      if (two) bulk_g2s(dst + 3 * row_len, w + (long long)yb * row_len, rbytes, &mbar[sb]);
-    }
-  };
-  if (threadIdx.x == 0) {
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
-    mbar_init_fence();
-  }
-  __syncthreads();
-  uint32_t ph0 = 0u, ph1 = 0u;
-  bool pend0 = false, pend1 = false;
-  int item = blockIdx.x, sb = 0;
-  if (item < nitems) {
-    if (threadIdx.x == 0) issue(item, 0);
-    pend0 = true;
-  }
-  bool bad = false;
-  for (; item < nitems; item += gridDim.x, sb ^= 1) {
-    const int nxt = item + gridDim.x;
-    if (nxt < nitems) {
-      if (threadIdx.x == 0) issue(nxt, sb ^ 1);
-      if (sb) pend0 = true;
-      else pend1 = true;
-    }
-    const bool ok = mbar_wait(&mbar[sb], sb ? ph1 : ph0, kRowsWaitLimit);
-    if (__syncthreads_or(!ok)) { bad = true; break; }
-    if (sb) { ph1 ^= 1u; pend1 = false; }
-    else { ph0 ^= 1u; pend0 = false; }
-    const int c = item / npairs, ya = 2 * (item - c * npairs), yb = ya + 1;
-    const bool has_b = yb < nrows;
-    const double* xa = stg + sb * sdb;
-    const double* xb = xa + row_len;
-    const double* wa = xa + 2 * row_len;
-    const double* wb = xa + 3 * row_len;
-    auto load_in = [&](int i) -> cx_t<R> {
-      double va = 0.0, vb = 0.0;
-      if (i < row_len) {
-        va = xa[i] * (w ? wa[i] : 1.0);
-        if (has_b) vb = xb[i] * (w ? wb[i] : 1.0);
-      }
-      return mk<R>((R)va, (R)vb);
-    };
-    const int tx = opaque_tid();
-    constexpr RadixList L = fixed_radices(FIX);
-    constexpr int R0 = L.r[0];
-    if constexpr (R0 % 2 == 0) {
-      if (2 * row_len <= FIX) stockham_first_pass_ld<R, R0, -1, EPT, true, true>(buf, FIX, load_in, tx);
-      else stockham_first_pass_ld<R, R0, -1, EPT, true, false>(buf, FIX, load_in, tx);
-    } else {
-      stockham_first_pass_ld<R, R0, -1, EPT, true, false>(buf, FIX, load_in, tx);
-    }
-    fft_fixed<R, -1, EPT, true, FIX, 1, L.nr, R0>(buf, pl, tx);
-    for (int e = tx; e < Hx * 2; e += blockDim.x) {
-      const int kx = e >> 1, which = e & 1;
-      const int y = ya + which;
-      if (y >= nrows) continue;
-      const cx_t<R> zk = buf[fpad<R, true>(kx)];
-      const cx_t<R> zm = buf[fpad<R, true>(kx == 0 ? 0 : n - kx)];   // (n - kx) mod n
-      cx_t<R> out;
-      if (!which) out = mk<R>(R(0.5) * (zk.x + zm.x), R(0.5) * (zk.y - zm.y));
-      else out = mk<R>(R(0.5) * (zk.y + zm.y), R(-0.5) * (zk.x - zm.x));
-      S[((long long)c * Hx + kx) * ld + y] = out;
-    }
-    __syncthreads();   // the transform buffer and staging buffer sb are free again
-  }
-  if (bad) {
-    if (threadIdx.x == 0) {
-      atomicExch(err, 1);
-      // copies still in flight land before the CTA exits (bounded)
-      if (pend0) mbar_wait(&mbar[0], ph0, kRowsWaitLimit);
-      if (pend1) mbar_wait(&mbar[1], ph1, kRowsWaitLimit);
-    }
-    __syncthreads();
-  }
-}
-
-// one item of k_rows_inv_pipe: the packed spectrum of the row pair (the
-// arithmetic of k_rows_inv's load) from staging buffer st, the transform,
-// and the kept outputs written to HBM.  Not inlined: the item's registers are
-// then those of one transform, not of one transform plus the item loop.
-template <typename R, int EPT, int FIX>
-__device__ __noinline__ void inv_pipe_item(const FftPlanT<R>& pl, const cx_t<R>* st, cx_t<R>* buf, int Hx,
-                                           double* dst, int ya, int ng) {
-  using C = cx_t<R>;
-  constexpr int n = FIX;
-  const int tx = threadIdx.x;
-  for (int kk = tx; kk < Hx; kk += blockDim.x) {
-    C A = st[2 * kk], B = st[2 * kk + 1];
-    if (kk == 0 || kk == n / 2) { A.y = R(0); B.y = R(0); }   // n is even
-    buf[fpad<R, true>(kk)] = mk<R>(A.x - B.y, A.y + B.x);
-    if (kk >= 1 && kk <= n - Hx) {
-      A.y = -A.y;
-      B.y = -B.y;
-      buf[fpad<R, true>(n - kk)] = mk<R>(A.x - B.y, A.y + B.x);
-    }
-  }
-  __syncthreads();
-  const int yb = ya + 1;
-  auto st_out = [&](int i, C z) {
-    if (i < ng) {
-      dst[(long long)ya * ng + i] = (double)z.x;
-      dst[(long long)yb * ng + i] = (double)z.y;
-    }
-  };
-  constexpr RadixList L = fixed_radices(FIX);
-  constexpr int RL = L.r[L.nr - 1];
-  fft_fixed<R, +1, EPT, true, FIX, 0, L.nr - 1, 1>(buf, pl);
-  if constexpr (RL % 2 == 0) {
-    if (2 * ng <= FIX) stockham_last_pass_st<R, RL, +1, EPT, true, true>(buf, pl, FIX, st_out);
-    else stockham_last_pass_st<R, RL, +1, EPT, true, false>(buf, pl, FIX, st_out);
-  } else {
-    stockham_last_pass_st<R, RL, +1, EPT, true, false>(buf, pl, FIX, st_out);
-  }
-}
-
-template <typename R, int EPT, int FIX>
-__global__ void __launch_bounds__(pipe_threads<EPT, FIX>(), pipe_min_blocks<R, EPT, FIX>()) k_rows_inv_pipe(
-    FftPlanT<R> pl, const cx_t<R>* __restrict__ S, int ld, int nrows, int Hx, double* __restrict__ h,
-    long long comp_stride, int ng) {
-  pdl_entry();
-  using C = cx_t<R>;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int np = padded_len<R>(FIX);
-  C* buf = reinterpret_cast<C*>(smraw);
-  C* stg = reinterpret_cast<C*>(smraw + align16(sizeof(C) * np));   // [2][Hx][2]
-  const int npairs = nrows / 2, nitems = 3 * npairs;   // nrows even
-  // rows ya, ya + 1 of every spectrum column of component c: 2 C per column
-  auto issue = [&](int item, int sb) {
-    const int c = item / npairs, ya = 2 * (item - c * npairs);
-    C* dst = stg + (size_t)sb * Hx * 2;
-    const C* src = S + (long long)c * Hx * ld + ya;
-    for (int kk = threadIdx.x; kk < Hx; kk += blockDim.x) {
-      if constexpr (sizeof(C) == 8) {
-        cp_async<16>(dst + 2 * kk, src + (long long)kk * ld);
-      } else {
-        cp_async<16>(dst + 2 * kk, src + (long long)kk * ld);
-        cp_async<16>(dst + 2 * kk + 1, src + (long long)kk * ld + 1);
-      }
-    }
-  };
-  int item = blockIdx.x, sb = 0;
-  if (item < nitems) issue(item, 0);
-  cp_async_commit();
-  for (; item < nitems; item += gridDim.x, sb ^= 1) {
-    const int nxt = item + gridDim.x;
-    if (nxt < nitems) issue(nxt, sb ^ 1);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
-    const int c = item / npairs, ya = 2 * (item - c * npairs);
-    inv_pipe_item<R, EPT, FIX>(pl, stg + (size_t)sb * Hx * 2, buf, Hx, h + (long long)c * comp_stride, ya, ng);
-    __syncthreads();   // the transform buffer and staging buffer sb are free again
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");   // (only empty groups remain)
-}
-
 // ── Newell tensor (81-point average of the closed-form integrals) ────────
 // Same term grouping as the reference's ctt/calt (demag_fft.cu:27-91).
 __device__ void newell_point(double thick, double sx, double sy, double out[9]) {
@@ -689,7 +476,6 @@ struct HostFft {
 struct LaunchCfg {
   int nb = 1, ept = 8;
   bool stage = false;
-  bool pipe = false;   // rows: the persistent double-buffered kernel (nb = 1, compile-time plans)
 };
 
 struct DemagPlan {
@@ -712,11 +498,7 @@ struct DemagPlan {
   float* d_tzzf = nullptr;
   float2* d_txyf = nullptr;
   LaunchCfg rows[2], cols[2];    // [0] FP64 chain, [1] FP32 chain (autotuned)
-  int* d_err = nullptr;          // wait-ran-out flag of the asynchronous-copy kernels (the context's SLOT_TCERR)
-  int num_sms = 148;
-  // resident CTAs per SM of the persistent row kernels: [prec][ept 8/16][window] (fwd), [prec][ept] (inv)
-  int occ_fwd[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
-  int occ_inv[2][2] = {{0, 0}, {0, 0}};
+  int* d_err = nullptr;          // wait-ran-out flag of the tensor-core column stage (the context's SLOT_TCERR)
   DemagTc* tc = nullptr;         // tensor-core column stage (k_demag_tc.cu), when the shape allows
   cudaGraphExec_t gexec = nullptr;   // captured chain for gkey = (y, w, h) on the context's own stream
   const void* gkey[3] = {nullptr, nullptr, nullptr};
@@ -875,40 +657,6 @@ static ColsFn<R> cols_fn(int fix, int ept, bool stage) {
 }
 static ColsFwdFn cols_fwd_fn(int fix, int ept) { return ept == 8 ? cols_fwd_fn_t<8>(fix) : cols_fwd_fn_t<16>(fix); }
 
-template <typename R>
-using RowsFwdPipeFn = void (*)(FftPlanT<R>, const double*, long long, int, int, const double*, cx_t<R>*, int, int, int,
-                               int*);
-template <typename R>
-using RowsInvPipeFn = void (*)(FftPlanT<R>, const cx_t<R>*, int, int, int, double*, long long, int);
-template <typename R, int EPT>
-static RowsFwdPipeFn<R> fwd_pipe_fn_t(int fix) {
-  switch (fix) {
-    case 1024: return k_rows_fwd_pipe<R, EPT, 1024>;
-    case 2048: return k_rows_fwd_pipe<R, EPT, 2048>;
-    case 3072: return k_rows_fwd_pipe<R, EPT, 3072>;
-    case 4096: return k_rows_fwd_pipe<R, EPT, 4096>;
-    default: return nullptr;
-  }
-}
-template <typename R, int EPT>
-static RowsInvPipeFn<R> inv_pipe_fn_t(int fix) {
-  switch (fix) {
-    case 1024: return k_rows_inv_pipe<R, EPT, 1024>;
-    case 2048: return k_rows_inv_pipe<R, EPT, 2048>;
-    case 3072: return k_rows_inv_pipe<R, EPT, 3072>;
-    case 4096: return k_rows_inv_pipe<R, EPT, 4096>;
-    default: return nullptr;
-  }
-}
-template <typename R>
-static RowsFwdPipeFn<R> fwd_pipe_fn(int fix, int ept) {
-  return ept == 8 ? fwd_pipe_fn_t<R, 8>(fix) : fwd_pipe_fn_t<R, 16>(fix);
-}
-template <typename R>
-static RowsInvPipeFn<R> inv_pipe_fn(int fix, int ept) {
-  return ept == 8 ? inv_pipe_fn_t<R, 8>(fix) : inv_pipe_fn_t<R, 16>(fix);
-}
-
 // threads per block a kernel can be launched with (its register use)
 static int max_threads(const void* fn) {
   cudaFuncAttributes at{};
@@ -919,33 +667,10 @@ static int max_threads(const void* fn) {
   return at.maxThreadsPerBlock;
 }
 
-static bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
-
-// the persistent forward kernel takes this call: a compile-time plan, rows
-// and component strides whole 16-byte multiples, aligned bases, resident CTAs
-template <typename R>
-static bool fwd_pipe_usable(const DemagPlan* d, int ept, const double* in, long long cs, int row_len, const double* w) {
-  return d->fx.fix && row_len % 2 == 0 && cs % 2 == 0 && al16(in) && (!w || al16(w)) &&
-         d->occ_fwd[kp<R>()][ept == 16][w != nullptr] > 0;
-}
-template <typename R>
-static bool inv_pipe_usable(const DemagPlan* d, int ept) {
-  return d->fx.fix && d->ny % 2 == 0 && d->occ_inv[kp<R>()][ept == 16] > 0;
-}
-
 template <typename R>
 static int launch_rows_fwd(const DemagPlan* d, cudaStream_t s, const double* in, long long cs, int row_len,
                            int nrows, const double* w, cx_t<R>* S, int ld, int ncomp, const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fx.dev<R>();
-  if (k.pipe && k.nb == 1 && fwd_pipe_usable<R>(d, k.ept, in, cs, row_len, w)) {
-    const int items = ncomp * ((nrows + 1) / 2);
-    const int grid = std::min(items, d->num_sms * d->occ_fwd[kp<R>()][k.ept == 16][w != nullptr]);
-    const size_t sm = fwd_pipe_smem<R>(d->px, row_len, w != nullptr);
-    klaunch(fwd_pipe_fn<R>(d->fx.fix, k.ept), grid, d->fx.tx_for(k.ept), sm, s, pl, in, cs, row_len, nrows, w, S, ld,
-            d->hx, ncomp, d->d_err);
-    LLG_CUDA_TRY(cudaPeekAtLastError());
-    return 0;
-  }
   const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((nrows + 2 * k.nb - 1) / (2 * k.nb), ncomp), b(d->fx.tx_for(k.ept), k.nb);
   klaunch(rows_fwd_fn<R>(d->fx.fix, k.nb, k.ept), g, b, sm, s, pl, in, cs, row_len, nrows, w, S, ld, d->hx);
@@ -957,14 +682,6 @@ template <typename R>
 static int launch_rows_inv(const DemagPlan* d, cudaStream_t s, const cx_t<R>* S, double* h, long long cs,
                            const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fx.dev<R>();
-  if (k.pipe && k.nb == 1 && inv_pipe_usable<R>(d, k.ept)) {
-    const int items = 3 * (d->ny / 2);
-    const int grid = std::min(items, d->num_sms * d->occ_inv[kp<R>()][k.ept == 16]);
-    klaunch(inv_pipe_fn<R>(d->fx.fix, k.ept), grid, d->fx.tx_for(k.ept), inv_pipe_smem<R>(d->px, d->hx), s, pl, S,
-            d->ny, d->ny, d->hx, h, cs, d->ng);
-    LLG_CUDA_TRY(cudaPeekAtLastError());
-    return 0;
-  }
   const size_t sm = sizeof(cx_t<R>) * (size_t)k.nb * padded_len<R>(d->px);
   const dim3 g((d->ny + 2 * k.nb - 1) / (2 * k.nb), 3), b(d->fx.tx_for(k.ept), k.nb);
   klaunch(rows_inv_fn<R>(d->fx.fix, k.nb, k.ept), g, b, sm, s, pl, S, d->ny, d->ny, d->hx, h, cs, d->ng);
@@ -1026,33 +743,6 @@ static int set_smem_all(DemagPlan* d) {
           (rc = set_smem((const void*)rows_inv_fn<R>(d->fx.fix, nb, ept), r)))
         return rc;
     }
-  // persistent row kernels: shared memory opt-in and resident CTAs per SM
-  // (0 when the kernel does not fit: the launch then takes the plain kernel)
-  if (d->fx.fix) {
-    for (int ept = 8; ept <= 16; ept *= 2) {
-      const int threads = d->fx.tx_for(ept);
-      const void* ff = (const void*)fwd_pipe_fn<R>(d->fx.fix, ept);
-      for (int win = 0; win <= 1; win++) {
-        const size_t sm = fwd_pipe_smem<R>(d->px, d->ng, win != 0);
-        int occ = 0;
-        if (sm <= 227 * 1024 && threads <= max_threads(ff) && !set_smem(ff, sm) &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ff, threads, sm) != cudaSuccess) {
-          cudaGetLastError();
-          occ = 0;
-        }
-        d->occ_fwd[kp<R>()][ept == 16][win] = occ;
-      }
-      const void* fi = (const void*)inv_pipe_fn<R>(d->fx.fix, ept);
-      const size_t smi = inv_pipe_smem<R>(d->px, d->hx);
-      int occ = 0;
-      if (smi <= 227 * 1024 && threads <= max_threads(fi) && !set_smem(fi, smi) &&
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fi, threads, smi) != cudaSuccess) {
-        cudaGetLastError();
-        occ = 0;
-      }
-      d->occ_inv[kp<R>()][ept == 16] = occ;
-    }
-  }
   const size_t c0 = cols_smem<R>(d, false), c1 = cols_smem<R>(d, true);
   for (int ept = 8; ept <= 16; ept *= 2) {
     if ((rc = set_smem((const void*)cols_fn<R>(d->fy.fix, ept, false), c0))) return rc;
@@ -1118,23 +808,18 @@ static int demag_autotune(llg_ctx* c, DemagPlan* d, cx_t<R>* S, const R* txx, co
   };
   LaunchCfg best_r = d->rows[kp<R>()], best_c = d->cols[kp<R>()];
   float tbest = 1e30f;
-  for (int pipe = 0; pipe <= 1; pipe++)
-    for (int nb = 1; nb <= 2; nb++)
-      for (int ept = 8; ept <= 16; ept *= 2) {
-        if (!rows_ok<R>(d, nb, ept)) continue;
-        if (pipe && (nb != 1 || !fwd_pipe_usable<R>(d, ept, c->d_hd, cs, d->ng, nullptr) ||
-                     !inv_pipe_usable<R>(d, ept)))
-          continue;
-        LaunchCfg k;
-        k.nb = nb;
-        k.ept = ept;
-        k.pipe = pipe != 0;
-        const float t = timed([&]() {
-          int rc = launch_rows_fwd<R>(d, s, c->d_hd, cs, d->ng, d->ny, nullptr, S, d->ny, 3, k);
-          return rc ? rc : launch_rows_inv<R>(d, s, S, c->d_pm, cs, k);
-        });
-        if (t < tbest) { tbest = t; best_r = k; }
-      }
+  for (int nb = 1; nb <= 2; nb++)
+    for (int ept = 8; ept <= 16; ept *= 2) {
+      if (!rows_ok<R>(d, nb, ept)) continue;
+      LaunchCfg k;
+      k.nb = nb;
+      k.ept = ept;
+      const float t = timed([&]() {
+        int rc = launch_rows_fwd<R>(d, s, c->d_hd, cs, d->ng, d->ny, nullptr, S, d->ny, 3, k);
+        return rc ? rc : launch_rows_inv<R>(d, s, S, c->d_pm, cs, k);
+      });
+      if (t < tbest) { tbest = t; best_r = k; }
+    }
   if (tune_cols) {
     tbest = 1e30f;
     for (int ept = 8; ept <= 16; ept *= 2)
@@ -1182,7 +867,6 @@ int demag_create(llg_ctx* c) {
   d->hx = d->px / 2 + 1;
   d->strength = p.demag_strength;
   d->d_err = reinterpret_cast<int*>(c->d_scal + SLOT_TCERR);
-  d->num_sms = c->num_sms;
   int rc = fft_init(d->fx, d->px, kRowsNB);
   if (!rc) rc = fft_init(d->fy, d->py, 3);
   if (rc) { demag_destroy(d); return rc; }
@@ -1373,8 +1057,8 @@ int demag_stage(llg_ctx* c, int stage, const double* y, double* h) {
 }
 
 // a plan whose kernels wait on asynchronous completions (the tensor-core
-// column stage, the persistent row kernels) can have set the flag
-static bool demag_waits(const DemagPlan* d) { return d && (d->tc || d->rows[0].pipe || d->rows[1].pipe); }
+// column stage) can have set the flag
+static bool demag_waits(const DemagPlan* d) { return d && d->tc; }
 
 int demag_check(llg_ctx* c) {
   if (!demag_waits(c->demag)) return 0;
@@ -1382,7 +1066,7 @@ int demag_check(llg_ctx* c) {
   cudaMemcpyAsync(&f, c->demag->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
   cudaStreamSynchronize(c->stream);
   if (f) {
-    llg_set_error("demag: a tensor-core or asynchronous-copy completion wait ran out (results invalid)");
+    llg_set_error("demag: a tensor-core completion wait ran out (results invalid)");
     return LLG_ERR_TIMEOUT;
   }
   return 0;
@@ -1393,7 +1077,7 @@ int demag_check_last(llg_ctx* c) {
   int f = 0;
   memcpy(&f, c->h_scal + SLOT_TCERR, sizeof(int));
   if (f) {
-    llg_set_error("demag: a tensor-core or asynchronous-copy completion wait ran out (results invalid)");
+    llg_set_error("demag: a tensor-core completion wait ran out (results invalid)");
     return LLG_ERR_TIMEOUT;
   }
   return 0;
