@@ -444,3 +444,29 @@ def test_full_demag_jacobian_integration_matches_oracle(oracle_lib, gpu):
     print(f"GMRES iterations per Newton iteration, strength 8: reference Jv {its[llg.JV_REFERENCE]:.3f}, "
           f"with the demag derivative {its[llg.JV_FULL_DEMAG]:.3f}")
     assert its[llg.JV_FULL_DEMAG] <= its[llg.JV_REFERENCE] + 1e-12
+
+
+# Every compile-time transform length (1024, 2048, 3072, 4096: fixed_radices,
+# dev_fft.cuh) in the row and in the column direction, open and periodic,
+# against the oracle: FP64 rel 1e-11, the mixed chain (FP32 rows, FP32 or
+# tensor-core columns) rel 5e-6.
+FIXED_SHAPES = [(llg.DEMAG_OPEN, 512, 24), (llg.DEMAG_OPEN, 1024, 12), (llg.DEMAG_OPEN, 1536, 8),
+                (llg.DEMAG_OPEN, 2048, 6), (llg.DEMAG_PERIODIC, 3072, 5), (llg.DEMAG_OPEN, 20, 512),
+                (llg.DEMAG_OPEN, 12, 1024), (llg.DEMAG_OPEN, 6, 2048), (llg.DEMAG_PERIODIC, 9, 4096)]
+
+
+@pytest.mark.parametrize("prec", [llg.DEMAG_FP64, llg.DEMAG_MIXED])
+@pytest.mark.parametrize("mode,ng,ny", FIXED_SHAPES)
+def test_demag_fixed_plan_lengths_match_oracle(oracle_lib, gpu, mode, ng, ny, prec):
+    import torch
+    p = llg.default_params(ng, ny, demag_mode=mode, demag_strength=2.0, bc=llg.BC_PERIODIC, demag_precision=prec)
+    ctx = llg.Context(p)
+    o = oracle_lib.Oracle(p)
+    y = np.random.default_rng(21).uniform(-1.0, 1.0, 3 * ng * ny)
+    dh = torch.zeros(3 * ng * ny, dtype=torch.float64, device="cuda")
+    ctx.demag_apply(dev(torch, y), dh)
+    torch.cuda.synchronize()
+    err = rel_err(dh.cpu().numpy(), o.demag(y))
+    print(f"{'open' if mode == llg.DEMAG_OPEN else 'periodic'} {ng}x{ny} "
+          f"{'FP64' if prec == llg.DEMAG_FP64 else 'mixed'}: rel err {err:.2e}")
+    assert err < (1e-11 if prec == llg.DEMAG_FP64 else 5e-6)
