@@ -17,10 +17,12 @@
 //                 the tensor, written SoA for the first ng columns only.
 // Every transform is a Stockham autosort FFT in shared memory (natural order
 // in and out, no reordering tables): each pass stages the thread's radix-R
-// butterflies (R = 8/4/2/3/5; any other prime through a generic path) in
-// registers, synchronises, and scatters the results in place.  A CTA row of
-// threads owns one transform; HBM sees each element of y, S and h once per
-// kernel.
+// butterflies in registers, synchronises, and scatters the results in place.
+// The lengths 1024/2048/3072/4096 run a compile-time plan (radix 16 first,
+// then one 12/8/6/4/2 pass; the kernels are instantiated per length, FIX),
+// every other length a runtime plan (radix 8/4/2/3/5, any other prime through
+// a generic path).  A CTA row of threads owns one transform; HBM sees each
+// element of y, S and h once per kernel.
 // The tensor is stored wrapped at displacement d mod P (d in [-P/2, P-1-P/2]),
 // which equals the reference's centring + output shift; the open-boundary
 // tensor has its unused d = -P/2 lines zeroed, so its spectra are real.  Only
@@ -129,10 +131,13 @@ __device__ __forceinline__ void col_fft(cx_t<R>* buf, const FftPlanT<R>& pl) {
 }
 
 // ── K2: column transform + tensor multiply + inverse column transform ─────
-// CTA = one x-frequency column; threadIdx.y = component.  The three spectrum
-// columns and (STAGE) this column's tensor spectra are fetched with
-// asynchronous copies (cp.async) at entry, so the tensor read overlaps the
-// forward transform instead of stalling the multiply.
+// CTA = one x-frequency column; threadIdx.y = component when blockDim.y = 3,
+// or one row of threads transforms the three components in turn when
+// blockDim.y = 1 (long FP64 columns, whose registers allow only a third of
+// the threads).  The three spectrum columns and (STAGE) this column's tensor
+// spectra are fetched with asynchronous copies (cp.async) at entry, so the
+// tensor read overlaps the forward transform instead of stalling the
+// multiply.
 template <typename R, int EPT, bool STAGE, int FIX>
 __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
                             const R* __restrict__ txx, const R* __restrict__ tyy, const R* __restrict__ tzz,
@@ -143,18 +148,19 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
   C* sm = reinterpret_cast<C*>(smraw);
   const int kx = blockIdx.x;
   const int n = FIX > 0 ? FIX : pl.n;
-  const int c = threadIdx.y;
-  C* buf = sm + c * n;
-  C* col = S + ((long long)c * Hx + kx) * ld;
   const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
   const long long tb = (long long)kx * n;
   R* sxx = reinterpret_cast<R*>(sm + 3 * n);
   R* syy = sxx + n;
   R* szz = syy + n;
   C* sxy = reinterpret_cast<C*>(szz + n);
-  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) {
-    if (yy < nrows) cp_async<sizeof(C)>(&buf[yy], &col[yy]);
-    else buf[yy] = mk<R>(R(0), R(0));
+  for (int c = threadIdx.y; c < 3; c += blockDim.y) {
+    C* buf = sm + c * n;
+    const C* col = S + ((long long)c * Hx + kx) * ld;
+    for (int yy = threadIdx.x; yy < n; yy += blockDim.x) {
+      if (yy < nrows) cp_async<sizeof(C)>(&buf[yy], &col[yy]);
+      else buf[yy] = mk<R>(R(0), R(0));
+    }
   }
   cp_async_commit();
   if (STAGE) {
@@ -170,7 +176,7 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
   cp_async_commit();
   cp_async_wait<1>();
   __syncthreads();
-  col_fft<R, -1, EPT, FIX>(buf, pl);
+  for (int c = threadIdx.y; c < 3; c += blockDim.y) col_fft<R, -1, EPT, FIX>(sm + c * n, pl);   // uniform trip count
   cp_async_wait<0>();
   __syncthreads();
   for (int ky = tid; ky < n; ky += T) {
@@ -185,8 +191,12 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
     sm[2 * n + ky] = mk<R>(d * mz.x, d * mz.y);
   }
   __syncthreads();
-  col_fft<R, +1, EPT, FIX>(buf, pl);
-  for (int yy = threadIdx.x; yy < nrows; yy += blockDim.x) col[yy] = buf[yy];
+  for (int c = threadIdx.y; c < 3; c += blockDim.y) {
+    C* buf = sm + c * n;
+    col_fft<R, +1, EPT, FIX>(buf, pl);
+    C* col = S + ((long long)c * Hx + kx) * ld;
+    for (int yy = threadIdx.x; yy < nrows; yy += blockDim.x) col[yy] = buf[yy];
+  }
 }
 
 // forward column transform only (tensor spectra at init, FP64)
@@ -476,6 +486,7 @@ struct HostFft {
 struct LaunchCfg {
   int nb = 1, ept = 8;
   bool stage = false;
+  int cy = 3;   // columns: components transformed concurrently (3) or in turn (1)
 };
 
 struct DemagPlan {
@@ -693,7 +704,7 @@ template <typename R>
 static int launch_cols_conv(const DemagPlan* d, cudaStream_t s, cx_t<R>* S, const R* txx, const R* tyy,
                             const R* tzz, const cx_t<R>* txy, const LaunchCfg& k) {
   const FftPlanT<R> pl = d->fy.dev<R>();
-  const dim3 b(d->fy.tx_for(k.ept), 3);
+  const dim3 b(d->fy.tx_for(k.ept), k.cy);
   const size_t base = sizeof(cx_t<R>) * 3 * (size_t)d->py;
   const size_t sm = k.stage ? base + (sizeof(R) * 3 + sizeof(cx_t<R>)) * (size_t)d->py : base;
   klaunch(cols_fn<R>(d->fy.fix, k.ept, k.stage), d->hx, b, sm, s, pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy);
@@ -723,8 +734,8 @@ static size_t cols_smem(const DemagPlan* d, bool stage) {
   return stage ? base + (sizeof(R) * 3 + sizeof(cx_t<R>)) * (size_t)d->py : base;
 }
 template <typename R>
-static bool cols_ok(const DemagPlan* d, int ept, bool stage) {
-  const int threads = d->fy.tx_for(ept) * 3;
+static bool cols_ok(const DemagPlan* d, int ept, bool stage, int cy = 3) {
+  const int threads = d->fy.tx_for(ept) * cy;
   if (threads > 1024 || threads > max_threads((const void*)cols_fn<R>(d->fy.fix, ept, stage))) return false;
   if (!stage) return cols_smem<R>(d, false) <= 227 * 1024;
   return d->py % (int)(16 / sizeof(R)) == 0 && cols_smem<R>(d, true) <= 200 * 1024;
@@ -754,9 +765,11 @@ static int set_smem_all(DemagPlan* d) {
   LaunchCfg& cl = d->cols[kp<R>()];
   rw.nb = 1;
   rw.ept = rows_ok<R>(d, 1, 8) ? 8 : 16;
-  cl.ept = cols_ok<R>(d, 8, false) ? 8 : 16;
-  cl.stage = cols_ok<R>(d, cl.ept, true);
-  if (!rows_ok<R>(d, rw.nb, rw.ept) || !cols_ok<R>(d, cl.ept, false)) {
+  cl.cy = 3;
+  if (!cols_ok<R>(d, 8, false) && !cols_ok<R>(d, 16, false)) cl.cy = 1;   // long FP64 columns
+  cl.ept = cols_ok<R>(d, 8, false, cl.cy) ? 8 : 16;
+  cl.stage = cols_ok<R>(d, cl.ept, true, cl.cy);
+  if (!rows_ok<R>(d, rw.nb, rw.ept) || !cols_ok<R>(d, cl.ept, false, cl.cy)) {
     llg_set_error("demag grid too large for the shared-memory transform");
     return LLG_ERR_NOTSUP;
   }
@@ -822,12 +835,14 @@ static int demag_autotune(llg_ctx* c, DemagPlan* d, cx_t<R>* S, const R* txx, co
     }
   if (tune_cols) {
     tbest = 1e30f;
+    for (int cy = 3; cy >= 1; cy -= 2)
     for (int ept = 8; ept <= 16; ept *= 2)
       for (int st = 0; st <= 1; st++) {
-        if (!cols_ok<R>(d, ept, st != 0)) continue;
+        if (!cols_ok<R>(d, ept, st != 0, cy)) continue;
         LaunchCfg k;
         k.ept = ept;
         k.stage = st != 0;
+        k.cy = cy;
         const float t = timed([&]() { return launch_cols_conv<R>(d, s, S, txx, tyy, tzz, txy, k); });
         if (t < tbest) { tbest = t; best_c = k; }
       }
