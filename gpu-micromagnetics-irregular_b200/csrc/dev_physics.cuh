@@ -200,10 +200,8 @@ __device__ __forceinline__ void load_tile(const DevProblem& P, Tile<NF>& T, cons
   __syncthreads();
 }
 
-// field at a tile cell from the staged neighbours (exchange + aniso + DMI);
-// W = the staged plane's row length
-template <int W>
-__device__ __forceinline__ void tile_field(const DevProblem& P, const double (*F)[TY + 2][W],
+// field at a tile cell from the staged neighbours (exchange + aniso + DMI)
+__device__ __forceinline__ void tile_field(const DevProblem& P, const double (*F)[TY + 2][TX + 2],
                                            int sx, int sy, const double m[3], const double msk[3],
                                            const double nsk[3], double h[3]) {
   double an[3];

@@ -358,19 +358,12 @@ __global__ void __launch_bounds__(TX * TY, 4) k_arnoldi_tile(DevProblem P, const
 // with it.  The gate of a cell is read ahead of the stencil wait, its stored
 // block inverse ahead of the stencil arithmetic.
 constexpr int AP_SLOTS = (TY + 2) * TX + (TY + 2) * 2;   // staged stencil slots per component
-// Plane rows hold [pad][halo][TX interior cells][halo][pad]: the interior
-// starts 16 bytes into the row (2 doubles; 4 floats in the FP32 input plane)
-// and rows are whole multiples of 16 bytes, so a tile whose columns lie inside
-// the grid stages its interior rows with 16-byte copies.
-constexpr int APW = TX + 4, APX = 2;                     // double planes: row length, interior offset
-constexpr int APWF = TX + 8, APXF = 4;                   // float input plane (FP32 basis)
-constexpr int AP_PLANE = (TY + 2) * APW;                 // doubles per stencil component
-constexpr int AP_PLANEF = (TY + 2) * APWF;               // floats per FP32 input component
+constexpr int AP_PLANE = (TY + 2) * (TX + 2);            // doubles per stencil component
 constexpr int AP_CELLS = TX * TY;
 constexpr int AP_NT = TX * TY;
 __host__ __device__ constexpr int ap_buf_doubles(int jv_full, int f32 = 0) {
   // (an FP32 basis stages its input in a float plane after the doubles)
-  return 9 * AP_PLANE + (jv_full ? 3 : 0) * AP_CELLS + (f32 ? (3 * AP_PLANEF + 1) / 2 : 0);
+  return 9 * AP_PLANE + (jv_full ? 3 : 0) * AP_CELLS + (f32 ? (3 * AP_PLANE + 1) / 2 : 0);
 }
 
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool ok) {
@@ -382,11 +375,6 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src, bool ok) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
   const int sz = ok ? 4 : 0;   // 0: zero-fill, nothing read
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(sz) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool ok) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-  const int sz = ok ? 16 : 0;   // 0: zero-fill, nothing read
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(sz) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
@@ -419,75 +407,30 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const V
   const int gx = (ng + TX - 1) / TX, ntiles = gx * ((ny + TY - 1) / TY);
   const int bufd = ap_buf_doubles(P.jv_full, F32 ? 1 : 0);
   const int foff = ap_buf_doubles(P.jv_full);   // the float staging plane (FP32 basis)
-  typedef double Plane[TY + 2][APW];
-  typedef float FPlane[TY + 2][APWF];
-  // 16-byte interior copies need every row start of the staged arrays at a
-  // 16-byte boundary: 16-byte-aligned bases, ng even (doubles) or a multiple
-  // of 4 (the float input)
-  const bool vec = (ng % (F32 ? 4 : 2)) == 0 &&
-                   ((reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(s) |
-                     reinterpret_cast<uintptr_t>(in)) & 15u) == 0;
+  typedef double Plane[TY + 2][TX + 2];
+  typedef float FPlane[TY + 2][TX + 2];
 
   auto issue = [&](int t, double* B) {
     const int x0 = (t % gx) * TX, y0 = (t / gx) * TY;
     Plane* Y = reinterpret_cast<Plane*>(B);
     Plane* V = Y + 3;
     Plane* S = Y + 6;
-    FPlane* Fv = reinterpret_cast<FPlane*>(B + foff);
-    if (vec && x0 + TX <= ng) {
-      // interior rows: TX/2 16-byte chunks of y, s (and an FP64 input) per row
-      for (int q = tid; q < (TY + 2) * (TX / 2); q += AP_NT) {
-        const int sy = q / (TX / 2), k2 = q - sy * (TX / 2);
-        int gi = x0 + 2 * k2, gj = y0 - 1 + sy;
-        const bool ok = map_nb(gi, gj, ng, ny, P.bc);
-        const long long cell = ok ? (long long)gj * ng + gi : 0;
+    for (int q = tid; q < AP_SLOTS; q += AP_NT) {
+      int sx, sy;
+      ap_slot(q, sx, sy);
+      int gi = x0 - 1 + sx, gj = y0 - 1 + sy;
+      const bool ok = map_nb(gi, gj, ng, ny, P.bc);
+      const long long cell = ok ? (long long)gj * ng + gi : 0;
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-          cp_async16(&Y[a][sy][APX + 2 * k2], y + a * (long long)n + cell, ok);
-          if constexpr (!F32) cp_async16(&V[a][sy][APX + 2 * k2], in + a * (long long)n + cell, ok);
-          cp_async16(&S[a][sy][APX + 2 * k2], s + a * (long long)n + cell, ok);
+      for (int a = 0; a < 3; a++) {
+        cp_async8(&Y[a][sy][sx], y + a * (long long)n + cell, ok);
+        if constexpr (F32) {
+          FPlane* Fv = reinterpret_cast<FPlane*>(B + foff);
+          cp_async4(&Fv[a][sy][sx], in + a * (long long)n + cell, ok);
+        } else {
+          cp_async8(&V[a][sy][sx], in + a * (long long)n + cell, ok);
         }
-      }
-      if constexpr (F32) {   // the FP32 input: TX/4 16-byte chunks per row
-        for (int q = tid; q < (TY + 2) * (TX / 4); q += AP_NT) {
-          const int sy = q / (TX / 4), k4 = q - sy * (TX / 4);
-          int gi = x0 + 4 * k4, gj = y0 - 1 + sy;
-          const bool ok = map_nb(gi, gj, ng, ny, P.bc);
-          const long long cell = ok ? (long long)gj * ng + gi : 0;
-#pragma unroll
-          for (int a = 0; a < 3; a++) cp_async16(&Fv[a][sy][APXF + 4 * k4], in + a * (long long)n + cell, ok);
-        }
-      }
-      // halo columns: one cell each side of every staged row
-      for (int q = tid; q < (TY + 2) * 2; q += AP_NT) {
-        const int sy = q >> 1, side = q & 1;
-        int gi = side ? x0 + TX : x0 - 1, gj = y0 - 1 + sy;
-        const bool ok = map_nb(gi, gj, ng, ny, P.bc);
-        const long long cell = ok ? (long long)gj * ng + gi : 0;
-        const int sx = side ? APX + TX : APX - 1, sxf = side ? APXF + TX : APXF - 1;
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-          cp_async8(&Y[a][sy][sx], y + a * (long long)n + cell, ok);
-          if constexpr (F32) cp_async4(&Fv[a][sy][sxf], in + a * (long long)n + cell, ok);
-          else cp_async8(&V[a][sy][sx], in + a * (long long)n + cell, ok);
-          cp_async8(&S[a][sy][sx], s + a * (long long)n + cell, ok);
-        }
-      }
-    } else {
-      // per-cell copies (a tile that overhangs the grid, or an odd grid)
-      for (int q = tid; q < AP_SLOTS; q += AP_NT) {
-        int sx, sy;
-        ap_slot(q, sx, sy);
-        int gi = x0 - 1 + sx, gj = y0 - 1 + sy;
-        const bool ok = map_nb(gi, gj, ng, ny, P.bc);
-        const long long cell = ok ? (long long)gj * ng + gi : 0;
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-          cp_async8(&Y[a][sy][sx + APX - 1], y + a * (long long)n + cell, ok);
-          if constexpr (F32) cp_async4(&Fv[a][sy][sx + APXF - 1], in + a * (long long)n + cell, ok);
-          else cp_async8(&V[a][sy][sx + APX - 1], in + a * (long long)n + cell, ok);
-          cp_async8(&S[a][sy][sx + APX - 1], s + a * (long long)n + cell, ok);
-        }
+        cp_async8(&S[a][sy][sx], s + a * (long long)n + cell, ok);
       }
     }
     if (P.jv_full) {
@@ -524,16 +467,14 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const V
       ap_slot(q, sx, sy);
       int ii = x0 - 1 + sx, jj = y0 - 1 + sy;
       const bool ok = map_nb(ii, jj, ng, ny, P.bc);
-      const int px = sx + APX - 1;
       if constexpr (F32) {
         const FPlane* Fv = reinterpret_cast<const FPlane*>(B + foff);
-        const int pxf = sx + APXF - 1;
 #pragma unroll
         for (int a = 0; a < 3; a++)
-          V[a][sy][px] = ok ? 1.0 * ((ain * (double)Fv[a][sy][pxf]) / S[a][sy][px]) : 0.0;
+          V[a][sy][sx] = ok ? 1.0 * ((ain * (double)Fv[a][sy][sx]) / S[a][sy][sx]) : 0.0;
       } else {
 #pragma unroll
-        for (int a = 0; a < 3; a++) V[a][sy][px] = ok ? 1.0 * ((ain * V[a][sy][px]) / S[a][sy][px]) : 0.0;
+        for (int a = 0; a < 3; a++) V[a][sy][sx] = ok ? 1.0 * ((ain * V[a][sy][sx]) / S[a][sy][sx]) : 0.0;
       }
     }
     __syncthreads();
@@ -541,7 +482,7 @@ __global__ void __launch_bounds__(AP_NT, 3) k_arnoldi_pipe(DevProblem P, const V
       double Pi[9];
       load_pinv(pinv, n, cell, Pi);   // first use after the stencil arithmetic below
       const double* C = B + 9 * AP_PLANE;
-      const int sx = tx + APX, sy = ty + 1;
+      const int sx = tx + 1, sy = ty + 1;
       double m[3], vv[3], ss[3];
 #pragma unroll
       for (int a = 0; a < 3; a++) {
