@@ -835,10 +835,13 @@ static int demag_autotune(llg_ctx* c, DemagPlan* d, cx_t<R>* S, const R* txx, co
     }
   if (tune_cols) {
     tbest = 1e30f;
+    // components in turn (cy = 1) only where no concurrent shape fits: it
+    // timed well alone but ran slower in the stream (1024-point FP64 columns)
+    const bool any3 = cols_ok<R>(d, 8, false) || cols_ok<R>(d, 16, false);
     for (int cy = 3; cy >= 1; cy -= 2)
     for (int ept = 8; ept <= 16; ept *= 2)
       for (int st = 0; st <= 1; st++) {
-        if (!cols_ok<R>(d, ept, st != 0, cy)) continue;
+        if ((cy == 1 && any3) || !cols_ok<R>(d, ept, st != 0, cy)) continue;
         LaunchCfg k;
         k.ept = ept;
         k.stage = st != 0;
