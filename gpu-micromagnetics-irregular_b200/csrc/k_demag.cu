@@ -776,8 +776,8 @@ static int set_smem_all(DemagPlan* d) {
   return 0;
 }
 
-// ── autotuner: time every valid launch shape of the row pair (forward +
-// inverse) and of the column kernel on this plan's buffers, keep the fastest.
+// ── autotuner: time every valid pair of row-transform and column launch
+// shapes as the three-kernel chain on this plan's buffers, keep the fastest.
 // All shapes compute bitwise-identical results (same butterflies, same
 // operation order per element), so tuning never changes numerics.  Results
 // are cached per (precision, transform size, grid) for later plans.
@@ -808,48 +808,65 @@ static int demag_autotune(llg_ctx* c, DemagPlan* d, cx_t<R>* S, const R* txx, co
   cudaEvent_t e0, e1;
   LLG_CUDA_TRY(cudaEventCreate(&e0));
   LLG_CUDA_TRY(cudaEventCreate(&e1));
-  auto timed = [&](auto&& launch) -> float {
-    if (launch()) return 1e30f;
-    cudaEventRecord(e0, s);
-    for (int k = 0; k < 3; k++)
-      if (launch()) return 1e30f;
-    cudaEventRecord(e1, s);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    return ms;
-  };
   LaunchCfg best_r = d->rows[kp<R>()], best_c = d->cols[kp<R>()];
-  float tbest = 1e30f;
+  std::vector<LaunchCfg> rcand, ccand;
   for (int nb = 1; nb <= 2; nb++)
     for (int ept = 8; ept <= 16; ept *= 2) {
       if (!rows_ok<R>(d, nb, ept)) continue;
       LaunchCfg k;
       k.nb = nb;
       k.ept = ept;
-      const float t = timed([&]() {
-        int rc = launch_rows_fwd<R>(d, s, c->d_hd, cs, d->ng, d->ny, nullptr, S, d->ny, 3, k);
-        return rc ? rc : launch_rows_inv<R>(d, s, S, c->d_pm, cs, k);
-      });
-      if (t < tbest) { tbest = t; best_r = k; }
+      rcand.push_back(k);
     }
   if (tune_cols) {
-    tbest = 1e30f;
     // components in turn (cy = 1) only where no concurrent shape fits: it
-    // timed well alone but ran slower in the stream (1024-point FP64 columns)
+    // ran slower in the stream for 1024-point FP64 columns
     const bool any3 = cols_ok<R>(d, 8, false) || cols_ok<R>(d, 16, false);
     for (int cy = 3; cy >= 1; cy -= 2)
-    for (int ept = 8; ept <= 16; ept *= 2)
-      for (int st = 0; st <= 1; st++) {
-        if ((cy == 1 && any3) || !cols_ok<R>(d, ept, st != 0, cy)) continue;
-        LaunchCfg k;
-        k.ept = ept;
-        k.stage = st != 0;
-        k.cy = cy;
-        const float t = timed([&]() { return launch_cols_conv<R>(d, s, S, txx, tyy, tzz, txy, k); });
-        if (t < tbest) { tbest = t; best_c = k; }
-      }
+      for (int ept = 8; ept <= 16; ept *= 2)
+        for (int st = 0; st <= 1; st++) {
+          if ((cy == 1 && any3) || !cols_ok<R>(d, ept, st != 0, cy)) continue;
+          LaunchCfg k;
+          k.ept = ept;
+          k.stage = st != 0;
+          k.cy = cy;
+          ccand.push_back(k);
+        }
+  } else {
+    ccand.push_back(best_c);   // (the tensor-core column stage, or the fixed shape)
   }
+  // Every (rows, columns) pair is timed as the integrator issues it: the
+  // three kernels back to back under programmatic dependent launch, so that
+  // neighbours which cannot share an SM, or slow each other in the stream,
+  // are seen (isolated per-kernel times picked shapes that ran slower there).
+  auto chain = [&](const LaunchCfg& kr, const LaunchCfg& kc) -> int {
+    int rc = launch_rows_fwd<R>(d, s, c->d_hd, cs, d->ng, d->ny, nullptr, S, d->ny, 3, kr);
+    if (!rc) {
+      if (!tune_cols && d->tc && sizeof(R) == 4) rc = demag_tc_cols(c, d->tc, reinterpret_cast<float2*>(S));
+      else rc = launch_cols_conv<R>(d, s, S, txx, tyy, tzz, txy, kc);
+    }
+    return rc ? rc : launch_rows_inv<R>(d, s, S, c->d_pm, cs, kr);
+  };
+  float tbest = 1e30f;
+  for (const LaunchCfg& kr : rcand)
+    for (const LaunchCfg& kc : ccand) {
+      if (chain(kr, kc)) continue;   // warm-up (plain launches)
+      cudaEventRecord(e0, s);
+      int bad = 0;
+      {
+        PdlScope pdl(true);
+        for (int k = 0; k < 3 && !bad; k++) bad = chain(kr, kc);
+      }
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (!bad && ms < tbest) {
+        tbest = ms;
+        best_r = kr;
+        best_c = kc;
+      }
+    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   LLG_CUDA_TRY(cudaGetLastError());
