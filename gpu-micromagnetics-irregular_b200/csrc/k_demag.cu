@@ -131,18 +131,69 @@ __device__ __forceinline__ void col_fft(cx_t<R>* buf, const FftPlanT<R>& pl) {
 }
 
 // ── K2: column transform + tensor multiply + inverse column transform ─────
-// CTA = one x-frequency column; threadIdx.y = component when blockDim.y = 3,
-// or one row of threads transforms the three components in turn when
-// blockDim.y = 1 (long FP64 columns, whose registers allow only a third of
-// the threads).  The three spectrum columns and (STAGE) this column's tensor
-// spectra are fetched with asynchronous copies (cp.async) at entry, so the
-// tensor read overlaps the forward transform instead of stalling the
-// multiply.
+// CTA = one x-frequency column.  The three spectrum columns and (STAGE) this
+// column's tensor spectra are fetched with asynchronous copies (cp.async) at
+// entry, so the tensor read overlaps the forward transform instead of
+// stalling the multiply.
 template <typename R, int EPT, bool STAGE, int FIX>
-__global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
+__device__ __forceinline__ void cols_conv_concurrent(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
                             const R* __restrict__ txx, const R* __restrict__ tyy, const R* __restrict__ tzz,
                             const cx_t<R>* __restrict__ txy) {
-  pdl_entry();
+  using C = cx_t<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int kx = blockIdx.x;
+  const int n = FIX > 0 ? FIX : pl.n;
+  const int c = threadIdx.y;
+  C* buf = sm + c * n;
+  C* col = S + ((long long)c * Hx + kx) * ld;
+  const int T = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const long long tb = (long long)kx * n;
+  R* sxx = reinterpret_cast<R*>(sm + 3 * n);
+  R* syy = sxx + n;
+  R* szz = syy + n;
+  C* sxy = reinterpret_cast<C*>(szz + n);
+  for (int yy = threadIdx.x; yy < n; yy += blockDim.x) {
+    if (yy < nrows) cp_async<sizeof(C)>(&buf[yy], &col[yy]);
+    else buf[yy] = mk<R>(R(0), R(0));
+  }
+  cp_async_commit();
+  if (STAGE) {
+    constexpr int PR = 16 / sizeof(R), PC = 16 / sizeof(C);  // elements per 16-byte copy
+    const int hr = n / PR, hc = n / PC;
+    for (int e = tid; e < 3 * hr + hc; e += T) {
+      if (e < hr) cp_async<16>(&sxx[PR * e], &txx[tb + PR * e]);
+      else if (e < 2 * hr) cp_async<16>(&syy[PR * (e - hr)], &tyy[tb + PR * (e - hr)]);
+      else if (e < 3 * hr) cp_async<16>(&szz[PR * (e - 2 * hr)], &tzz[tb + PR * (e - 2 * hr)]);
+      else cp_async<16>(&sxy[PC * (e - 3 * hr)], &txy[tb + PC * (e - 3 * hr)]);
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncthreads();
+  col_fft<R, -1, EPT, FIX>(buf, pl);
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int ky = tid; ky < n; ky += T) {
+    const C mx = sm[ky], my = sm[n + ky], mz = sm[2 * n + ky];
+    R a, b, d;
+    C xy;
+    if (STAGE) { a = sxx[ky]; b = syy[ky]; d = szz[ky]; xy = sxy[ky]; }
+    else { a = __ldg(&txx[tb + ky]); b = __ldg(&tyy[tb + ky]); d = __ldg(&tzz[tb + ky]); xy = __ldg(&txy[tb + ky]); }
+    const C hxy = cmul<R>(xy, my), hyx = cmul<R>(xy, mx);
+    sm[ky] = mk<R>(a * mx.x + hxy.x, a * mx.y + hxy.y);
+    sm[n + ky] = mk<R>(hyx.x + b * my.x, hyx.y + b * my.y);
+    sm[2 * n + ky] = mk<R>(d * mz.x, d * mz.y);
+  }
+  __syncthreads();
+  col_fft<R, +1, EPT, FIX>(buf, pl);
+  for (int yy = threadIdx.x; yy < nrows; yy += blockDim.x) col[yy] = buf[yy];
+}
+
+template <typename R, int EPT, bool STAGE, int FIX>
+__device__ __forceinline__ void cols_conv_in_turn(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
+                            const R* __restrict__ txx, const R* __restrict__ tyy, const R* __restrict__ tzz,
+                            const cx_t<R>* __restrict__ txy) {
   using C = cx_t<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
@@ -197,6 +248,19 @@ __global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int
     C* col = S + ((long long)c * Hx + kx) * ld;
     for (int yy = threadIdx.x; yy < nrows; yy += blockDim.x) col[yy] = buf[yy];
   }
+}
+
+// The kernel: CY = 3 transforms the three components concurrently (one CTA
+// row each), CY = 1 in turn with one row of threads (long FP64 columns,
+// whose registers allow only a third of the threads).  The two bodies are
+// separate so that the common form keeps its straight-line code.
+template <typename R, int EPT, bool STAGE, int FIX, int CY>
+__global__ void k_cols_conv(FftPlanT<R> pl, cx_t<R>* __restrict__ S, int ld, int nrows, int Hx,
+                            const R* __restrict__ txx, const R* __restrict__ tyy, const R* __restrict__ tzz,
+                            const cx_t<R>* __restrict__ txy) {
+  pdl_entry();
+  if constexpr (CY == 3) cols_conv_concurrent<R, EPT, STAGE, FIX>(pl, S, ld, nrows, Hx, txx, tyy, tzz, txy);
+  else cols_conv_in_turn<R, EPT, STAGE, FIX>(pl, S, ld, nrows, Hx, txx, tyy, tzz, txy);
 }
 
 // forward column transform only (tensor spectra at init, FP64)
@@ -638,9 +702,9 @@ static RowsInvFn<R> rows_inv_fn_t(int fix) {
   LLG_FIX_SWITCH(fix, K_OF)
 #undef K_OF
 }
-template <typename R, int EPT, bool ST>
+template <typename R, int EPT, bool ST, int CY>
 static ColsFn<R> cols_fn_t(int fix) {
-#define K_OF(F) k_cols_conv<R, EPT, ST, F>
+#define K_OF(F) k_cols_conv<R, EPT, ST, F, CY>
   LLG_FIX_SWITCH(fix, K_OF)
 #undef K_OF
 }
@@ -661,10 +725,14 @@ static RowsInvFn<R> rows_inv_fn(int fix, int nb, int ept) {
   if (nb == 1) return ept == 8 ? rows_inv_fn_t<R, 1, 8>(fix) : rows_inv_fn_t<R, 1, 16>(fix);
   return ept == 8 ? rows_inv_fn_t<R, 2, 8>(fix) : rows_inv_fn_t<R, 2, 16>(fix);
 }
+template <typename R, int CY>
+static ColsFn<R> cols_fn_cy(int fix, int ept, bool stage) {
+  if (ept == 8) return stage ? cols_fn_t<R, 8, true, CY>(fix) : cols_fn_t<R, 8, false, CY>(fix);
+  return stage ? cols_fn_t<R, 16, true, CY>(fix) : cols_fn_t<R, 16, false, CY>(fix);
+}
 template <typename R>
-static ColsFn<R> cols_fn(int fix, int ept, bool stage) {
-  if (ept == 8) return stage ? cols_fn_t<R, 8, true>(fix) : cols_fn_t<R, 8, false>(fix);
-  return stage ? cols_fn_t<R, 16, true>(fix) : cols_fn_t<R, 16, false>(fix);
+static ColsFn<R> cols_fn(int fix, int ept, bool stage, int cy = 3) {
+  return cy == 3 ? cols_fn_cy<R, 3>(fix, ept, stage) : cols_fn_cy<R, 1>(fix, ept, stage);
 }
 static ColsFwdFn cols_fwd_fn(int fix, int ept) { return ept == 8 ? cols_fwd_fn_t<8>(fix) : cols_fwd_fn_t<16>(fix); }
 
@@ -707,7 +775,8 @@ static int launch_cols_conv(const DemagPlan* d, cudaStream_t s, cx_t<R>* S, cons
   const dim3 b(d->fy.tx_for(k.ept), k.cy);
   const size_t base = sizeof(cx_t<R>) * 3 * (size_t)d->py;
   const size_t sm = k.stage ? base + (sizeof(R) * 3 + sizeof(cx_t<R>)) * (size_t)d->py : base;
-  klaunch(cols_fn<R>(d->fy.fix, k.ept, k.stage), d->hx, b, sm, s, pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz, txy);
+  klaunch(cols_fn<R>(d->fy.fix, k.ept, k.stage, k.cy), d->hx, b, sm, s, pl, S, d->ny, d->ny, d->hx, txx, tyy, tzz,
+          txy);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -736,7 +805,7 @@ static size_t cols_smem(const DemagPlan* d, bool stage) {
 template <typename R>
 static bool cols_ok(const DemagPlan* d, int ept, bool stage, int cy = 3) {
   const int threads = d->fy.tx_for(ept) * cy;
-  if (threads > 1024 || threads > max_threads((const void*)cols_fn<R>(d->fy.fix, ept, stage))) return false;
+  if (threads > 1024 || threads > max_threads((const void*)cols_fn<R>(d->fy.fix, ept, stage, cy))) return false;
   if (!stage) return cols_smem<R>(d, false) <= 227 * 1024;
   return d->py % (int)(16 / sizeof(R)) == 0 && cols_smem<R>(d, true) <= 200 * 1024;
 }
@@ -756,8 +825,10 @@ static int set_smem_all(DemagPlan* d) {
     }
   const size_t c0 = cols_smem<R>(d, false), c1 = cols_smem<R>(d, true);
   for (int ept = 8; ept <= 16; ept *= 2) {
-    if ((rc = set_smem((const void*)cols_fn<R>(d->fy.fix, ept, false), c0))) return rc;
-    if (c1 <= 200 * 1024 && (rc = set_smem((const void*)cols_fn<R>(d->fy.fix, ept, true), c1))) return rc;
+    for (int cy = 3; cy >= 1; cy -= 2) {
+      if ((rc = set_smem((const void*)cols_fn<R>(d->fy.fix, ept, false, cy), c0))) return rc;
+      if (c1 <= 200 * 1024 && (rc = set_smem((const void*)cols_fn<R>(d->fy.fix, ept, true, cy), c1))) return rc;
+    }
   }
   // default shapes (before tuning): one transform per CTA, fewest elements
   // per thread that the kernel's registers allow
