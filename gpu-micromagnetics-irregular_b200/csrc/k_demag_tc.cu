@@ -52,6 +52,7 @@ namespace {
 constexpr int P = 1024;
 constexpr int NCOL = 4;                           // x-frequency columns per group
 constexpr int NWARP = 12, NT = NWARP * 32;
+constexpr int kTcWpr = 2;                         // warps per (component, lane quarter) role
 constexpr int LBO_K = 128;                        // K-major: K-adjacent core matrices
 constexpr int SBO_MN = 128, LBO_MN = 16 * 128 + 16;  // MN-major, M = 128 (16 B pad per K group)
 constexpr int AMAT = 8 * LBO_MN;                  // one 128 x 64 FP16 operand, either layout
@@ -103,10 +104,18 @@ __device__ __forceinline__ void acc_ld16(uint32_t tl, uint32_t col, float (&v)[1
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = fmaf(lo[i], LO_UNSCALE, v[i]);
 }
+// the same for 8 columns
+__device__ __forceinline__ void acc_ld8(uint32_t tl, uint32_t col, float (&v)[8]) {
+  float lo[8];
+  tmem_ld8x2(tl + col, tl + col + 64, v, lo);
+#pragma unroll
+  for (int i = 0; i < 8; i++) v[i] = fmaf(lo[i], LO_UNSCALE, v[i]);
+}
 
-template <int D1>
-__global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
+template <int D1, int WPR>
+__global__ void __launch_bounds__(NT * WPR, 1) k_cols_tc(TcArgs a) {
   pdl_entry();
+  constexpr int NTW = NT * WPR;
   constexpr int K1 = 2 * D1;
   constexpr int oF1h = 0, oF1l = 128 * K1, oF2h = 256 * K1, oF2l = oF2h + 8192, oG1h = oF2h + 16384,
                 oG1l = oG1h + 256 * D1;
@@ -121,21 +130,23 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
   __shared__ float2 s_tw[32][32]; // w1024^(k l) at [k][l]: lane l reads [k][l], no bank conflicts
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int c = warp >> 2, q = warp & 3;
+  // WPR warps share each (component, TMEM lane quarter) role, each taking
+  // its share of the accumulator column blocks in every epilogue
+  const int q = warp & 3, role = warp >> 2, c = role / WPR, h = role - c * WPR;
   // Two teams run the stage sequence independently: warps 0-7 the coupled x
   // and y components, warps 8-11 the z component.  Each has its own named
   // barrier, MMA-issuing thread and completion mbarrier, so one team's
   // epilogue (CUDA cores, TMEM read-back) overlaps the other's MMAs and
   // neither waits at the other's barriers.
   const int team = (c < 2) ? 0 : 1;
-  const int team_lead = team ? 256 : 0, team_threads = team ? 128 : 256;
+  const int team_lead = team ? 256 * WPR : 0, team_threads = team ? 128 * WPR : 256 * WPR;
   const int c_lo = team ? 2 : 0, c_hi = team ? 3 : 2;
   auto team_sync = [&]() {
     asm volatile("bar.sync %0, %1;\n" ::"r"(1 + team), "r"(team_threads) : "memory");
   };
 
-  for (int i = tid; i < BB / 16; i += NT) reinterpret_cast<uint4*>(sm)[i] = a.bmat[i];
-  for (int i = tid; i < 32 * 32; i += NT) s_tw[i >> 5][i & 31] = a.tw[((i >> 5) * (i & 31)) & (P - 1)];
+  for (int i = tid; i < BB / 16; i += NTW) reinterpret_cast<uint4*>(sm)[i] = a.bmat[i];
+  for (int i = tid; i < 32 * 32; i += NTW) s_tw[i >> 5][i & 31] = a.tw[((i >> 5) * (i & 31)) & (P - 1)];
   if (warp == 0) tmem_alloc(&tmem_slot, TMEM_COLS);
   if (tid == 0) {
     mbar_init(&mbar[0], 1);
@@ -228,11 +239,12 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       int e = 0;
       if (mx > 0.f) frexpf(mx, &e);   // mx < 2^e
       e = max(e, -127);               // 2^-e stays a finite float (subnormal-only columns)
-      if (lane == 0) s_e[c][q] = e;
+      if (lane == 0 && h == 0) s_e[c][q] = e;
       const float sc = ldexpf(1.f, -e);   // v * 2^-e: exact, or rounded as ldexpf rounds
       const int r = 32 * q + lane;
 #pragma unroll
       for (int j = 0; j < K1 / 8; j++) {
+        if (j / (K1 / 8 / WPR) != h) continue;   // this warp's share of the K chunks
         H8 hh, ll;
 #pragma unroll
         for (int t = 0; t < 4; t++) split_h2(v[4 * j + t].x * sc, v[4 * j + t].y * sc, hh.h2[t], ll.h2[t]);
@@ -244,7 +256,7 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
     if (!(good = run_stage(0))) break;
     // ── F1 epilogue: twiddle w1024^(n2 k1), 2^-5 -> F2 operand (MN-major) ──
 #pragma unroll 1
-    for (int j = 0; j < 4; j++) {
+    for (int j = h * (4 / WPR); j < (h + 1) * (4 / WPR); j++) {
       float v[16];
       acc_ld16(tl, 128 * c + 16 * j, v);
       H8 hr, lr, hi, li;
@@ -290,42 +302,67 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
           x[i] = (colok && c < 2) ? __ldg(&a.txy[e]) : make_float2(0.f, 0.f);
         }
       };
-      load_t(0, tn, tq);
+      // (with two warps per role the other warps hide the tensor loads, and the
+      // next block's entries would not fit in the register budget)
+      constexpr bool AHEAD = WPR == 1;
+      const int j0 = h * (4 / WPR), j1 = j0 + 4 / WPR;
+      if constexpr (AHEAD) load_t(j0, tn, tq);
 #pragma unroll 1
-      for (int j = 0; j < 4; j++) {
+      for (int j = j0; j < j1; j++) {
         float nn[8];
         float2 nq[8];
-        if (j < 3) load_t(j + 1, nn, nq);
-        float X0[16], X1[16];
-        if (c < 2) {
-          acc_ld16(tl, 16 * j, X0);
-          acc_ld16(tl, 128 + 16 * j, X1);
+        if constexpr (AHEAD) {
+          if (j + 1 < j1) load_t(j + 1, nn, nq);
         } else {
-          acc_ld16(tl, 256 + 16 * j, X0);
+          load_t(j, tn, tq);
         }
+        // the accumulator block: all 16 columns at once, or (two warps per
+        // role, tighter register budget) 8 columns per half
+        constexpr int XW = (WPR == 1) ? 16 : 8;
+        float X0[XW], X1[XW];
+        auto ld_x = [&](int col0) {
+          if constexpr (XW == 16) {
+            if (c < 2) {
+              acc_ld16(tl, col0, X0);
+              acc_ld16(tl, 128 + col0, X1);
+            } else {
+              acc_ld16(tl, 256 + col0, X0);
+            }
+          } else {
+            if (c < 2) {
+              acc_ld8(tl, col0, X0);
+              acc_ld8(tl, 128 + col0, X1);
+            } else {
+              acc_ld8(tl, 256 + col0, X0);
+            }
+          }
+        };
+        if constexpr (XW == 16) ld_x(16 * j);
 #pragma unroll
         for (int half = 0; half < 2; half++) {
+          if constexpr (XW == 8) ld_x(16 * j + 8 * half);
           H8 hh, ll;
 #pragma unroll
           for (int t = 0; t < 4; t++) {
             const int i = 4 * half + t;
+            const int xi2 = (XW == 16) ? 2 * i : 2 * t;   // this frequency's (re, im) in X
             float hr = 0.f, hm = 0.f;
             if (colok) {
               const float n = tn[i];
               const float2 nxy = tq[i];
               if (c == 0) {
-                const float xr = X0[2 * i] * fx, xi = X0[2 * i + 1] * fx;
-                const float yr = X1[2 * i] * fy, yi = X1[2 * i + 1] * fy;
+                const float xr = X0[xi2] * fx, xi = X0[xi2 + 1] * fx;
+                const float yr = X1[xi2] * fy, yi = X1[xi2 + 1] * fy;
                 hr = n * xr + (nxy.x * yr - nxy.y * yi);
                 hm = n * xi + (nxy.x * yi + nxy.y * yr);
               } else if (c == 1) {
-                const float xr = X0[2 * i] * fx, xi = X0[2 * i + 1] * fx;
-                const float yr = X1[2 * i] * fy, yi = X1[2 * i + 1] * fy;
+                const float xr = X0[xi2] * fx, xi = X0[xi2 + 1] * fx;
+                const float yr = X1[xi2] * fy, yi = X1[xi2 + 1] * fy;
                 hr = (nxy.x * xr - nxy.y * xi) + n * yr;
                 hm = (nxy.x * xi + nxy.y * xr) + n * yi;
               } else {
-                hr = n * X0[2 * i];
-                hm = n * X0[2 * i + 1];
+                hr = n * X0[xi2];
+                hm = n * X0[xi2 + 1];
               }
             }
             split_h2(hr * a.s_t, -hm * a.s_t, hh.h2[t], ll.h2[t]);
@@ -334,7 +371,7 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
           *reinterpret_cast<uint4*>(Ah + o) = hh.u;
           *reinterpret_cast<uint4*>(Al + o) = ll.u;
         }
-        if (j < 3) {
+        if (AHEAD && j + 1 < j1) {
 #pragma unroll
           for (int i = 0; i < 8; i++) {
             tn[i] = nn[i];
@@ -342,12 +379,12 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
           }
         }
       }
-      if (lane == 0) s_eo[c][q] = em;
+      if (lane == 0 && h == 0) s_eo[c][q] = em;
     }
     if (!(good = run_stage(2))) break;
     // ── G2 epilogue: twiddle w1024^(n2 k1), 2^-5 -> G1 operand (MN-major) ──
 #pragma unroll 1
-    for (int j = 0; j < 4; j++) {
+    for (int j = h * (4 / WPR); j < (h + 1) * (4 / WPR); j++) {
       float v[16];
       acc_ld16(tl, 128 * c + 16 * j, v);
       H8 hr, lr, hi, li;
@@ -377,7 +414,7 @@ __global__ void __launch_bounds__(NT, 1) k_cols_tc(TcArgs a) {
       const float so = ldexpf(1.f, s_eo[c][q] + 16 - a.e_t);
       float2* dst = a.S + ((long long)c * a.hx + (colok ? kx : 0)) * a.ld;
 #pragma unroll 1
-      for (int j = 0; j < D1 / 8; j++) {
+      for (int j = h * (D1 / 8 / WPR); j < (h + 1) * (D1 / 8 / WPR); j++) {
         float v[16];
         acc_ld16(tl, 128 * c + 16 * j, v);
         if (colok) {
@@ -547,7 +584,7 @@ int demag_tc_create(llg_ctx* c, int px, int py, int hx, int ny, const float* txx
   if (mx > 0.f) frexpf(mx, &e);
   t->e_t = -e;
   t->s_t = ldexpf(1.f, t->e_t - 6);
-  const void* fn = (D1 == 16) ? (const void*)k_cols_tc<16> : (const void*)k_cols_tc<32>;
+  const void* fn = (D1 == 16) ? (const void*)k_cols_tc<16, kTcWpr> : (const void*)k_cols_tc<32, kTcWpr>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem) != cudaSuccess) {
     llg_set_error("demag_tc_create: shared-memory opt-in failed");
     return fail(LLG_ERR_CUDA);
@@ -575,8 +612,8 @@ int demag_tc_cols(llg_ctx* c, DemagTc* t, float2* Sf) {
   a.s_t = t->s_t;
   a.e_t = t->e_t;
   a.err = t->d_err;
-  if (t->D1 == 16) klaunch(k_cols_tc<16>, t->grid, NT, t->smem, c->stream, a);
-  else klaunch(k_cols_tc<32>, t->grid, NT, t->smem, c->stream, a);
+  if (t->D1 == 16) klaunch(k_cols_tc<16, kTcWpr>, t->grid, NT * kTcWpr, t->smem, c->stream, a);
+  else klaunch(k_cols_tc<32, kTcWpr>, t->grid, NT * kTcWpr, t->smem, c->stream, a);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
