@@ -770,7 +770,10 @@ def run_config2(args, world, rank, local):
     windowed open demag of strength 1, two domains (+x left, -x right) with
     0.01 jitter, rtol 1e-4.  Each form is timed over t 0 -> steps*dt from a
     fresh instance; then the mixed forms replay plain FP64's recorded steps
-    over the same window and max|dm| against FP64 is reported at the end."""
+    over the same window and max|dm| against FP64 is reported at t = 1, 5
+    and the end, beside an FP64 control whose demag strength is changed by
+    1e-9 (same steps), which measures how much the film itself amplifies a
+    perturbation."""
     import torch
     torch.cuda.set_device(local)
     n_ng, n_ny = 1536, 512
@@ -781,8 +784,11 @@ def run_config2(args, world, rank, local):
     t_end = args.steps * args.dt
     kmax = int(round(t_end / 0.1))
 
-    def run(prec, krylov, record=False, replay=None, timed=False):
-        p = llg.default_params(n_ng, n_ny, demag_mode=llg.DEMAG_OPEN, demag_strength=1.0, windowed=1,
+    t_marks = [t for t in (1.0, 5.0) if t < t_end] + [t_end]
+    k_marks = {int(round(t / 0.1)): t for t in t_marks}
+
+    def run(prec, krylov, record=False, replay=None, timed=False, strength=1.0):
+        p = llg.default_params(n_ng, n_ny, demag_mode=llg.DEMAG_OPEN, demag_strength=strength, windowed=1,
                                norm_kind=llg.NORM_REG, bc=llg.BC_FREE, demag_precision=prec)
         ctx = llg.Context(p)
         ctx.set_window(geo["w"], geo["msk3"], geo["nsk3"])
@@ -793,14 +799,17 @@ def run_config2(args, world, rank, local):
         if replay is not None:
             ctx.replay_steps(*replay)
         yout = torch.zeros_like(y0)
+        marks = {}
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for k in range(1, kmax + 1):
             ctx.integrate(0.1 * k, yout)
+            if not timed and k in k_marks:
+                marks[k_marks[k]] = yout.cpu().numpy()   # (accuracy runs only: the copy is not timed)
         e1.record()
         torch.cuda.synchronize()
-        out = {"y": yout.cpu().numpy(), "ms": e0.elapsed_time(e1), "stats": ctx.stats()}
+        out = {"y": yout.cpu().numpy(), "ms": e0.elapsed_time(e1), "stats": ctx.stats(), "marks": marks}
         if record:
             out["steps"] = ctx.recorded_steps()
         ctx.close()
@@ -810,12 +819,16 @@ def run_config2(args, world, rank, local):
     res = {}
     for name, prec, kr in (("plain", llg.DEMAG_FP64, llg.KRYLOV_FP64), ("mixed", llg.DEMAG_MIXED, llg.KRYLOV_FP64),
                            ("mixed32", llg.DEMAG_MIXED, llg.KRYLOV_FP32)):
-        r_ = run(prec, kr, record=(name == "plain"))
+        r_ = run(prec, kr, record=(name == "plain"), timed=True)
         res[name] = r_
+    # accuracy: FP64 recorded again with its marks (the timed runs copy nothing out)
+    ref = run(llg.DEMAG_FP64, llg.KRYLOV_FP64, replay=res["plain"]["steps"])
     acc = {}
-    for name, prec, kr in (("mixed", llg.DEMAG_MIXED, llg.KRYLOV_FP64), ("mixed32", llg.DEMAG_MIXED, llg.KRYLOV_FP32)):
-        r_ = run(prec, kr, replay=res["plain"]["steps"])
-        acc[name] = float(np.abs(r_["y"] - res["plain"]["y"]).max())
+    for name, prec, kr, st in (("mixed", llg.DEMAG_MIXED, llg.KRYLOV_FP64, 1.0),
+                               ("mixed32", llg.DEMAG_MIXED, llg.KRYLOV_FP32, 1.0),
+                               ("control_fp64_strength_1e-9", llg.DEMAG_FP64, llg.KRYLOV_FP64, 1.0 + 1e-9)):
+        r_ = run(prec, kr, replay=res["plain"]["steps"], strength=st)
+        acc[name] = {str(t): float(np.abs(r_["marks"][t] - ref["marks"][t]).max()) for t in t_marks}
     val = {k: t_end / (v["ms"] / 1000.0) for k, v in res.items()}
     line = {
         "metric": "sim-time/wall-s @1536x512 polycrystal, mixed vs plain FP64", "value": val["mixed32"],
