@@ -343,7 +343,11 @@ struct Integrator {
                  : fused_psolve_scale_dot(c, rhs, ewt, V[0], SLOT_A, nullptr, SLOT_V0SC)))
       return LS_CONV_FAIL;
     ka[0] = c->d_scal + SLOT_V0SC;
-    int queued = (lmax >= 2) ? 2 : 1;
+    // one Arnoldi iteration before the first read-back: enqueuing two saved
+    // a read-back when GMRES needs a second iteration but wasted an operator
+    // step, a Gram-Schmidt pass and their dots whenever one sufficed, which
+    // cost more (measured at 1536x512: 397 -> 386 us per BDF step)
+    int queued = 1;
     for (int l = 0; l < queued; l++) enqueue_iter(l);
     ok(fetch_range(c, 0, slot_ss(queued - 1) + 1));
     if (err) return LS_CONV_FAIL;
