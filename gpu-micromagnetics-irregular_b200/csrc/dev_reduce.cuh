@@ -110,5 +110,18 @@ __device__ __forceinline__ bool finalize(double* partials, int nb, unsigned int*
   return true;
 }
 
+// Called by every thread of a reduction's last block once its results are
+// stored: warp 0 carries out the read-back request p (Pub).  __syncwarp
+// orders thread 0's stores of the results before the other lanes' loads; the
+// loads are volatile so that they come from L2, where the earlier kernels'
+// values are.
+__device__ __forceinline__ void publish_carried(const Pub& p) {
+  if (p.seq == 0 || threadIdx.x >= 32) return;
+  __syncwarp();
+  for (int i = p.lo + (int)threadIdx.x; i < p.hi; i += 32) p.mail[i] = ((const volatile double*)p.scal)[i];
+  __threadfence_system();
+  __syncwarp();
+  if (threadIdx.x == 0) *reinterpret_cast<volatile unsigned long long*>(p.mail + NSCAL) = p.seq;
+}
 
 }  // namespace

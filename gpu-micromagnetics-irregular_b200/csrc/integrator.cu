@@ -315,7 +315,9 @@ struct Integrator {
     for (int i = k0; i < k1; i++) s.a[at + i - k0] = ka[i];
     return s;
   }
-  void enqueue_iter(int l) {
+  // pub_lo >= 0: the Gram-Schmidt update, the iteration's last kernel,
+  // carries the read-back of d_scal[pub_lo, slot_ss(l)] (arm_publish)
+  void enqueue_iter(int l, int pub_lo) {
     const int k = l + 1;
     const KScale ys = basis_scales(0, k, 0);   // V[k] itself: the fresh operator output, unscaled
     if (kf32) {
@@ -324,12 +326,14 @@ struct Integrator {
       float* W[MAXLL + 1];
       for (int i = 0; i <= k; i++) { Y[i] = Vf(i); W[i] = Vf(i); }
       ok(vdot_multi_dev_f(c, k + 1, Vf(k), Y, slot_it(l), &ys));
+      if (pub_lo >= 0) arm_publish(c, pub_lo, slot_ss(l) + 1);
       ok(vgs_update_dev_f(c, k, W, slot_it(l), slot_ss(l), &ys, slot_sc(l)));
     } else {
       ok(launch_arnoldi_op(c, V[l], ewt, V[k], y, gamma, 1, nullptr, ka[l]));
       const double* Y[MAXLL + 1];
       for (int i = 0; i <= k; i++) Y[i] = V[i];
       ok(vdot_multi_dev(c, k + 1, V[k], Y, slot_it(l), &ys));
+      if (pub_lo >= 0) arm_publish(c, pub_lo, slot_ss(l) + 1);
       ok(vgs_update_dev(c, k, V, slot_it(l), slot_ss(l), &ys, slot_sc(l)));
     }
     ka[k] = c->d_scal + slot_sc(l);
@@ -348,7 +352,7 @@ struct Integrator {
     // step, a Gram-Schmidt pass and their dots whenever one sufficed, which
     // cost more (measured at 1536x512: 397 -> 386 us per BDF step)
     int queued = 1;
-    for (int l = 0; l < queued; l++) enqueue_iter(l);
+    for (int l = 0; l < queued; l++) enqueue_iter(l, l == queued - 1 ? 0 : -1);
     ok(fetch_range(c, 0, slot_ss(queued - 1) + 1));
     if (err) return LS_CONV_FAIL;
     ewt_fresh = ewt_pending;
@@ -361,7 +365,7 @@ struct Integrator {
     double rot = 1.0;
     for (int l = 0; l < lmax; l++) {
       if (l >= queued) {
-        enqueue_iter(l);
+        enqueue_iter(l, slot_it(l));
         queued = l + 1;
         ok(fetch_range(c, slot_it(l), slot_ss(l) + 1));
         if (err) return LS_CONV_FAIL;
@@ -425,6 +429,7 @@ struct Integrator {
       const KScale xs = basis_scales(0, krydim, 0);
       const bool taken = converged || ls_curiter == 0;
       if (taken && fuse_update) {
+        arm_publish(c, SLOT_A, SLOT_A + 2);
         ok(kf32 ? fused_lincomb_update_f(c, krydim, yg, Xf, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A, &xs)
                 : fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A, &xs));
         ok(fetch_scalars(c, SLOT_A, 2, upd_s));
@@ -510,6 +515,7 @@ struct Integrator {
       // returns 0), apply it to the correction vector in the same pass
       const bool taken = converged || ls_curiter == 0;
       if (taken && fuse_update) {
+        arm_publish(c, SLOT_A, SLOT_A + 2);
         ok(fused_lincomb_update(c, krydim, yg, X, ewt, harvest ? rhs : nullptr, ycor_zero, acor, SLOT_A));
         ok(fetch_scalars(c, SLOT_A, 2, upd_s));
         update_done = true;
@@ -781,8 +787,9 @@ struct Integrator {
         if (update_done) {   // the GMRES solution pass already applied it
           s[0] = upd_s[0];
           s[1] = upd_s[1];
-        } else if (ok(fused_update_wrms2(c, ycor_zero, ycor, del, ewt, SLOT_A))) {
-          ok(fetch_scalars(c, SLOT_A, 2, s));
+        } else {
+          arm_publish(c, SLOT_A, SLOT_A + 2);
+          if (ok(fused_update_wrms2(c, ycor_zero, ycor, del, ewt, SLOT_A))) ok(fetch_scalars(c, SLOT_A, 2, s));
         }
         update_done = false;
         ycor_zero = false;

@@ -249,7 +249,7 @@ __global__ void k_lincomb_div(int nv, CPack c, XPackT<VT> X, const double* __res
 // ycor = 1*ycor + 1*del (ycor_in null: zero); sums (del*w)^2 and (ycor*w)^2
 __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, double* ycor, const double* __restrict__ del,
                                                      const double* __restrict__ w, long long n, double* partials,
-                                                     unsigned int* counter, double* out, const DevArgs* da) {
+                                                     unsigned int* counter, double* out, const DevArgs* da, Pub pub) {
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   double acc[2] = {0.0, 0.0};
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(RT) k_update_wrms2(const double* ycor_in, doub
     acc[1] += q * q;
   }
   block_sum<2>(acc, sm);
-  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  if (finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc)) publish_carried(pub);
 }
 
 // GMRES correction and Newton update in one pass: d = (sum_k c_k X_k) / w
@@ -279,7 +279,7 @@ template <typename VT = double>
 __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPackT<VT> X, const double* __restrict__ w,
                                                        double* del, const double* ycor_in, double* ycor, long long n,
                                                        double* partials, unsigned int* counter, double* out,
-                                                       KScale ks) {
+                                                       KScale ks, Pub pub) {
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   // scales of the X vectors (1 when stored normalised), staged once: read
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPackT<V
     }
   }
   block_sum<2>(acc, sm);
-  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  if (finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc)) publish_carried(pub);
 }
 
 // k_lincomb_update with the vector count NV fixed at compile time: the loads
@@ -334,7 +334,7 @@ template <int NV, typename VT>
 __global__ void __launch_bounds__(RT) k_lincomb_update_k(CPack c, XPackT<VT> X, const double* __restrict__ w,
                                                          double* del, const double* ycor_in, double* ycor,
                                                          long long n, double* partials, unsigned int* counter,
-                                                         double* out, KScale ks) {
+                                                         double* out, KScale ks, Pub pub) {
   pdl_entry();
   __shared__ double sm[2 * (RT / 32)];
   __shared__ double xs[NV];
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(RT) k_lincomb_update_k(CPack c, XPackT<VT> X, 
     }
   }
   block_sum<2>(acc, sm);
-  finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc);
+  if (finalize<2>(partials, gridDim.x, counter, out, 0, 1.0, acc)) publish_carried(pub);
 }
 
 // sums (x1*w)^2 and ((a x2 + b x3)*w)^2
@@ -657,8 +657,10 @@ int fused_lincomb_div_f(llg_ctx* c, int nv, const double* coef, const float* con
 int fused_update_wrms2(llg_ctx* c, bool ycor_zero, double* ycor, const double* del, const double* w, int slot,
                        const DevArgs* da) {
   LLG_COUNT(KID_REDUCE);
+  // (the device-resident form reads nothing back through the mailbox)
+  const Pub pub = da ? Pub{} : take_publish(c);
   klaunch(k_update_wrms2, red_blocks(c->neq), RT, 0, c->stream, ycor_zero ? nullptr : ycor, ycor, del, w, c->neq, c->d_red, c->d_counter,
-                                                           c->d_scal + slot, da);
+                                                           c->d_scal + slot, da, pub);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
 }
@@ -685,8 +687,9 @@ static int lincomb_update_impl(llg_ctx* c, int nv, const double* coef, const VT*
   const int nb = red_blocks(c->neq);
   const double* yin = ycor_zero ? nullptr : ycor;
   double* out = c->d_scal + slot;
+  const Pub pub = take_publish(c);
 #define LU_K(NV) klaunch(k_lincomb_update_k<NV, VT>, nb, RT, 0, c->stream, cp, xp, w, del, yin, ycor, c->neq, c->d_red, \
-                         c->d_counter, out, kk)
+                         c->d_counter, out, kk, pub)
   switch (nv) {
     case 1: LU_K(1); break;
     case 2: LU_K(2); break;
@@ -698,7 +701,7 @@ static int lincomb_update_impl(llg_ctx* c, int nv, const double* coef, const VT*
     case 8: LU_K(8); break;
     default:
       klaunch(k_lincomb_update<VT>, nb, RT, 0, c->stream, nv, cp, xp, w, del, yin, ycor, c->neq, c->d_red,
-              c->d_counter, out, kk);
+              c->d_counter, out, kk, pub);
   }
 #undef LU_K
   LLG_CUDA_TRY(cudaPeekAtLastError());

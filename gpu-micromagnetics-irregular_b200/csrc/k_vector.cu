@@ -237,7 +237,7 @@ __global__ void k_scale_cols(int q, CoefPack f, MPtrPack zn, long long n) {
 template <typename VT = double>
 __global__ void __launch_bounds__(RT) k_gs_update(int k, VPack<VT> X, const double* __restrict__ dots, VT* z,
                                                   long long n, double* partials, unsigned int* counter,
-                                                  double* out, KScale ks, double* aout) {
+                                                  double* out, KScale ks, double* aout, Pub pub) {
   pdl_entry();
   __shared__ double sm[RT / 32];
   // scales of the X vectors, staged once: read through pointers, they would be
@@ -276,6 +276,7 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, VPack<VT> X, const doub
   const bool last = finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
   // the updated vector's scale; dots[k] is its sum of squares before the update
   if (last && aout && threadIdx.x == 0) *aout = gs_scale_of(out[0], dots + k);
+  if (last) publish_carried(pub);
 }
 
 // k_gs_update with the vector count K fixed at compile time: the loads of
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, VPack<VT> X, const doub
 template <int K, typename VT>
 __global__ void __launch_bounds__(RT) k_gs_update_k(VPack<VT> X, const double* __restrict__ dots, VT* z, long long n,
                                                     double* partials, unsigned int* counter, double* out, KScale ks,
-                                                    double* aout) {
+                                                    double* aout, Pub pub) {
   pdl_entry();
   __shared__ double sm[RT / 32];
   __shared__ double xs[K];
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(RT) k_gs_update_k(VPack<VT> X, const double* _
   block_sum<1>(acc, sm);
   const bool last = finalize<1>(partials, gridDim.x, counter, out, 0, 1.0, acc);
   if (last && aout && threadIdx.x == 0) *aout = gs_scale_of(out[0], dots + K);
+  if (last) publish_carried(pub);
 }
 
 // one warp copies d_scal[lo, hi) into the mapped host mailbox, makes the
@@ -427,17 +429,40 @@ int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double
   return 0;
 }
 
+void arm_publish(llg_ctx* c, int lo, int hi) {
+  c->pub_armed = Pub{};
+  if (lo < 0 || hi > NSCAL || hi <= lo) return;   // fetch_range reports it
+  c->pub_armed = Pub{c->d_scal, c->d_mail, lo, hi, ++c->mail_seq};
+}
+
+Pub take_publish(llg_ctx* c) {
+  const Pub p = c->pub_armed;
+  c->pub_armed = Pub{};
+  if (p.seq) c->pub_carried = p;
+  return p;
+}
+
 // Read-back of d_scal[lo, hi) into h_scal: the publish kernel runs after the
 // producing kernels (stream order) and the host polls the mailbox's sequence
 // word, instead of a device-to-host copy plus a stream synchronisation (the
 // copy engine's start-up and the wake-up were most of a read-back's cost).
+// When the last launch carried a request for this range (arm_publish), its
+// last block has published and only the poll remains.
 // The poll is bounded by wall time; past it (or after a launch error) the
 // stream is synchronised, which reports any device-side failure.
 int fetch_range(llg_ctx* c, int lo, int hi) {
+  const Pub carried = c->pub_carried;
+  c->pub_carried = Pub{};
+  c->pub_armed = Pub{};
   if (lo < 0 || hi > NSCAL || hi <= lo) { llg_set_error("fetch_range: bad slots"); return LLG_ERR_ARG; }
-  const unsigned long long seq = ++c->mail_seq;
-  klaunch(k_publish, 1, 32, 0, c->stream, c->d_scal, lo, hi, c->d_mail, seq);
-  LLG_CUDA_TRY(cudaPeekAtLastError());
+  unsigned long long seq;
+  if (carried.seq && carried.lo == lo && carried.hi == hi) {
+    seq = carried.seq;
+  } else {
+    seq = ++c->mail_seq;
+    klaunch(k_publish, 1, 32, 0, c->stream, c->d_scal, lo, hi, c->d_mail, seq);
+    LLG_CUDA_TRY(cudaPeekAtLastError());
+  }
   volatile unsigned long long* flag = reinterpret_cast<volatile unsigned long long*>(c->h_mail + NSCAL);
   bool seen = false;
   const auto t0 = std::chrono::steady_clock::now();
@@ -471,7 +496,8 @@ static int vgs_update_impl(llg_ctx* c, int k, VT* const* V, int slot_dots, int s
   double* ss = c->d_scal + slot_ss;
   double* aout = slot_aout >= 0 ? c->d_scal + slot_aout : nullptr;
   const KScale kk = ks ? *ks : kz;
-#define GS_K(K) klaunch(k_gs_update_k<K, VT>, nb, RT, 0, c->stream, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout)
+  const Pub pub = take_publish(c);
+#define GS_K(K) klaunch(k_gs_update_k<K, VT>, nb, RT, 0, c->stream, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout, pub)
   switch (k) {
     case 1: GS_K(1); break;
     case 2: GS_K(2); break;
@@ -482,7 +508,8 @@ static int vgs_update_impl(llg_ctx* c, int k, VT* const* V, int slot_dots, int s
     case 7: GS_K(7); break;
     case 8: GS_K(8); break;
     default:
-      klaunch(k_gs_update<VT>, nb, RT, 0, c->stream, k, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout);
+      klaunch(k_gs_update<VT>, nb, RT, 0, c->stream, k, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout,
+              pub);
   }
 #undef GS_K
   LLG_CUDA_TRY(cudaPeekAtLastError());

@@ -83,6 +83,17 @@ struct DemagTc;     // k_demag_tc.cu
 struct Integrator;  // integrator.cu
 struct Learned;     // k_learned.cu
 
+// A read-back carried by the reduction that produces its last value: warp 0
+// of that kernel's last block copies scal[lo, hi) into the mapped mailbox and
+// then writes the sequence word, in place of a separate publish launch after
+// it (seq 0: nothing to publish).
+struct Pub {
+  const double* scal;
+  double* mail;
+  int lo, hi;
+  unsigned long long seq;
+};
+
 struct llg_ctx {
   llg_params p{};
   DevProblem dp{};
@@ -125,6 +136,8 @@ struct llg_ctx {
   double* h_mail = nullptr;     // NSCAL values + the sequence word (host view)
   double* d_mail = nullptr;     // the same memory, device view
   unsigned long long mail_seq = 0;
+  Pub pub_armed{};              // requested, not yet given to a launch
+  Pub pub_carried{};            // given to the last launch that took one
   int red_blocks_max = 0;
 
   DemagPlan* demag = nullptr;
@@ -238,6 +251,12 @@ int vwrms_diff_dev(llg_ctx* c, double a, const double* x, double b, const double
 int fetch_scalars(llg_ctx* c, int slot, int n, double* out);
 // copy d_scal[lo, hi) to c->h_scal[lo, hi) and wait (one read-back)
 int fetch_range(llg_ctx* c, int lo, int hi);
+// request the read-back of d_scal[lo, hi) from the next reduction launched
+// through a helper that carries one (vgs_update_dev[_f], fused_update_wrms2,
+// fused_lincomb_update[_f]); a fetch_range of the same range right after it
+// then only waits.  take_publish: the launch helpers' side.
+void arm_publish(llg_ctx* c, int lo, int hi);
+Pub take_publish(llg_ctx* c);
 // device-coefficient forms used by the read-back-light SPGMR
 // (aout: also write the updated vector's KScale scale there, gs_scale_of with
 // the vector's pre-update sum of squares at d_scal[slot_dots + k])
