@@ -44,8 +44,10 @@ struct Integrator {
   long long neq = 0;
   int qmax = 5, maxl = 5, classical_gs = 1, mxstep = 500;
   // LLG_KRYLOV_FP32: the basis V[0..maxl] holds floats (the same allocations);
-  // the read-back-light SPGMR then calls the float variants of its kernels
-  bool kf32 = false;
+  // the read-back-light SPGMR then calls the float variants of its kernels.
+  // kf32_req: requested; kf32: in use (a learned-preconditioner context
+  // keeps FP64 until the network is off, then switches in cv_nls)
+  bool kf32_req = false, kf32 = false;
   float* Vf(int i) const { return reinterpret_cast<float*>(V[i]); }
   double rtol = 1e-4, atol = 1e-6;
   double* zn[QMAXL + 1] = {};
@@ -814,8 +816,16 @@ struct Integrator {
   }
   int cv_nls(int nflag) {
     convfail = ((nflag == FIRST_CALL) || (nflag == PREV_ERR_FAIL)) ? CV_NO_FAILURES : CV_FAIL_OTHER;
+    if (kf32_req && !kf32 && !learned_active(c)) {
+      // the learned preconditioner is off for good: block-Jacobi continues on
+      // the FP32 basis, whose operator reads an FP32 block inverse (a fresh
+      // setup below)
+      kf32 = true;
+      c->pinv_f32 = 1;
+      c->have_setup = 0;
+    }
     const int call_setup = (nflag == PREV_CONV_FAIL) || (nflag == PREV_ERR_FAIL) || (nst == 0) ||
-                           (nst >= nstlp + MSBP) || (fabs(gamrat - 1.0) > DGMAX);
+                           (nst >= nstlp + MSBP) || (fabs(gamrat - 1.0) > DGMAX) || !c->have_setup;
     ycor_zero = true;
     const int flag = newton(call_setup);
     // (CVODE also forms y = zn0 + acor here; nothing in this integrator reads it)
@@ -1202,15 +1212,16 @@ int integrator_create(llg_ctx* c, double t0, const double* y0, const llg_solver_
   b->rtol = o->rtol;
   b->atol = o->atol;
   b->device_resident = o->device_resident ? 1 : 0;
-  b->kf32 = (o->krylov_precision == LLG_KRYLOV_FP32);
+  b->kf32_req = (o->krylov_precision == LLG_KRYLOV_FP32);
+  b->kf32 = b->kf32_req && c->p.precond_kind != LLG_PREC_LEARNED;
   if (o->krylov_precision != LLG_KRYLOV_FP64 && o->krylov_precision != LLG_KRYLOV_FP32) {
     delete b;
     llg_set_error("krylov_precision must be LLG_KRYLOV_FP64 or LLG_KRYLOV_FP32");
     return LLG_ERR_ARG;
   }
-  if (b->kf32 && (!b->classical_gs || c->p.precond_kind == LLG_PREC_LEARNED)) {
+  if (b->kf32_req && !b->classical_gs) {
     delete b;
-    llg_set_error("FP32 Krylov basis needs classical Gram-Schmidt and the block-Jacobi preconditioner");
+    llg_set_error("FP32 Krylov basis needs classical Gram-Schmidt");
     return LLG_ERR_NOTSUP;
   }
   const size_t vb = sizeof(double) * (size_t)b->neq;
@@ -1587,7 +1598,9 @@ int integrator_checkpoint_load(llg_ctx* c, const void* buf, uint64_t n) {
     q += vb;
   }
   LLG_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  c->have_setup = hd.have_setup;
+  // (a learned-preconditioner context restarts on the FP64 basis: an FP32
+  // block inverse saved after its hand-over is not used, the next step sets up)
+  c->have_setup = (c->pinv_f32 == (hd.krylov_precision == LLG_KRYLOV_FP32 ? 1 : 0)) ? hd.have_setup : 0;
   c->gamma_setup = hd.gamma_setup;
   c->nfe_demag = hd.nfe_demag;
   b->ycor_zero = false;

@@ -149,9 +149,12 @@ typedef struct llg_solver_opts {
  * Arnoldi operator, the Gram-Schmidt dots and update and the final
  * correction; every product, dot and sum is still formed in FP64, and the
  * state, the norms and the Newton update stay FP64.  Host-driven integrator
- * with classical Gram-Schmidt and block-Jacobi only (LLG_ERR_NOTSUP
- * otherwise; the device-resident form is not used with it).  No reference
- * counterpart (SUNDIALS keeps the basis in the state's precision).         */
+ * with classical Gram-Schmidt only (LLG_ERR_NOTSUP otherwise; the
+ * device-resident form is not used with it).  With LLG_PREC_LEARNED the
+ * basis stays FP64 while the network runs; once it is off for good (no
+ * weights, or the cost policy or a failed solve dropped it) the next step
+ * starts a fresh block-Jacobi setup and continues on the FP32 basis.  No
+ * reference counterpart (SUNDIALS keeps the basis in the state's precision). */
 #define LLG_KRYLOV_FP64       0
 #define LLG_KRYLOV_FP32       1
 

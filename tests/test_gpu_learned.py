@@ -163,3 +163,43 @@ def test_cost_aware_policy_judges_on_the_same_trajectory(gpu):
     assert st["kappa"] > 0.0 and st["it_learned"] > 0.0 and st["it_block_jacobi"] > 0.0
     pays = st["it_learned"] * 1.6 + (st["it_learned"] + 1.0) * st["kappa"] < st["it_block_jacobi"] * 1.6
     assert st["fell_back"] == (0 if pays else 2)
+
+
+def test_fp32_basis_takes_over_when_the_network_is_dropped(gpu):
+    """LLG_KRYLOV_FP32 with the learned preconditioner: FP64 basis while the
+    network runs, then (once the cost policy or a failed solve drops it)
+    block-Jacobi on the FP32 basis.  An untrained network is dropped; the
+    run then leaves the FP64-basis run of the same settings (the FP32 basis
+    took over) and, on a damped film (alpha 0.2, demag strength 1), stays
+    within 1e-3 of it and of block-Jacobi FP64 over t 0 -> 2 (the bound the
+    FP32-basis form meets with its own step selection)."""
+    import torch
+    ng, ny = 192, 128
+    g = llg.default_geom(ng, ny, geometry_kind=llg.GEOM_HOLE_SQUARE, hole_radius_frac_y=0.125, ic_jitter_eps=0.01)
+    geo = llg.build_geometry(g)
+    act = np.tile(geo["active"].astype(np.float64), 3)
+
+    def ctx(precond):
+        c = llg.Context(llg.default_params(ng, ny, demag_mode=llg.DEMAG_OPEN, demag_strength=1.0, alpha=0.2,
+                                           norm_kind=llg.NORM_REG, precond_kind=precond))
+        c.set_mask(act)
+        return c
+
+    theta = (np.random.default_rng(23).standard_normal(L.nparams()) * 0.02).astype(np.float32)
+    cb = ctx(llg.PREC_BLOCK_JACOBI)
+    ref, _ = _integrate(torch, cb, geo, 2.0, llg.default_solver_opts())
+    cb.close()
+    res = {}
+    for kp in (llg.KRYLOV_FP64, llg.KRYLOV_FP32):
+        c = ctx(llg.PREC_LEARNED)
+        c.learned_set_weights(theta)
+        y, st = _integrate(torch, c, geo, 2.0, llg.default_solver_opts(krylov_precision=kp))
+        res[kp] = (y, st, c.learned_status())
+        c.close()
+    (y64, s64, l64), (y32, s32, l32) = res[llg.KRYLOV_FP64], res[llg.KRYLOV_FP32]
+    d64, dref = float(np.abs(y32 - y64).max()), float(np.abs(y32 - ref).max())
+    print("FP64 basis", s64, l64, "FP32 after the network", s32, l32, "max|dm| vs FP64 basis", d64,
+          "vs block-Jacobi", dref)
+    assert l32["fell_back"] != 0 and l32["napply"] > 0
+    assert not np.array_equal(y32, y64)
+    assert np.isfinite(y32).all() and d64 <= 1e-3 and dref <= 1e-3

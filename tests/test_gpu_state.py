@@ -267,7 +267,28 @@ def test_fp32_krylov_basis_tracks_fp64_basis(gpu):
     with pytest.raises(llg.LLGError, match="LLG_ERR_NOTSUP|failed with status -105"):
         _ctx(p, geo).integrator_init(0.0, y0, llg.default_solver_opts(krylov_precision=llg.KRYLOV_FP32,
                                                                       gs_type=llg.GS_MODIFIED))
+
+
+def test_fp32_basis_with_an_inactive_learned_preconditioner_is_block_jacobi(gpu):
+    """LLG_PREC_LEARNED with LLG_KRYLOV_FP32 keeps the FP64 basis while the
+    network runs and hands over to block-Jacobi on the FP32 basis once it is
+    off.  A learned context without weights is off from the first step, so
+    its run must equal the block-Jacobi FP32-basis run bit for bit, with the
+    same counters."""
+    import torch
+    p, geo = _hole(alpha=0.2, prec=llg.DEMAG_MIXED)
     pl = llg.default_params(p.ng, p.ny, demag_mode=llg.DEMAG_OPEN, demag_strength=4.0, alpha=0.2,
-                            norm_kind=llg.NORM_REG, precond_kind=llg.PREC_LEARNED)
-    with pytest.raises(llg.LLGError):
-        _ctx(pl, geo).integrator_init(0.0, y0, llg.default_solver_opts(krylov_precision=llg.KRYLOV_FP32))
+                            norm_kind=llg.NORM_REG, demag_precision=llg.DEMAG_MIXED, precond_kind=llg.PREC_LEARNED)
+    y0 = torch.from_numpy(geo["y0"]).cuda()
+    opts = llg.default_solver_opts(krylov_precision=llg.KRYLOV_FP32)
+    out = []
+    for pp in (p, pl):
+        c = _ctx(pp, geo)
+        c.integrator_init(0.0, y0, opts)
+        out.append((_run(torch, c, 1, 10, torch.zeros_like(y0)), c.stats()))
+        c.close()
+    (ya, sa), (yb, sb) = out
+    print("block-Jacobi", sa, "learned (no weights)", sb)
+    assert np.array_equal(ya, yb)
+    for k in COUNTERS:
+        assert sa[k] == sb[k], k
