@@ -172,10 +172,13 @@ __global__ void k_rhs_resid_compact(DevProblem P, const double* __restrict__ y, 
 }
 
 // (streams at HBM speed, so it rebuilds the block from the frozen (m, h),
-// 48 B/cell, rather than reading the 72 B/cell inverse that psetup stores)
+// 48 B/cell, rather than reading the 72 B/cell FP64 inverse that psetup
+// stores; pinvf non-null: the FP32 inverse stored for an FP32 Krylov basis,
+// 36 B/cell, which the Arnoldi operator applies too, is read instead)
 template <typename VT = double>
 __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const double* __restrict__ pm,
                                                          const double* __restrict__ ph,
+                                                         const float* __restrict__ pinvf,
                                                          const double* __restrict__ r,
                                                          const double* __restrict__ ewt, VT* __restrict__ v0,
                                                          double gamma, double* partials, unsigned int* counter,
@@ -186,14 +189,18 @@ __global__ void __launch_bounds__(RT) k_psolve_scale_dot(DevProblem P, const dou
   const int n = P.ncell;
   if (da) gamma = da->gamma_setup;
   for (int k = blockIdx.x * RT + threadIdx.x; k < n; k += gridDim.x * RT) {
-    const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
-    const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
     const double rr[3] = {r[k], r[n + k], r[2 * n + k]};
-    double msk[3], nsk[3];
-    cell_axes(P, k, msk, nsk);
-    const double ws = P.windowed ? P.w[k] : 1.0;
     double Pi[9];
-    block_inverse(P, m, h, msk, ws, gamma, Pi);
+    if (pinvf) {
+      load_pinv(pinvf, n, k, Pi);
+    } else {
+      const double m[3] = {pm[k], pm[n + k], pm[2 * n + k]};
+      const double h[3] = {ph[k], ph[n + k], ph[2 * n + k]};
+      double msk[3], nsk[3];
+      cell_axes(P, k, msk, nsk);
+      const double ws = P.windowed ? P.w[k] : 1.0;
+      block_inverse(P, m, h, msk, ws, gamma, Pi);
+    }
     double g = 1.0;
     if (!P.windowed && P.act) g = P.act[k] ? 1.0 : 0.0;
     const double z0 = g * (Pi[0] * rr[0] + Pi[1] * rr[1] + Pi[2] * rr[2]);
@@ -595,8 +602,10 @@ static int psolve_scale_dot_impl(llg_ctx* c, const double* r, const double* ewt,
                                  int slot_aout) {
   if (!c->have_setup && !da) { llg_set_error("psolve before psetup"); return LLG_ERR_STATE; }
   LLG_COUNT(KID_PSOLVE);
-  klaunch(k_psolve_scale_dot<VT>, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pm, c->d_ph, r, ewt, v0,
-          c->gamma_setup, c->d_red, c->d_counter, c->d_scal + slot, da,
+  const float* pinvf = (sizeof(VT) == sizeof(float) && c->pinv_f32 && !da) ? reinterpret_cast<const float*>(c->d_pinv)
+                                                                          : nullptr;
+  klaunch(k_psolve_scale_dot<VT>, cell_blocks(c->ncell), RT, 0, c->stream, c->dp, c->d_pm, c->d_ph, pinvf, r, ewt,
+          v0, c->gamma_setup, c->d_red, c->d_counter, c->d_scal + slot, da,
           slot_aout >= 0 ? c->d_scal + slot_aout : nullptr);
   LLG_CUDA_TRY(cudaPeekAtLastError());
   return 0;
