@@ -459,7 +459,10 @@ def replay_accuracy(form, rank, t_out=(1.0, 5.0, 20.0, 200.0), t_floor=(1.0, 5.0
 
 def e2e_run(args, form, world, rank):
     """Same metric through the public API from host buffers: pinned y0 and
-    mask uploaded inside the timed region, one y(t) frame read back per step."""
+    mask uploaded inside the timed region, one y(t) frame read back per step.
+    The frames are read back on a copy stream from two alternating device
+    buffers, so each device-to-host copy overlaps the next step's work (a
+    buffer is written again only after its copy has finished)."""
     import torch
     p, g, o = form_params(form, 12345 + rank)
     n = p.ng * p.ny
@@ -470,9 +473,11 @@ def e2e_run(args, form, world, rank):
     geo2 = llg.build_geometry(g, want=("active", "y0"))
     mask_h = torch.from_numpy(np.tile(geo2["active"].astype(np.float64), 3)).pin_memory()
     y0_h = torch.from_numpy(geo2["y0"]).pin_memory()
-    frame_h = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+    frame_h = [torch.empty(3 * n, dtype=torch.float64).pin_memory() for _ in range(2)]
     y0_d = torch.empty(3 * n, dtype=torch.float64, device="cuda")
-    yo_d = torch.empty_like(y0_d)
+    yo_d = [torch.empty_like(y0_d) for _ in range(2)]
+    copy_stream = torch.cuda.Stream()
+    copied = [None, None]
     torch.cuda.synchronize()
     dist_barrier(world)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -481,21 +486,32 @@ def e2e_run(args, form, world, rank):
     y0_d.copy_(y0_h, non_blocking=True)
     ctx2.integrator_init(0.0, y0_d, o)
     tt = 0.0
-    for _ in range(args.steps):
+    main = torch.cuda.current_stream()
+    for i in range(args.steps):
+        b = i % 2
+        if copied[b] is not None:
+            main.wait_event(copied[b])   # the frame copy out of this buffer is done
         for k in range(sub):
-            ctx2.integrate(tt + args.dt * (k + 1) / sub, yo_d)
+            ctx2.integrate(tt + args.dt * (k + 1) / sub, yo_d[b])
         tt += args.dt
-        frame_h.copy_(yo_d, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(main)
+        copy_stream.wait_event(done)
+        with torch.cuda.stream(copy_stream):
+            frame_h[b].copy_(yo_d[b], non_blocking=True)
+            copied[b] = torch.cuda.Event()
+            copied[b].record(copy_stream)
+    main.wait_stream(copy_stream)
     f1.record()
     torch.cuda.synchronize()
     ems = dist_max(f0.elapsed_time(f1), world)
     ctx2.close()
     return {"value": world * args.steps * args.dt / (ems / 1000.0), "unit": UNIT,
             "h2d_bytes_per_step": int((y0_h.numel() * 8 + mask_h.numel() * 8) / args.steps),
-            "d2h_bytes_per_step": int(frame_h.numel() * 8),
+            "d2h_bytes_per_step": int(frame_h[0].numel() * 8),
             "note": "the timed window through the public API from host buffers: fresh instance from t=0, pinned "
-                    "y0 + mask uploaded inside the timed region (amortised over the steps), one y(t) frame "
-                    "copied back per step"}
+                    "y0 + mask uploaded and the integrator set up inside the timed region (amortised over the "
+                    "steps), one y(t) frame copied back per step on a copy stream, overlapping the next step"}
 
 
 def run_ours(args, world, rank, local):
