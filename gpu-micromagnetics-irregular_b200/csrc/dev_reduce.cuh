@@ -25,6 +25,30 @@ int red_blocks(long long n) {
   return (int)b;
 }
 
+// red_blocks(n) capped at the blocks that are resident at once (per_sm of
+// the kernel times the SMs): for kernels whose registers leave fewer than
+// red_blocks' count resident, each thread then takes more slice elements
+// instead of a second, partly filled wave running after the first.  The
+// partition still depends only on n, the kernel and the device.
+template <typename KernelT>
+int occ_per_sm(KernelT kernel) {
+  int p = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, kernel, RT, 0) != cudaSuccess) {
+    (void)cudaGetLastError();
+    p = 0;
+  }
+  return p;
+}
+inline int red_blocks_resident(long long n, int per_sm, int num_sms) {
+  const int b = red_blocks(n);
+  if (per_sm <= 0) return b;
+  const long long cap = (long long)per_sm * num_sms;
+  return (int)(b < cap ? b : cap);
+}
+// per_sm of one kernel, queried once per process (each expansion is its own
+// function-local static)
+#define LLG_PER_SM(kern) ([]() { static const int p_ = occ_per_sm(kern); return p_; }())
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -336,7 +336,9 @@ __global__ void __launch_bounds__(RT) k_lincomb_update(int nv, CPack c, XPackT<V
 // k_lincomb_update with the vector count NV fixed at compile time: the loads
 // of all NV vectors (and of w, ycor) for the UB slice elements are issued
 // before any of them is used.  Per element the same operations in the same
-// order, so the result is bitwise that of k_lincomb_update.
+// order, so the vectors are bitwise those of k_lincomb_update; it runs on one
+// resident wave of blocks (red_blocks_resident), so its two sums are added in
+// another partition.
 template <int NV, typename VT>
 __global__ void __launch_bounds__(RT) k_lincomb_update_k(CPack c, XPackT<VT> X, const double* __restrict__ w,
                                                          double* del, const double* ycor_in, double* ycor,
@@ -697,8 +699,9 @@ static int lincomb_update_impl(llg_ctx* c, int nv, const double* coef, const VT*
   const double* yin = ycor_zero ? nullptr : ycor;
   double* out = c->d_scal + slot;
   const Pub pub = take_publish(c);
-#define LU_K(NV) klaunch(k_lincomb_update_k<NV, VT>, nb, RT, 0, c->stream, cp, xp, w, del, yin, ycor, c->neq, c->d_red, \
-                         c->d_counter, out, kk, pub)
+#define LU_K(NV)                                                                                                   \
+  klaunch(k_lincomb_update_k<NV, VT>, red_blocks_resident(c->neq, LLG_PER_SM((k_lincomb_update_k<NV, VT>)), c->num_sms), \
+          RT, 0, c->stream, cp, xp, w, del, yin, ycor, c->neq, c->d_red, c->d_counter, out, kk, pub)
   switch (nv) {
     case 1: LU_K(1); break;
     case 2: LU_K(2); break;

@@ -282,8 +282,9 @@ __global__ void __launch_bounds__(RT) k_gs_update(int k, VPack<VT> X, const doub
 // k_gs_update with the vector count K fixed at compile time: the loads of
 // all K basis vectors (and of z) for the UB slice elements are issued before
 // any of them is used, where the runtime-k loop waits on one vector at a
-// time.  Per element the same operations in the same order, so the result is
-// bitwise that of k_gs_update.
+// time.  Per element the same operations in the same order, so z is bitwise
+// that of k_gs_update; it runs on one resident wave of blocks
+// (red_blocks_resident), so its sum of squares is added in another partition.
 template <int K, typename VT>
 __global__ void __launch_bounds__(RT) k_gs_update_k(VPack<VT> X, const double* __restrict__ dots, VT* z, long long n,
                                                     double* partials, unsigned int* counter, double* out, KScale ks,
@@ -497,7 +498,9 @@ static int vgs_update_impl(llg_ctx* c, int k, VT* const* V, int slot_dots, int s
   double* aout = slot_aout >= 0 ? c->d_scal + slot_aout : nullptr;
   const KScale kk = ks ? *ks : kz;
   const Pub pub = take_publish(c);
-#define GS_K(K) klaunch(k_gs_update_k<K, VT>, nb, RT, 0, c->stream, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout, pub)
+#define GS_K(K)                                                                                                  \
+  klaunch(k_gs_update_k<K, VT>, red_blocks_resident(c->neq, LLG_PER_SM((k_gs_update_k<K, VT>)), c->num_sms), RT, \
+          0, c->stream, pk, dots, V[k], c->neq, c->d_red, c->d_counter, ss, kk, aout, pub)
   switch (k) {
     case 1: GS_K(1); break;
     case 2: GS_K(2); break;
