@@ -39,11 +39,13 @@ int occ_per_sm(KernelT kernel) {
   }
   return p;
 }
-inline int red_blocks_resident(long long n, int per_sm, int num_sms) {
-  const int b = red_blocks(n);
+inline int cap_resident(int b, int per_sm, int num_sms) {
   if (per_sm <= 0) return b;
   const long long cap = (long long)per_sm * num_sms;
   return (int)(b < cap ? b : cap);
+}
+inline int red_blocks_resident(long long n, int per_sm, int num_sms) {
+  return cap_resident(red_blocks(n), per_sm, num_sms);
 }
 // per_sm of one kernel, queried once per process (each expansion is its own
 // function-local static)

@@ -744,7 +744,8 @@ int fused_predict(llg_ctx* c, int q, double* const* zn, const double* f, bool pe
   const int pe = pend ? 1 : 0, de = do_ewt ? 1 : 0;
   double* out = c->d_scal + slot;
 #define PRED(Q)                                                                                                \
-  klaunch(k_predict_fused<Q>, nb, RT, 0, c->stream, zp, fp, pe, de, rtol, atol, ewt, y, c->ncell, c->p.norm_kind,   \
+  klaunch(k_predict_fused<Q>, cap_resident(nb, LLG_PER_SM((k_predict_fused<Q>)), c->num_sms), RT, 0, c->stream,  \
+          zp, fp, pe, de, rtol, atol, ewt, y, c->ncell, c->p.norm_kind,                                          \
                                                c->p.norm_eps, c->d_red, c->d_counter, out, lz, lp, acor,         \
                                                lz ? zsave : nullptr)
   switch (q) {
@@ -770,7 +771,8 @@ int fused_complete(llg_ctx* c, int q, int qmax, const double* l, const double* a
   LLG_COUNT(KID_ELEMWISE);
   const int sv = save ? 1 : 0, nm = norms ? 1 : 0, st = store ? 1 : 0;
 #define COMP(Q)                                                                                    \
-  klaunch(k_complete_norms<Q>, red_blocks(c->neq), RT, 0, c->stream, qmax, lp, acor, zp, zn[qmax], sv, nm, -cquot, \
+  klaunch(k_complete_norms<Q>, red_blocks_resident(c->neq, LLG_PER_SM((k_complete_norms<Q>)), c->num_sms), RT, 0, \
+          c->stream, qmax, lp, acor, zp, zn[qmax], sv, nm, -cquot,                                                   \
                                                                 w, c->neq, c->d_red, c->d_counter,             \
                                                                 c->d_scal + slot, st)
   switch (q) {
